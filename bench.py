@@ -1,0 +1,472 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 batched Gaussian-splat camera renderer.
+
+python bench.py [--gpus N --steps K --warmup W] [--workload batched-1m-sh3|plain-10k-256]
+                [--impl b200|reference]
+
+One step renders the whole workload once (every camera, all four outputs).
+Default workload (batched-1m-sh3): 1,000,000 Gaussians with degree-3
+spherical harmonics, 64 pinhole cameras at 640x480 on a radius-8 orbit;
+seeded synthetic data of those shapes (no dataset).  Under torchrun each rank
+renders its own 64-camera rig against a replica of the scene (cameras are
+independent units; no collective on the data path), so scaling is weak.
+
+The JSON line reports Mpix/s: ``value`` is device-timed with the inputs
+resident in HBM, ``e2e`` is the same metric through the public
+RendererService API with the camera batch copied from pinned host memory and
+all four outputs copied back to pinned host memory inside the timed region.
+``roofline`` is for the kernel stage with the largest device time, timed live
+with CUDA events recorded by the library between its stages.
+``cpu_baseline`` times the CPU oracle (the restatement of the reference
+equation, there being no CPU renderer in the reference) on a bounded camera
+sample of the same workload.  ``--impl reference`` times that CPU path as the
+reference arm.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "vectorized-gaussian-renderer-public_b200"))
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "Mpix/s ragged batch + fwd+bwd ms/iter, chosen vs plain form at 1e-4 RGB err"
+UNIT = "Mpix/s"
+STAGES = ("setup", "project_emit", "sort_histogram", "sort_passes", "tile_ranges", "composite")
+KERNEL_NAMES = {
+    "setup": "camera_setup_kernel",
+    "project_emit": "project_emit_kernel",
+    "sort_histogram": "sort_histogram_kernel",
+    "sort_passes": "sort_onesweep_kernel",
+    "tile_ranges": "tile_ranges_kernel",
+    "composite": "composite_kernel",
+}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args() -> argparse.Namespace:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    parser.add_argument("--workload", choices=("batched-1m-sh3", "plain-10k-256"), default="batched-1m-sh3")
+    parser.add_argument("--cpu-sample-cameras", type=int, default=2)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-e2e", action="store_true")
+    return parser.parse_args()
+
+
+# --------------------------------------------------------------------------- workloads
+def make_workload(name: str, rank: int):
+    from vgr_b200 import workloads
+
+    if name == "plain-10k-256":
+        scene, rig = workloads.plain_workload()
+        return scene, rig, None, {"workload": name, "gaussians": 10_000, "cameras": 1,
+                                  "height": 256, "width": 256, "tile_size": 16, "color": "rgb"}
+    scene, rig = workloads.batched_workload()
+    if rank:
+        rig = workloads.orbit_cameras(64, seed=2 + rank)
+    return scene, rig, 3, {"workload": name, "gaussians": 1_000_000, "cameras": 64,
+                           "height": 480, "width": 640, "tile_size": 16, "color": "sh3"}
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def recorded_traffic(workload: str) -> dict[str, float]:
+    """Per-launch DRAM bytes from committed ncu summaries, if present."""
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(path.read_text()).get(workload, {})
+    except Exception:
+        return {}
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while timing."""
+
+    FIELDS = (
+        "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc: subprocess.Popen | None = None
+        self.lines: list[str] = []
+        self.thread: threading.Thread | None = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._pump, daemon=True)
+        self.thread.start()
+
+    def _pump(self) -> None:
+        assert self.proc is not None and self.proc.stdout is not None
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        sm, sm_max, power, reasons = [], [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                sm_max.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        under_load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {
+            "sm_mhz": statistics.median(under_load) if under_load else None,
+            "sm_max_mhz": max(sm_max) if sm_max else None,
+            "power_w_max": max(power) if power else None,
+            "samples": len(sm),
+            "reasons": sorted(reasons),
+        }
+
+
+# --------------------------------------------------------------------------- CPU path
+def oracle_inputs(scene, rig, cameras: list[int]):
+    from oracle import camera as oc
+
+    cov = oc.precompute_covariances(scene.scales.numpy(), scene.rotations.numpy())
+    return dict(
+        means=scene.means.numpy(), covariances=cov, opacities=scene.opacities.numpy(),
+        features=scene.features.numpy(), semantic_ids=scene.semantic_ids.numpy(),
+        registered_scene_ids=[0], scene_offsets=[0, scene.means.shape[0]],
+        viewmats=rig.viewmats.numpy()[cameras], intrinsics=rig.intrinsics.numpy()[cameras],
+        camera_scene_ids=[0] * len(cameras), height=rig.height, width=rig.width,
+    )
+
+
+def time_cpu(scene, rig, sh_degree, cameras: list[int], steps: int) -> tuple[float, float, int]:
+    """Mpix/s of the CPU oracle over ``steps`` renders of ``cameras``."""
+    from oracle import camera as oc
+
+    threads = os.cpu_count() or 1
+    kwargs = oracle_inputs(scene, rig, cameras)
+    kwargs["sh_degree"] = -1 if sh_degree is None else sh_degree
+    kwargs["threads"] = threads
+    start = time.perf_counter()
+    for _ in range(steps):
+        oc.render(**kwargs)
+    seconds = time.perf_counter() - start
+    pixels = len(cameras) * rig.height * rig.width * steps
+    return pixels / seconds / 1e6, seconds, threads
+
+
+# --------------------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------- arms
+def run_reference(args) -> None:
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    scene, rig, sh_degree, config = make_workload(args.workload, 0)
+    sample = list(range(min(args.cpu_sample_cameras, rig.viewmats.shape[0])))
+    for _ in range(max(args.warmup, 0) and 1):
+        time_cpu(scene, rig, sh_degree, sample[:1], 1)
+    value, seconds, threads = time_cpu(scene, rig, sh_degree, sample, max(args.steps, 1))
+    sample_desc = (f"{len(sample)} of {rig.viewmats.shape[0]} cameras per step "
+                   f"({len(sample) * rig.height * rig.width} px, full scene), {args.steps} steps")
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(seconds * 1e3 / max(args.steps, 1), 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": config,
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample_desc},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def stage_bytes(counters: dict, scene, rig, passes: int, sh_degree) -> dict[str, float]:
+    """Algorithmic bytes per launch of each stage.
+
+    G Gaussians, B cameras, V visible records, I tile intersections, P pixels.
+    """
+    g = scene.means.shape[0]
+    b = rig.viewmats.shape[0]
+    v = counters["visible_gaussians"]
+    i = counters["tile_intersections"]
+    p = b * rig.height * rig.width
+    color = 4 * scene.features.shape[1]
+    scene_read = g * (12 + 24 + 4)  # mean, covariance, opacity (once, L2 reuse across cameras)
+    return {
+        "setup": b * (64 + 36 + 64 + 8) + b * 56,
+        "project_emit": scene_read + v * color + v * 48 + i * 12,
+        "sort_histogram": i * 8,
+        "sort_passes": passes * i * 24,
+        "tile_ranges": i * 8,
+        "composite": i * (4 + 48 + 8) + p * 28,
+    }
+
+
+def run_b200(args) -> None:
+    world, rank, local = dist_setup()
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device (the renderer has no CPU fallback)")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    from vgr_b200 import CustomCudaBackend, RendererService, _native
+
+    scene, rig, sh_degree, config = make_workload(args.workload, rank)
+    batch = rig.viewmats.shape[0]
+    backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=config["tile_size"])
+    service = RendererService(backend, height=rig.height, width=rig.width, max_views=batch)
+    service.initialize(stage=None, device=device)
+    service.load_scene(0, **scene.to(device).as_kwargs())
+    viewmats = rig.viewmats.to(device)
+    intrinsics = rig.intrinsics.to(device)
+    scene_ids = torch.zeros((batch,), dtype=torch.int64, device=device)
+    outputs = service.prepare_outputs(batch)
+
+    # Calibrate capacity with the adaptive policy, then time in explicit mode
+    # (the capacity is checked again after the timed region).
+    service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
+    counters = backend.read_counters()
+    backend.adaptive_capacity = False
+
+    for _ in range(args.warmup):
+        service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
+    torch.cuda.synchronize(device)
+
+    stream = torch.cuda.current_stream(device)
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(_native.STAGE_EVENTS)]
+              for _ in range(args.steps)]
+    for ev in events:
+        backend.set_stage_events(ev)
+    backend.set_stage_events(None)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    lib = _native.load_library()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = lib.vgr_kernel_launch_count()
+    start.record(stream)
+    for step in range(args.steps):
+        backend.set_stage_events(events[step])
+        service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    launches = lib.vgr_kernel_launch_count() - launches0
+    barrier(world)
+    clocks = sampler.stop()
+    backend.set_stage_events(None)
+    elapsed_ms = max_over_ranks(start.elapsed_time(stop), world, device)
+    check = backend.check_capacity()
+    stage_ms = {name: [] for name in STAGES}
+    for ev in events:
+        for k, name in enumerate(STAGES):
+            stage_ms[name].append(ev[k].elapsed_time(ev[k + 1]))
+    stage_avg = {name: statistics.fmean(vals) for name, vals in stage_ms.items()}
+
+    pixels_per_step = batch * rig.height * rig.width
+    value = world * pixels_per_step * args.steps / (elapsed_ms / 1e3) / 1e6
+
+    # End to end through the public API with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        host_view = rig.viewmats.pin_memory()
+        host_intr = rig.intrinsics.pin_memory()
+        host_out = {name: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for name, t in outputs.items()}
+        h2d = host_view.numel() * 4 + host_intr.numel() * 4
+        d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+        e2e_steps = max(2, min(args.steps, 10))
+        for _ in range(2):
+            viewmats.copy_(host_view, non_blocking=True)
+            service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        e_start = torch.cuda.Event(enable_timing=True)
+        e_stop = torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        for _ in range(e2e_steps):
+            viewmats.copy_(host_view, non_blocking=True)
+            intrinsics.copy_(host_intr, non_blocking=True)
+            service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
+            for name, t in outputs.items():
+                host_out[name].copy_(t, non_blocking=True)
+        e_stop.record(stream)
+        torch.cuda.synchronize(device)
+        e_ms = max_over_ranks(e_start.elapsed_time(e_stop), world, device)
+        e2e = {
+            "value": round(world * pixels_per_step * e2e_steps / (e_ms / 1e3) / 1e6, 3),
+            "unit": UNIT,
+            "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "steps": e2e_steps,
+        }
+
+    # Roofline of the dominant stage.
+    from vgr_b200.cuda_backend import _emitted_sort_key_end_bit  # noqa: F401
+
+    near_bits = np.float32(backend.near_plane).view(np.uint32)
+    far_bits = np.float32(backend.far_plane).view(np.uint32)
+    tiles = batch * math.ceil(rig.height / config["tile_size"]) * math.ceil(rig.width / config["tile_size"])
+    key_bits = int(far_bits - near_bits).bit_length() + (tiles - 1).bit_length()
+    passes = math.ceil(key_bits / 8)
+    bytes_per_stage = stage_bytes(counters, scene, rig, passes, sh_degree)
+    dominant = max(stage_avg, key=stage_avg.get)
+    peak, peak_kind = measured_peaks()
+    traffic_table = recorded_traffic(config["workload"])
+    achieved = bytes_per_stage[dominant] / (stage_avg[dominant] / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm",
+        "kernel": KERNEL_NAMES[dominant],
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "peak_source": f"hbm_gbs of {peak_kind}",
+        "traffic": traffic_table.get(KERNEL_NAMES[dominant]),
+        "algorithmic_bytes": int(bytes_per_stage[dominant]),
+        "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
+        "stage_frac_of_measured_hbm": {
+            k: round(bytes_per_stage[k] / (stage_avg[k] / 1e3) / 1e9 / peak, 4)
+            for k in STAGES if stage_avg[k] > 0
+        },
+    }
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = list(range(min(args.cpu_sample_cameras, batch)))
+        cpu_value, _, threads = time_cpu(scene, rig, sh_degree, sample, 1)
+        cpu_baseline = {
+            "value": round(cpu_value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of {batch} cameras ({len(sample) * rig.height * rig.width} px), full scene, 1 render",
+        }
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(value, 3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(elapsed_ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {**config, "parallelism": f"camera-shard x{world}" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (scene 240 MB, keys/values > 126 MB)",
+                       "visible_records": counters["visible_gaussians"],
+                       "tile_intersections": counters["tile_intersections"]},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu_baseline,
+            "clocks": clocks,
+            "capacity_check": {k: check[k] for k in ("visible_overflow", "intersection_overflow")},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,219 @@
+/*
+ * vgr_b200.h -- C ABI of the B200-native batched Gaussian-splat sensor renderer.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream (as void*),
+ * enqueues its work on that stream, never synchronises the host and never
+ * allocates device memory.  Functions return VGR_OK (0) on success or a
+ * negative VGR_ERR_* code; vgr_last_error() then returns a thread-local
+ * message naming the violated contract (the same checks the reference
+ * performs with TORCH_CHECK in its pybind binding).
+ *
+ * The entry points replace the functions the reference exports from its
+ * PyTorch extension modules:
+ *   src/isaacsim_gaussian_renderer/native/renderer.cpp:312-337        (camera)
+ *   src/isaacsim_gaussian_renderer/native/lidar_renderer.cpp:213-216  (LiDAR)
+ * Each declaration below names the reference function and the file:line of
+ * its definition.  Tensor-order enums of the reference camera module are
+ * at src/isaacsim_gaussian_renderer/native/renderer_cuda.cu:48-98; the
+ * structs below carry the same tensors by name.
+ */
+#ifndef VGR_B200_H_
+#define VGR_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VGR_OK 0
+#define VGR_ERR_INVALID_ARGUMENT (-1)
+#define VGR_ERR_CUDA (-2)
+#define VGR_ERR_SCRATCH_TOO_SMALL (-3)
+#define VGR_ERR_UNSUPPORTED (-4)
+
+/* Counter slots, same order as the reference COUNTER_NAMES
+ * (src/isaacsim_gaussian_renderer/cuda_backend.py:22-28). */
+#define VGR_COUNTER_VISIBLE 0
+#define VGR_COUNTER_INTERSECTIONS 1
+#define VGR_COUNTER_VISIBLE_OVERFLOW 2
+#define VGR_COUNTER_INTERSECTION_OVERFLOW 3
+#define VGR_COUNTER_ACTIVE_TILES 4
+#define VGR_COUNTER_COUNT 5
+
+/* One projected (camera, Gaussian) record: 48 bytes, 16-byte aligned.
+ *   a = (mean_x, mean_y, conic_xx, conic_xy)
+ *   b = (conic_yy, opacity, depth, bits(gaussian id))
+ *   c = (red, green, blue, bits(two fp16 half-extents of the footprint box)) */
+#define VGR_RECORD_BYTES 48
+
+/* Packed scene in the reference's canonical layout (scene.py:12-33 after
+ * covariance precompute, cuda_backend.py:2080-2108). */
+typedef struct vgr_scene {
+  const float* means;                  /* [G,3] */
+  const float* covariances;            /* [G,6] upper triangle 00,01,02,11,12,22 */
+  const float* opacities;              /* [G] activated */
+  const float* features;               /* [G,F]; F>=3 */
+  int64_t feature_width;               /* F */
+  const int64_t* semantic_ids;         /* [G] */
+  const int64_t* registered_scene_ids; /* [S] */
+  const int64_t* scene_offsets;        /* [S+1] packed offsets */
+  int64_t scene_count;                 /* S */
+  int64_t gaussian_count;              /* G */
+  int64_t max_scene_gaussians;         /* max_s (offsets[s+1]-offsets[s]) */
+} vgr_scene;
+
+/* Camera batch.  The plain form leaves the four per-camera resolution arrays
+ * NULL and renders every camera at (height,width) of vgr_render_options.
+ * The ragged form passes per-camera widths/heights plus exclusive prefixes of
+ * tiles and pixels over the batch (device int64 arrays of length B+1). */
+typedef struct vgr_cameras {
+  const float* viewmats;           /* [B,4,4] world->OpenCV camera */
+  const float* intrinsics;         /* [B,3,3] */
+  const float* env_xforms;         /* [B,4,4] object->world */
+  const int64_t* camera_scene_ids; /* [B] */
+  const int64_t* active_camera_ids;/* [A] or NULL (all cameras) */
+  int64_t batch;                   /* B */
+  int64_t active_count;            /* A (== B when active_camera_ids is NULL) */
+  const int32_t* widths;           /* ragged form: [B] or NULL */
+  const int32_t* heights;          /* ragged form: [B] or NULL */
+  const int64_t* tile_offsets;     /* ragged form: [B+1] or NULL */
+  const int64_t* pixel_offsets;    /* ragged form: [B+1] or NULL */
+  int64_t total_tiles;             /* ragged form: tile_offsets[B] (host copy) */
+  int64_t max_tiles_per_camera;    /* ragged form: max over cameras */
+} vgr_cameras;
+
+/* Outputs, pixel-major.  Plain form: [B,H,W,C]; ragged form: [P,C] with
+ * camera c at pixel_offsets[c].  depth/alpha/semantic may be NULL when
+ * full_sensor_output is 0 (RGB-only contract). */
+typedef struct vgr_outputs {
+  float* rgb;        /* 3 channels */
+  float* depth;      /* 1 channel */
+  float* alpha;      /* 1 channel */
+  int64_t* semantic; /* 1 channel */
+} vgr_outputs;
+
+typedef struct vgr_workspace {
+  void* records;                 /* visible_capacity * VGR_RECORD_BYTES, 16-B aligned */
+  int64_t visible_capacity;
+  uint64_t* keys_in;             /* [I] sort keys (tile<<32 | depth bits) */
+  uint64_t* keys_out;            /* [I] */
+  int32_t* values_in;            /* [I] visible-record indices */
+  int32_t* values_out;           /* [I] */
+  int64_t intersection_capacity; /* I */
+  int32_t* tile_starts;          /* [T] */
+  int32_t* tile_ends;            /* [T] */
+  int64_t tile_capacity;         /* T >= global tile count */
+  int64_t* counters;             /* [5] */
+  void* scratch;                 /* vgr_render_scratch_bytes(...) bytes, 256-B aligned */
+  int64_t scratch_bytes;
+  /* Optional structure-of-arrays mirrors of the visible records in the
+   * reference workspace layout (renderer_cuda.cu:74-80); NULL skips them. */
+  float* visible_means2d;        /* [V,2] */
+  float* visible_conics;         /* [V,3] */
+  float* visible_depths;         /* [V] */
+  float* visible_opacities;      /* [V] */
+  int32_t* visible_camera_ids;   /* [V] */
+  int32_t* visible_gaussian_ids; /* [V] */
+  int32_t* visible_radii;        /* [V,2] */
+} vgr_workspace;
+
+typedef struct vgr_render_options {
+  int64_t height;                 /* plain-form resolution */
+  int64_t width;
+  double near_plane;
+  double far_plane;
+  double gaussian_support_sigma;
+  double covariance_epsilon;
+  double semantic_min_alpha;
+  int32_t antialiased;
+  int32_t ray_gaussian_evaluation; /* must be 0 (exact-ray mode is not built) */
+  int32_t tile_size;               /* 4, 8 or 16 */
+  int32_t output_srgb;
+  int32_t deterministic;           /* accepted; ordering is always deterministic */
+  int32_t full_sensor_output;
+  int32_t fixed_capacity_sort;     /* accepted; the sort is always device-bounded */
+  int32_t reuse_projection;        /* composite only, from the last sorted lists */
+  int32_t compact_projection_cache;/* must be 0 (dense 1x1 path is not built) */
+  int32_t sh_degree;               /* -1: features[0..2] are linear RGB (reference);
+                                      0..3: real spherical harmonics, [G,(d+1)^2*3] */
+  int32_t sorted_buffer_hint;      /* reuse_projection: 1 if sorted data lives in *_out */
+  /* Optional timing hook (no counterpart in the reference): when non-NULL,
+   * stage_events[i] (cudaEvent_t) is recorded on the stream at stage
+   * boundary i: 0 start, 1 after camera setup, 2 after projection+emission,
+   * 3 after the sort histogram, 4 after the radix passes, 5 after tile
+   * ranges, 6 after compositing.  stage_event_count must be 7. */
+  void* const* stage_events;
+  int32_t stage_event_count;
+} vgr_render_options;
+
+#define VGR_STAGE_EVENTS 7
+
+/* Library identity. */
+const char* vgr_version(void);
+/* Number of kernels this library has launched in this process (all threads).
+ * No counterpart in the reference; used to attribute launches in benchmarks. */
+int64_t vgr_kernel_launch_count(void);
+/* Thread-local message of the last failing call on this thread. */
+const char* vgr_last_error(void);
+
+/* Scratch bytes vgr_render needs for a given intersection capacity, projection
+ * task bound (active cameras * max scene Gaussians), global tile count and
+ * active-camera bound.  No counterpart in the reference: the reference sizes
+ * CUB temporary storage through the two functions below. */
+int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
+                                 int64_t max_projection_tasks,
+                                 int64_t global_tiles,
+                                 int64_t max_active_cameras);
+
+/* Replaces sort_temp_bytes (renderer.cpp:76-81, renderer_cuda.cu:2463-2508).
+ * Returns the scratch bytes of the deterministic path for num_items keys and
+ * num_segments tiles, or a negative error code. */
+int64_t vgr_sort_temp_bytes(int64_t num_items, int64_t num_segments);
+
+/* Replaces radix_sort_double_buffer_temp_bytes (renderer.cpp:83-90,
+ * renderer_cuda.cu:2510-2534). */
+int64_t vgr_radix_sort_double_buffer_temp_bytes(int64_t num_items,
+                                                int64_t num_segments);
+
+/* Replaces precompute_covariances (renderer.cpp:92-131,
+ * renderer_cuda.cu:492-540,2374-2395): Sigma = R S S^T R^T from WXYZ
+ * quaternions and activated scales, upper triangle [G,6]. */
+int vgr_precompute_covariances(const float* scales, const float* rotations,
+                               int64_t gaussian_count, float* covariances,
+                               void* stream);
+
+/* Replaces prepare_chunked_active_ids (renderer.cpp:133-181,
+ * renderer_cuda.cu:2307-2338,2397-2444). */
+int vgr_prepare_chunked_active_ids(const int64_t* active_camera_ids,
+                                   int64_t active_count, int32_t* active_mask,
+                                   int64_t active_mask_capacity,
+                                   int64_t* chunk_active_ids,
+                                   int64_t chunk_rows, int64_t chunk_columns,
+                                   int64_t logical_batch,
+                                   int64_t physical_batch, void* stream);
+
+/* Replaces aggregate_chunk_counters (renderer.cpp:183-212,
+ * renderer_cuda.cu:2340-2360,2446-2461). */
+int vgr_aggregate_chunk_counters(const int64_t* chunk_counters,
+                                 int64_t chunk_rows, int64_t chunk_stride,
+                                 int64_t* counters,
+                                 int64_t* physical_capacity_counters,
+                                 int64_t chunk_count, void* stream);
+
+/* Replaces render (renderer.cpp:214-310, renderer_cuda.cu:2536-3456):
+ * projection + ordered compaction + tile emission, device-bounded stable LSD
+ * radix sort of (tile, depth) keys, tile ranges and the fused
+ * RGB/depth/alpha/semantic compositor.  *sorted_buffer_selector receives 1
+ * when keys_out/values_out hold the sorted lists and 0 when keys_in/values_in
+ * do (the reference's CUB DoubleBuffer selector). */
+int vgr_render(const vgr_scene* scene, const vgr_cameras* cameras,
+               const vgr_outputs* outputs, const vgr_workspace* workspace,
+               const vgr_render_options* options, void* stream,
+               int64_t* sorted_buffer_selector);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VGR_B200_H_ */

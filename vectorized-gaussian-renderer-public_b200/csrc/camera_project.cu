@@ -1,0 +1,652 @@
+// Camera setup, EWA projection, ordered compaction and tile emission.
+//
+// Follows the reference camera equation of
+// src/isaacsim_gaussian_renderer/native/renderer_cuda.cu:287-490 (projection,
+// cull, radius, conic) and :1691-1829 (tile cover and key), restructured for
+// B200: one persistent launch walks virtual blocks of kProjectChunk
+// (camera, Gaussian) tasks handed out by an atomic ticket, compacts visible
+// records and their tile intersections in task order through a decoupled
+// look-back prefix (so the visible list and the key list are deterministic,
+// ascending Gaussian id within each camera), and emits the keys cooperatively
+// from shared memory so every store is coalesced.  There is no host round
+// trip: the emitted count stays on the device for the sort.
+#include "vgr_camera.cuh"
+#include "vgr_kernels.h"
+
+namespace vgr {
+
+// ---------------------------------------------------------------------------
+// Camera setup: one CTA builds the per-active-camera plans, the exclusive
+// prefix of tiles over active cameras (the compositor's work list), and
+// zeroes counters and queue tickets so the frame needs no host memset.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) camera_setup_kernel(SetupParams p) {
+  __shared__ int64_t s_warp_sums[32];
+  __shared__ int64_t s_carry;
+  ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
+  CamPlan* plans = reinterpret_cast<CamPlan*>(p.scratch + p.layout.plans);
+  int64_t* tile_prefix = reinterpret_cast<int64_t*>(p.scratch + p.layout.tile_prefix);
+  const int tid = threadIdx.x;
+  if (tid < 32) {
+    reinterpret_cast<uint32_t*>(header)[tid] = 0u;
+  }
+  if (p.reset_counters && tid < 5) {
+    p.counters[tid] = 0;
+  }
+  if (p.reset_counters) {
+    uint32_t* hist = reinterpret_cast<uint32_t*>(p.scratch + p.layout.sort_hist);
+    for (int i = tid; i < kMaxSortPasses * kRadixBins; i += blockDim.x) hist[i] = 0u;
+  }
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+
+  for (int64_t base = 0; base < p.active_count; base += blockDim.x) {
+    const int64_t a = base + tid;
+    int64_t tiles = 0;
+    if (a < p.active_count) {
+      CamPlan plan;
+      const int64_t cam64 = p.active_ids ? p.active_ids[a] : a;
+      plan.camera = -1;
+      plan.scene_slot = -1;
+      plan.g_begin = 0;
+      plan.g_count = 0;
+      plan.width = 0;
+      plan.height = 0;
+      plan.tiles_x = 0;
+      plan.tiles_y = 0;
+      plan.tile_base = 0;
+      plan.pixel_base = 0;
+      if (cam64 >= 0 && cam64 < p.batch) {
+        const int cam = static_cast<int>(cam64);
+        plan.camera = cam;
+        const int64_t requested = p.camera_scene_ids[cam];
+        for (int s = 0; s < p.scene_count; ++s) {
+          if (p.registered_scene_ids[s] == requested) {
+            plan.scene_slot = s;
+            break;
+          }
+        }
+        if (plan.scene_slot >= 0) {
+          plan.g_begin = p.scene_offsets[plan.scene_slot];
+          plan.g_count = p.scene_offsets[plan.scene_slot + 1] - plan.g_begin;
+          if (plan.g_count < 0) plan.g_count = 0;
+        }
+        if (p.widths) {
+          plan.width = p.widths[cam];
+          plan.height = p.heights[cam];
+          plan.tile_base = p.tile_offsets[cam];
+          plan.pixel_base = p.pixel_offsets[cam];
+        } else {
+          plan.width = p.width;
+          plan.height = p.height;
+        }
+        plan.tiles_x = (plan.width + p.tile_size - 1) / p.tile_size;
+        plan.tiles_y = (plan.height + p.tile_size - 1) / p.tile_size;
+        if (!p.widths) {
+          plan.tile_base = static_cast<int64_t>(cam) * plan.tiles_x * plan.tiles_y;
+          plan.pixel_base = static_cast<int64_t>(cam) * plan.width * plan.height;
+        }
+        tiles = static_cast<int64_t>(plan.tiles_x) * plan.tiles_y;
+      }
+      plans[a] = plan;
+    }
+    // Block-wide exclusive scan of tiles.
+    int64_t v = tiles;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t n = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += n;
+    }
+    if (lane == 31) s_warp_sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      int64_t w = (lane < static_cast<int>(blockDim.x >> 5)) ? s_warp_sums[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t n = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += n;
+      }
+      s_warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const int64_t warp_prefix = warp > 0 ? s_warp_sums[warp - 1] : 0;
+    const int64_t inclusive = s_carry + warp_prefix + v;
+    if (a < p.active_count) tile_prefix[a] = inclusive - tiles;
+    __syncthreads();
+    if (tid == static_cast<int>(blockDim.x) - 1) s_carry = inclusive;
+    __syncthreads();
+  }
+  if (tid == 0) tile_prefix[p.active_count] = s_carry;
+}
+
+// ---------------------------------------------------------------------------
+// Per-camera constants of the projection, computed once per virtual block.
+// R = view_rotation * env_rotation and t = view_rotation * env_t + view_t,
+// so camera-space p = R m + t.
+// ---------------------------------------------------------------------------
+struct CamConst {
+  float r[9];
+  float t[3];
+  float fx, fy, cx, cy;
+  float lim_xp, lim_xn, lim_yp, lim_yn;
+  float width, height;
+};
+
+__device__ __forceinline__ void make_cam_const(const float* view, const float* env,
+                                               const float* intr, int width, int height,
+                                               CamConst* c) {
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col) {
+      c->r[row * 3 + col] =
+          ffma(view[row * 4 + 2], env[8 + col],
+               ffma(view[row * 4 + 1], env[4 + col], fmul(view[row * 4 + 0], env[col])));
+    }
+    c->t[row] = ffma(view[row * 4 + 2], env[11],
+                     ffma(view[row * 4 + 1], env[7],
+                          ffma(view[row * 4 + 0], env[3], view[row * 4 + 3])));
+  }
+  c->fx = intr[0];
+  c->fy = intr[4];
+  c->cx = intr[2];
+  c->cy = intr[5];
+  const float w = static_cast<float>(width);
+  const float h = static_cast<float>(height);
+  c->width = w;
+  c->height = h;
+  const float tan_x = fdiv(fmul(0.5f, w), c->fx);
+  const float tan_y = fdiv(fmul(0.5f, h), c->fy);
+  c->lim_xp = ffma(0.3f, tan_x, fdiv(fsub(w, c->cx), c->fx));
+  c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
+  c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
+  c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
+}
+
+struct Projected {
+  float mean_x, mean_y;
+  float conic0, conic1, conic2;
+  float opacity;
+  float depth;
+  float cov_a, cov_b, cov_c;
+  float px, py, pz;
+  int radius_x, radius_y;
+};
+
+// EWA projection of one Gaussian (renderer_cuda.cu:287-490 screen-space path).
+__device__ __forceinline__ bool project_gaussian(const float* __restrict__ means,
+                                                 const float* __restrict__ covariances,
+                                                 const float* __restrict__ opacities,
+                                                 int64_t g, const CamConst& c, float near_plane,
+                                                 float far_plane, float support_sigma,
+                                                 float cov_eps, bool antialiased,
+                                                 Projected* out) {
+  float o = opacities[g];
+  if (!(o >= kAlphaThreshold)) return false;
+  const float mx = means[g * 3 + 0];
+  const float my = means[g * 3 + 1];
+  const float mz = means[g * 3 + 2];
+  const float pz = ffma(c.r[8], mz, ffma(c.r[7], my, ffma(c.r[6], mx, c.t[2])));
+  if (pz < near_plane || pz > far_plane) return false;
+  const float px = ffma(c.r[2], mz, ffma(c.r[1], my, ffma(c.r[0], mx, c.t[0])));
+  const float py = ffma(c.r[5], mz, ffma(c.r[4], my, ffma(c.r[3], mx, c.t[1])));
+  const float iz = fdiv(1.0f, pz);
+  const float u = ffma(fmul(c.fx, px), iz, c.cx);
+  const float v = ffma(fmul(c.fy, py), iz, c.cy);
+
+  const float* s = covariances + g * 6;
+  const float s00 = s[0], s01 = s[1], s02 = s[2], s11 = s[3], s12 = s[4], s22 = s[5];
+  float tm[9];
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+    const float r0 = c.r[row * 3 + 0], r1 = c.r[row * 3 + 1], r2 = c.r[row * 3 + 2];
+    tm[row * 3 + 0] = ffma(r2, s02, ffma(r1, s01, fmul(r0, s00)));
+    tm[row * 3 + 1] = ffma(r2, s12, ffma(r1, s11, fmul(r0, s01)));
+    tm[row * 3 + 2] = ffma(r2, s22, ffma(r1, s12, fmul(r0, s02)));
+  }
+#define VGR_COV(i, j) \
+  ffma(tm[i * 3 + 2], c.r[j * 3 + 2], ffma(tm[i * 3 + 1], c.r[j * 3 + 1], fmul(tm[i * 3 + 0], c.r[j * 3 + 0])))
+  const float c00 = VGR_COV(0, 0);
+  const float c01 = VGR_COV(0, 1);
+  const float c02 = VGR_COV(0, 2);
+  const float c11 = VGR_COV(1, 1);
+  const float c12 = VGR_COV(1, 2);
+  const float c22 = VGR_COV(2, 2);
+#undef VGR_COV
+
+  const float tx = fmul(px, iz);
+  const float ty = fmul(py, iz);
+  const float clx = fmul(pz, fminf(c.lim_xp, fmaxf(-c.lim_xn, tx)));
+  const float cly = fmul(pz, fminf(c.lim_yp, fmaxf(-c.lim_yn, ty)));
+  const float iz2 = fmul(iz, iz);
+  const float j00 = fmul(c.fx, iz);
+  const float j02 = fmul(fmul(-c.fx, clx), iz2);
+  const float j11 = fmul(c.fy, iz);
+  const float j12 = fmul(fmul(-c.fy, cly), iz2);
+  const float a_raw =
+      ffma(fmul(j02, j02), c22, ffma(fmul(fmul(2.0f, j00), j02), c02, fmul(fmul(j00, j00), c00)));
+  const float b = ffma(fmul(j02, j12), c22,
+                       ffma(fmul(j02, j11), c12, ffma(fmul(j00, j12), c02, fmul(fmul(j00, j11), c01))));
+  const float c_raw =
+      ffma(fmul(j12, j12), c22, ffma(fmul(fmul(2.0f, j11), j12), c12, fmul(fmul(j11, j11), c11)));
+  const float a = fadd(a_raw, cov_eps);
+  const float cc = fadd(c_raw, cov_eps);
+  const float det = ffma(a, cc, -fmul(b, b));
+  if (!(det > 0.0f)) return false;
+  if (antialiased) {
+    const float det_raw = ffma(a_raw, c_raw, -fmul(b, b));
+    const float floor2 = fmul(kMinAntialiasCompensation, kMinAntialiasCompensation);
+    const float comp = fsqrt(fmaxf(floor2, fdiv(det_raw, det)));
+    o = fmul(o, comp);
+    if (!(o >= kAlphaThreshold)) return false;
+  }
+  const float ext_o = fsqrt(fmul(2.0f, vlog(fdiv(o, kAlphaThreshold))));
+  const float ext = fminf(support_sigma, ext_o);
+  const int rx = ceil_radius(fmul(ext, fsqrt(a)));
+  const int ry = ceil_radius(fmul(ext, fsqrt(cc)));
+  if (rx <= 0 && ry <= 0) return false;
+  const float frx = static_cast<float>(rx);
+  const float fry = static_cast<float>(ry);
+  if (fadd(u, frx) <= 0.0f || fadd(v, fry) <= 0.0f || fsub(u, frx) >= c.width ||
+      fsub(v, fry) >= c.height) {
+    return false;
+  }
+  const float idet = fdiv(1.0f, det);
+  out->mean_x = u;
+  out->mean_y = v;
+  out->conic0 = fmul(cc, idet);
+  out->conic1 = fmul(-b, idet);
+  out->conic2 = fmul(a, idet);
+  out->opacity = fminf(fmaxf(o, 0.0f), 1.0f);
+  out->depth = pz;
+  out->cov_a = a;
+  out->cov_b = b;
+  out->cov_c = cc;
+  out->px = px;
+  out->py = py;
+  out->pz = pz;
+  out->radius_x = rx;
+  out->radius_y = ry;
+  return true;
+}
+
+// Real spherical harmonics through degree 3 (the basis and constants of the
+// 3D Gaussian Splatting reference implementation, as used by gsplat), view
+// direction from the camera centre to the mean in object space, +0.5 offset,
+// clamped at zero.  coeffs is [(d+1)^2, 3], coefficient-major.
+__device__ __forceinline__ void eval_sh(int degree, const float* __restrict__ coeffs,
+                                        const CamConst& c, float px, float py, float pz,
+                                        float* rgb) {
+  float dx = ffma(c.r[6], pz, ffma(c.r[3], py, fmul(c.r[0], px)));
+  float dy = ffma(c.r[7], pz, ffma(c.r[4], py, fmul(c.r[1], px)));
+  float dz = ffma(c.r[8], pz, ffma(c.r[5], py, fmul(c.r[2], px)));
+  const float inv = fdiv(1.0f, fsqrt(ffma(dz, dz, ffma(dy, dy, fmul(dx, dx)))));
+  const float x = fmul(dx, inv), y = fmul(dy, inv), z = fmul(dz, inv);
+  float basis[16];
+  basis[0] = 0.28209479177387814f;
+  int count = 1;
+  if (degree >= 1) {
+    basis[1] = fmul(-0.4886025119029199f, y);
+    basis[2] = fmul(0.4886025119029199f, z);
+    basis[3] = fmul(-0.4886025119029199f, x);
+    count = 4;
+  }
+  const float xx = fmul(x, x), yy = fmul(y, y), zz = fmul(z, z);
+  const float xy = fmul(x, y), yz = fmul(y, z), xz = fmul(x, z);
+  if (degree >= 2) {
+    basis[4] = fmul(1.0925484305920792f, xy);
+    basis[5] = fmul(-1.0925484305920792f, yz);
+    basis[6] = fmul(0.31539156525252005f, fsub(fsub(fmul(2.0f, zz), xx), yy));
+    basis[7] = fmul(-1.0925484305920792f, xz);
+    basis[8] = fmul(0.5462742152960396f, fsub(xx, yy));
+    count = 9;
+  }
+  if (degree >= 3) {
+    basis[9] = fmul(fmul(-0.5900435899266435f, y), fsub(fmul(3.0f, xx), yy));
+    basis[10] = fmul(fmul(2.890611442640554f, xy), z);
+    basis[11] = fmul(fmul(-0.4570457994644658f, y), fsub(fsub(fmul(4.0f, zz), xx), yy));
+    basis[12] = fmul(fmul(0.3731763325901154f, z),
+                     fsub(fsub(fmul(2.0f, zz), fmul(3.0f, xx)), fmul(3.0f, yy)));
+    basis[13] = fmul(fmul(-0.4570457994644658f, x), fsub(fsub(fmul(4.0f, zz), xx), yy));
+    basis[14] = fmul(fmul(1.445305721320277f, z), fsub(xx, yy));
+    basis[15] = fmul(fmul(-0.5900435899266435f, x), fsub(xx, fmul(3.0f, yy)));
+    count = 16;
+  }
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    float acc = fmul(basis[0], coeffs[ch]);
+    for (int k = 1; k < count; ++k) acc = ffma(basis[k], coeffs[k * 3 + ch], acc);
+    rgb[ch] = fmaxf(fadd(acc, 0.5f), 0.0f);
+  }
+}
+
+// Conservative half-extents (pixels) of the region where a record can reach
+// alpha >= 1/255 before the power < -20 cut: the ellipse q(d) <= t with
+// t = min(40, 2 ln(255 o)).  Used only to skip warps that cannot be touched;
+// ill-conditioned footprints report an infinite box (no skipping).
+__device__ __forceinline__ uint32_t footprint_box(float opacity, float a, float b, float c) {
+  const float t = fminf(40.0f, 2.0f * __logf(255.0f * opacity)) * 1.002f + 0.02f;
+  const float det = a * c - b * b;
+  const float kappa = (a * c) / det;
+  float hx = sqrtf(fmaxf(t, 0.0f) * a) * 1.002f + 0.02f;
+  float hy = sqrtf(fmaxf(t, 0.0f) * c) * 1.002f + 0.02f;
+  if (!(kappa >= 0.0f && kappa <= 64.0f) || !(hx < 60000.0f) || !(hy < 60000.0f)) {
+    hx = __int_as_float(0x7f800000);
+    hy = __int_as_float(0x7f800000);
+  }
+  const __half2 h = __halves2half2(__float2half_ru(hx), __float2half_ru(hy));
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ uint64_t sat_pack(uint64_t vis, uint64_t isect) {
+  if (vis > kDescCountMask) vis = kDescCountMask;
+  if (isect > kDescCountMask) isect = kDescCountMask;
+  return (vis << 31) | isect;
+}
+
+// Warp-cooperative decoupled look-back over virtual blocks [0, b): returns
+// the (visible, intersection) exclusive prefix.  Lane l inspects b-1-l-32k.
+__device__ __forceinline__ void project_lookback(uint64_t* desc, int64_t b, uint64_t* out_vis,
+                                                 uint64_t* out_isect, int32_t* status) {
+  const int lane = threadIdx.x & 31;
+  uint64_t vis = 0, isect = 0;
+  int64_t window_end = b;  // inspect [window_end-32, window_end)
+  uint32_t spins = 0;
+  while (window_end > 0) {
+    const int64_t j = window_end - 1 - lane;
+    uint64_t d = kDescInclusive;  // out-of-range lanes act as a zero inclusive
+    if (j >= 0) d = ld_acquire_u64(desc + j);
+    const uint32_t not_ready = __ballot_sync(0xffffffffu, (d >> 62) == 0);
+    if (not_ready) {
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicOr(status, kDeviceErrorLookback);
+        break;
+      }
+      continue;
+    }
+    const uint32_t inclusive = __ballot_sync(0xffffffffu, (d >> 62) == 2);
+    // Lanes up to and including the first inclusive descriptor contribute.
+    const int stop = inclusive ? (__ffs(inclusive) - 1) : 31;
+    uint64_t dv = 0, di = 0;
+    if (lane <= stop && j >= 0) {
+      dv = (d >> 31) & kDescCountMask;
+      di = d & kDescCountMask;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      dv += __shfl_xor_sync(0xffffffffu, dv, o);
+      di += __shfl_xor_sync(0xffffffffu, di, o);
+    }
+    vis += dv;
+    isect += di;
+    if (inclusive) break;
+    window_end -= 32;
+  }
+  *out_vis = vis;
+  *out_isect = isect;
+}
+
+template <int kShDegree>
+__global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectParams p) {
+  __shared__ Record s_rec[kProjectChunk];
+  __shared__ uint32_t s_rect_min[kProjectChunk];   // min_tx | min_ty << 16
+  __shared__ uint32_t s_rect_size[kProjectChunk];  // ntx | nty << 16
+  __shared__ uint32_t s_prefix[kProjectChunk + 1]; // exclusive isect prefix
+  __shared__ int32_t s_radii[kProjectChunk * 2];
+  __shared__ int64_t s_gid[kProjectChunk];
+  __shared__ uint32_t s_warp_vis[kProjectThreads / 32];
+  __shared__ uint64_t s_warp_isect[kProjectThreads / 32];
+  __shared__ CamConst s_cam;
+  __shared__ CamPlan s_plan;
+  __shared__ int64_t s_vblock;
+  __shared__ uint64_t s_base_vis, s_base_isect;
+  __shared__ uint32_t s_nvis;
+  __shared__ uint32_t s_nisect;
+
+  ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
+  const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
+  uint64_t* desc = reinterpret_cast<uint64_t*>(p.scratch + p.layout.project_desc);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+
+  // Clear the tile ranges of this frame (written later by the range kernel).
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; i < p.tile_count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    p.tile_starts[i] = 0;
+    p.tile_ends[i] = 0;
+  }
+
+  const int64_t total_vblocks = p.total_vblocks;
+  while (true) {
+    if (tid == 0) s_vblock = atomicAdd(&header->project_queue, 1u);
+    __syncthreads();
+    const int64_t b = s_vblock;
+    if (b >= total_vblocks) break;
+    const int64_t chunk = b / p.active_count;
+    const int64_t slot = b - chunk * p.active_count;
+    if (tid == 0) {
+      s_plan = plans[slot];
+    }
+    __syncthreads();
+    const CamPlan plan = s_plan;
+    const int64_t local_begin = chunk * kProjectChunk;
+    const bool live = plan.camera >= 0 && plan.scene_slot >= 0 && local_begin < plan.g_count;
+    if (live && tid == 0) {
+      const int cam = plan.camera;
+      make_cam_const(p.viewmats + cam * 16, p.env_xforms + cam * 16, p.intrinsics + cam * 9,
+                     plan.width, plan.height, &s_cam);
+    }
+    __syncthreads();
+
+    uint32_t block_vis = 0;
+    uint64_t block_isect = 0;
+    if (live) {
+      const float its = 1.0f / static_cast<float>(p.tile_size);
+#pragma unroll
+      for (int round = 0; round < kProjectRounds; ++round) {
+        const int64_t local = local_begin + round * kProjectThreads + tid;
+        Projected pr;
+        bool vis = false;
+        uint32_t rect_min = 0, rect_size = 0, ntiles = 0;
+        if (local < plan.g_count) {
+          vis = project_gaussian(p.means, p.covariances, p.opacities, plan.g_begin + local, s_cam,
+                                 p.near_plane, p.far_plane, p.support_sigma, p.cov_eps,
+                                 p.antialiased, &pr);
+          if (vis) {
+            const float frx = static_cast<float>(pr.radius_x);
+            const float fry = static_cast<float>(pr.radius_y);
+            const int min_tx = max(0, floor_clamped(fsub(fmul(pr.mean_x, its), fmul(frx, its))));
+            const int min_ty = max(0, floor_clamped(fsub(fmul(pr.mean_y, its), fmul(fry, its))));
+            const int max_tx =
+                min(plan.tiles_x, ceil_clamped(fadd(fmul(pr.mean_x, its), fmul(frx, its))));
+            const int max_ty =
+                min(plan.tiles_y, ceil_clamped(fadd(fmul(pr.mean_y, its), fmul(fry, its))));
+            const int ntx = max(0, max_tx - min_tx);
+            const int nty = max(0, max_ty - min_ty);
+            ntiles = static_cast<uint32_t>(ntx) * static_cast<uint32_t>(nty);
+            rect_min = static_cast<uint32_t>(min(min_tx, 65535)) |
+                       (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
+            rect_size = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
+          }
+        }
+        // Block scan of (visible, tiles) in task order.
+        uint32_t v_incl = vis ? 1u : 0u;
+        uint64_t t_incl = ntiles;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t nv = __shfl_up_sync(0xffffffffu, v_incl, o);
+          const uint64_t nt = __shfl_up_sync(0xffffffffu, t_incl, o);
+          if (lane >= o) {
+            v_incl += nv;
+            t_incl += nt;
+          }
+        }
+        if (lane == 31) {
+          s_warp_vis[warp] = v_incl;
+          s_warp_isect[warp] = t_incl;
+        }
+        __syncthreads();
+        uint32_t wv = 0;
+        uint64_t wt = 0;
+        for (int w = 0; w < warp; ++w) {
+          wv += s_warp_vis[w];
+          wt += s_warp_isect[w];
+        }
+        uint32_t rv = 0;
+        uint64_t rt = 0;
+        for (int w = 0; w < kProjectThreads / 32; ++w) {
+          rv += s_warp_vis[w];
+          rt += s_warp_isect[w];
+        }
+        if (vis) {
+          const uint32_t rank = block_vis + wv + v_incl - 1;
+          const uint64_t excl = block_isect + wt + t_incl - ntiles;
+          Record rec;
+          float rgb[3];
+          const int64_t g = plan.g_begin + local;
+          if (kShDegree < 0) {
+            rgb[0] = p.features[g * p.feature_width + 0];
+            rgb[1] = p.features[g * p.feature_width + 1];
+            rgb[2] = p.features[g * p.feature_width + 2];
+          } else {
+            eval_sh(kShDegree, p.features + g * p.feature_width, s_cam, pr.px, pr.py, pr.pz, rgb);
+          }
+          rec.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
+          rec.b = make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(static_cast<int>(g)));
+          rec.c = make_float4(rgb[0], rgb[1], rgb[2],
+                              __uint_as_float(footprint_box(pr.opacity, pr.cov_a, pr.cov_b,
+                                                            pr.cov_c)));
+          s_rec[rank] = rec;
+          s_rect_min[rank] = rect_min;
+          s_rect_size[rank] = rect_size;
+          s_prefix[rank] = static_cast<uint32_t>(excl > 0x7fffffffull ? 0x7fffffffull : excl);
+          s_radii[rank * 2 + 0] = pr.radius_x;
+          s_radii[rank * 2 + 1] = pr.radius_y;
+          s_gid[rank] = g;
+        }
+        block_vis += rv;
+        block_isect += rt;
+        __syncthreads();
+      }
+    }
+    if (tid == 0) {
+      s_nvis = block_vis;
+      s_prefix[block_vis] =
+          static_cast<uint32_t>(block_isect > 0x7fffffffull ? 0x7fffffffull : block_isect);
+      s_nisect = s_prefix[block_vis];
+    }
+
+    // Decoupled look-back for the global (visible, intersection) offsets.
+    if (warp == 0) {
+      const uint64_t agg = sat_pack(block_vis, block_isect);
+      if (b == 0) {
+        if (lane == 0) st_release_u64(desc + b, kDescInclusive | agg);
+        if (lane == 0) {
+          s_base_vis = 0;
+          s_base_isect = 0;
+        }
+      } else {
+        if (lane == 0) st_release_u64(desc + b, kDescAggregate | agg);
+        uint64_t pv = 0, pi = 0;
+        project_lookback(desc, b, &pv, &pi, &header->status);
+        if (lane == 0) {
+          st_release_u64(desc + b, kDescInclusive | sat_pack(pv + block_vis, pi + block_isect));
+          s_base_vis = pv;
+          s_base_isect = pi;
+        }
+      }
+      if (lane == 0 && b == total_vblocks - 1) {
+        // The last virtual block owns the frame totals.
+        const uint64_t tv = s_base_vis + block_vis;
+        const uint64_t ti = s_base_isect + block_isect;
+        p.counters[0] = static_cast<int64_t>(tv);
+        p.counters[1] = static_cast<int64_t>(ti);
+        const uint64_t vcap = static_cast<uint64_t>(p.visible_capacity);
+        const uint64_t icap = static_cast<uint64_t>(p.intersection_capacity);
+        p.counters[2] = tv > vcap ? static_cast<int64_t>(tv - vcap) : 0;
+        p.counters[3] = ti > icap ? static_cast<int64_t>(ti - icap) : 0;
+      }
+    }
+    __syncthreads();
+
+    const uint32_t nvis = s_nvis;
+    if (nvis > 0) {
+      const uint64_t base_vis = s_base_vis;
+      const uint64_t base_isect = s_base_isect;
+      const uint64_t vcap = static_cast<uint64_t>(p.visible_capacity);
+      const uint64_t icap = static_cast<uint64_t>(p.intersection_capacity);
+      // Records: coalesced float4 stream of the compacted block.
+      float4* dst = reinterpret_cast<float4*>(p.records);
+      const float4* src = reinterpret_cast<const float4*>(s_rec);
+      for (uint32_t i = tid; i < nvis * 3; i += kProjectThreads) {
+        const uint64_t r = base_vis + i / 3;
+        if (r < vcap) dst[r * 3 + (i % 3)] = src[i];
+      }
+      if (p.mirror_means2d) {
+        for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
+          const uint64_t r = base_vis + i;
+          if (r >= vcap) continue;
+          const Record rec = s_rec[i];
+          p.mirror_means2d[r * 2 + 0] = rec.a.x;
+          p.mirror_means2d[r * 2 + 1] = rec.a.y;
+          p.mirror_conics[r * 3 + 0] = rec.a.z;
+          p.mirror_conics[r * 3 + 1] = rec.a.w;
+          p.mirror_conics[r * 3 + 2] = rec.b.x;
+          p.mirror_depths[r] = rec.b.z;
+          p.mirror_opacities[r] = rec.b.y;
+          p.mirror_camera_ids[r] = plan.camera;
+          p.mirror_gaussian_ids[r] = static_cast<int32_t>(s_gid[i]);
+          p.mirror_radii[r * 2 + 0] = s_radii[i * 2 + 0];
+          p.mirror_radii[r * 2 + 1] = s_radii[i * 2 + 1];
+        }
+      }
+      // Tile intersections: one key per covered tile, cooperative over the
+      // block's prefix so consecutive threads store consecutive keys.
+      const uint32_t nisect = s_nisect;
+      uint64_t limit = 0;
+      if (base_isect < icap) {
+        const uint64_t room = icap - base_isect;
+        limit = room < nisect ? room : nisect;
+      }
+      const int64_t tiles_x = plan.tiles_x;
+      for (uint32_t j = tid; j < limit; j += kProjectThreads) {
+        // Owner record: last i with s_prefix[i] <= j.
+        uint32_t lo = 0, hi = nvis;  // invariant s_prefix[lo] <= j < s_prefix[hi]
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (s_prefix[mid] <= j) lo = mid; else hi = mid;
+        }
+        const uint32_t i = lo;
+        const uint32_t local = j - s_prefix[i];
+        const uint32_t ntx = s_rect_size[i] & 0xffffu;
+        const uint32_t ty = local / ntx;
+        const uint32_t tx = local - ty * ntx;
+        const uint32_t min_tx = s_rect_min[i] & 0xffffu;
+        const uint32_t min_ty = s_rect_min[i] >> 16;
+        const uint64_t r = base_vis + i;
+        uint64_t key = ~0ull;
+        int32_t value = 0;
+        if (r < vcap) {
+          const uint64_t tile = static_cast<uint64_t>(plan.tile_base) +
+                                static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
+          key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[i].b.z));
+          value = static_cast<int32_t>(r);
+        }
+        p.keys[base_isect + j] = key;
+        p.values[base_isect + j] = value;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template __global__ void project_emit_kernel<-1>(ProjectParams);
+template __global__ void project_emit_kernel<0>(ProjectParams);
+template __global__ void project_emit_kernel<1>(ProjectParams);
+template __global__ void project_emit_kernel<2>(ProjectParams);
+template __global__ void project_emit_kernel<3>(ProjectParams);
+
+}  // namespace vgr

@@ -1,0 +1,558 @@
+// C ABI of the camera path (declared in include/vgr_b200.h).
+//
+// Validation mirrors the TORCH_CHECKs of the reference binding
+// (src/isaacsim_gaussian_renderer/native/renderer.cpp:214-310 and
+// renderer_cuda.cu:2561-2730); violations return VGR_ERR_INVALID_ARGUMENT with
+// the reference's message text in vgr_last_error().
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/vgr_b200.h"
+#include "vgr_api_internal.h"
+#include "vgr_kernels.h"
+#include "vgr_misc.h"
+
+namespace {
+
+thread_local char g_last_error[1024] = "";
+std::atomic<int64_t> g_launch_count{0};
+
+struct OccupancyCache {
+  int device = -1;
+  int sms = 0;
+  int project_blocks = 0;
+  int sort_blocks = 0;
+};
+thread_local OccupancyCache g_occ;
+
+int bit_length(uint64_t v) {
+  int bits = 0;
+  while (v) {
+    ++bits;
+    v >>= 1;
+  }
+  return bits;
+}
+
+uint32_t float_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+}  // namespace
+
+namespace vgr {
+
+int fail(int code, const char* fmt, ...) {
+  va_list args;
+  va_start(args, fmt);
+  std::vsnprintf(g_last_error, sizeof(g_last_error), fmt, args);
+  va_end(args);
+  return code;
+}
+
+int check_launch(const char* what, int launches) {
+  g_launch_count.fetch_add(launches, std::memory_order_relaxed);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    return fail(VGR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+  }
+  return VGR_OK;
+}
+
+int device_sms(int* sms) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return fail(VGR_ERR_CUDA, "cudaGetDevice failed");
+  if (g_occ.device != device) {
+    g_occ = OccupancyCache{};
+    g_occ.device = device;
+    if (cudaDeviceGetAttribute(&g_occ.sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+      return fail(VGR_ERR_CUDA, "cudaDeviceGetAttribute(MultiProcessorCount) failed");
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3>,
+                                                  kProjectThreads, 0);
+    cudaFuncSetAttribute(sort_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kSortDynamicSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.sort_blocks, sort_onesweep_kernel,
+                                                  kSortThreads, kSortDynamicSmem);
+    if (g_occ.project_blocks < 1) g_occ.project_blocks = 1;
+    if (g_occ.sort_blocks < 1) g_occ.sort_blocks = 1;
+    cudaGetLastError();
+  }
+  *sms = g_occ.sms;
+  return VGR_OK;
+}
+
+int64_t render_vblocks(int64_t active, int64_t max_scene_gaussians) {
+  return active * ((max_scene_gaussians + kProjectChunk - 1) / kProjectChunk);
+}
+
+}  // namespace vgr
+
+using namespace vgr;
+
+extern "C" const char* vgr_version(void) { return "vgr_b200 0.1.0 sm_100a"; }
+
+extern "C" const char* vgr_last_error(void) { return g_last_error; }
+
+extern "C" int64_t vgr_kernel_launch_count(void) { return g_launch_count.load(); }
+
+extern "C" int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
+                                            int64_t max_projection_tasks, int64_t global_tiles,
+                                            int64_t max_active_cameras) {
+  if (intersection_capacity <= 0 || max_projection_tasks < 0 || global_tiles <= 0 ||
+      max_active_cameras < 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "scratch query needs positive capacity and tile count, non-negative bounds");
+  }
+  const int64_t vblocks = (max_projection_tasks + kProjectChunk - 1) / kProjectChunk +
+                          max_active_cameras;
+  return make_scratch_layout(intersection_capacity, max_active_cameras, vblocks).total;
+}
+
+// Scratch for a drop-in caller that only knows (items, segments): active
+// cameras are bounded by the tile count, projection tasks by 64 per item,
+// and the visible records (one per item at most) are carved from the end.
+static int64_t adapter_scratch_bytes(int64_t num_items, int64_t num_segments) {
+  if (num_items <= 0) return fail(VGR_ERR_INVALID_ARGUMENT, "num_items must be positive");
+  if (num_segments <= 0) return fail(VGR_ERR_INVALID_ARGUMENT, "num_segments must be positive");
+  if (num_items > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "The first renderer implementation supports at most INT_MAX intersections");
+  }
+  if (num_segments > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "The first renderer implementation supports at most INT_MAX tile segments");
+  }
+  const int64_t active = num_segments < (1 << 20) ? num_segments : (1 << 20);
+  const int64_t base = vgr_render_scratch_bytes(num_items, 64 * num_items, num_segments, active);
+  return align_up(base, 256) + num_items * VGR_RECORD_BYTES;
+}
+
+extern "C" int64_t vgr_sort_temp_bytes(int64_t num_items, int64_t num_segments) {
+  return adapter_scratch_bytes(num_items, num_segments);
+}
+
+extern "C" int64_t vgr_radix_sort_double_buffer_temp_bytes(int64_t num_items,
+                                                           int64_t num_segments) {
+  return adapter_scratch_bytes(num_items, num_segments);
+}
+
+extern "C" int vgr_precompute_covariances(const float* scales, const float* rotations,
+                                          int64_t gaussian_count, float* covariances,
+                                          void* stream) {
+  if (gaussian_count < 0) return fail(VGR_ERR_INVALID_ARGUMENT, "gaussian count must be >= 0");
+  if (gaussian_count == 0) return VGR_OK;
+  if (!scales || !rotations || !covariances) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "scales, rotations, and covariances must be non-null");
+  }
+  const int64_t blocks = (gaussian_count + 255) / 256;
+  if (blocks > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "covariance precompute grid exceeds CUDA limit");
+  precompute_covariances_kernel<<<static_cast<unsigned>(blocks), 256, 0,
+                                  static_cast<cudaStream_t>(stream)>>>(scales, rotations,
+                                                                       gaussian_count, covariances);
+  return check_launch("precompute_covariances");
+}
+
+extern "C" int vgr_prepare_chunked_active_ids(const int64_t* active_camera_ids,
+                                              int64_t active_count, int32_t* active_mask,
+                                              int64_t active_mask_capacity,
+                                              int64_t* chunk_active_ids, int64_t chunk_rows,
+                                              int64_t chunk_columns, int64_t logical_batch,
+                                              int64_t physical_batch, void* stream) {
+  if (logical_batch <= 0 || physical_batch <= 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "logical and physical batches must be positive");
+  }
+  const int64_t chunk_count = (logical_batch + physical_batch - 1) / physical_batch;
+  if (active_mask_capacity < logical_batch) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "active_mask is too small for the logical batch");
+  }
+  if (chunk_rows < chunk_count || chunk_columns < physical_batch) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "chunk_active_ids is too small for the chunk schedule");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(active_mask, 0, static_cast<size_t>(logical_batch) * sizeof(int32_t), s) !=
+      cudaSuccess) {
+    return check_launch("prepare_chunked_active_ids memset", 0);
+  }
+  if (active_count > 0) {
+    const int64_t blocks = (active_count + 255) / 256;
+    mark_active_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(active_camera_ids, active_count,
+                                                                     active_mask, logical_batch);
+  }
+  const int64_t slots = chunk_count * physical_batch;
+  build_chunk_ids_kernel<<<static_cast<unsigned>((slots + 255) / 256), 256, 0, s>>>(
+      active_mask, logical_batch, physical_batch, slots, chunk_columns, chunk_active_ids);
+  return check_launch("prepare_chunked_active_ids", active_count > 0 ? 2 : 1);
+}
+
+extern "C" int vgr_aggregate_chunk_counters(const int64_t* chunk_counters, int64_t chunk_rows,
+                                            int64_t chunk_stride, int64_t* counters,
+                                            int64_t* physical_capacity_counters,
+                                            int64_t chunk_count, void* stream) {
+  if (chunk_stride < 5) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "chunk counters must have shape [N, >=5] and outputs >=5");
+  }
+  if (chunk_count <= 0 || chunk_count > chunk_rows) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "chunk_count exceeds the counter workspace");
+  }
+  aggregate_counters_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      chunk_counters, chunk_stride, chunk_count, counters, physical_capacity_counters);
+  return check_launch("aggregate_chunk_counters");
+}
+
+extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
+                          const vgr_outputs* out, const vgr_workspace* ws,
+                          const vgr_render_options* opt, void* stream_ptr,
+                          int64_t* sorted_buffer_selector) {
+  if (!scene || !cams || !out || !ws || !opt || !sorted_buffer_selector) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "render arguments must be non-null");
+  }
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  const bool ragged = cams->widths != nullptr;
+  if (!ragged && (opt->height <= 0 || opt->width <= 0)) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "height and width must be positive");
+  }
+  if (opt->height > INT_MAX || opt->width > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "resolution exceeds int32 range");
+  }
+  if (scene->max_scene_gaussians <= 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "max_scene_gaussians must be positive");
+  }
+  if (scene->gaussian_count < 0 || scene->gaussian_count > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "packed Gaussian ids must fit int32");
+  }
+  if (scene->max_scene_gaussians > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "max_scene_gaussians exceeds the first implementation limit");
+  }
+  if (!(opt->near_plane > 0.0)) return fail(VGR_ERR_INVALID_ARGUMENT, "near_plane must be positive");
+  if (!(opt->far_plane > opt->near_plane)) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "far_plane must be greater than near_plane");
+  }
+  if (!(opt->gaussian_support_sigma > 0.0)) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "gaussian_support_sigma must be positive");
+  }
+  if (!std::isfinite(opt->covariance_epsilon) || opt->covariance_epsilon < 0.0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "covariance_epsilon must be finite and non-negative");
+  }
+  if (!std::isfinite(opt->semantic_min_alpha) || opt->semantic_min_alpha < 0.0 ||
+      opt->semantic_min_alpha > 1.0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "semantic_min_alpha must be finite and in [0, 1]");
+  }
+  const int ts = opt->tile_size;
+  if (ts <= 0 || ts > 16 || (ts & (ts - 1)) != 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "tile_size must be a power of two in [1, 16]");
+  }
+  if (ts < 4) {
+    return fail(VGR_ERR_UNSUPPORTED,
+                "tile_size=%d selects the dense per-pixel path, which this build does not provide; "
+                "use tile_size 4, 8 or 16",
+                ts);
+  }
+  if (opt->compact_projection_cache) {
+    return fail(VGR_ERR_UNSUPPORTED, "compact_projection_cache requires tile_size=1");
+  }
+  if (opt->ray_gaussian_evaluation) {
+    return fail(VGR_ERR_UNSUPPORTED,
+                "ray_gaussian_evaluation (exact-ray mode) is not provided by this build");
+  }
+  if (opt->antialiased && opt->ray_gaussian_evaluation) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "antialiased rasterization is incompatible with exact-ray evaluation");
+  }
+  if (opt->sh_degree < -1 || opt->sh_degree > 3) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "sh_degree must be -1 (linear RGB) or in [0, 3]");
+  }
+  const int64_t min_features =
+      opt->sh_degree < 0 ? 3 : static_cast<int64_t>((opt->sh_degree + 1) * (opt->sh_degree + 1) * 3);
+  if (scene->feature_width < min_features) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                opt->sh_degree < 0 ? "features must provide at least RGB channels"
+                                   : "features are too narrow for the requested SH degree");
+  }
+  if (!scene->means || !scene->covariances || !scene->opacities || !scene->features ||
+      !scene->semantic_ids || !scene->registered_scene_ids || !scene->scene_offsets) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "scene tensors must be non-null");
+  }
+  if (!cams->viewmats || !cams->intrinsics || !cams->env_xforms || !cams->camera_scene_ids) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "camera tensors must be non-null");
+  }
+  if (cams->batch < 0 || cams->batch > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "camera batch must be in [0, INT_MAX]");
+  }
+  const int64_t active = cams->active_camera_ids ? cams->active_count : cams->batch;
+  if (active < 0 || active > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "active camera count must be in [0, INT_MAX]");
+  }
+  if (!out->rgb || (opt->full_sensor_output && (!out->depth || !out->alpha || !out->semantic))) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "output tensors must be non-null");
+  }
+
+  int64_t tiles_per_image = 0;
+  int64_t global_tiles = 0;
+  int tiles_x = 0, tiles_y = 0;
+  if (ragged) {
+    if (!cams->heights || !cams->tile_offsets || !cams->pixel_offsets) {
+      return fail(VGR_ERR_INVALID_ARGUMENT,
+                  "the ragged form needs widths, heights, tile_offsets and pixel_offsets");
+    }
+    global_tiles = cams->total_tiles;
+    tiles_per_image = 0;
+  } else {
+    tiles_x = static_cast<int>((opt->width + ts - 1) / ts);
+    tiles_y = static_cast<int>((opt->height + ts - 1) / ts);
+    tiles_per_image = static_cast<int64_t>(tiles_x) * tiles_y;
+    global_tiles = cams->batch * tiles_per_image;
+    if (tiles_x > 65535 || tiles_y > 65535) {
+      return fail(VGR_ERR_INVALID_ARGUMENT, "at most 65535 tiles per image row or column");
+    }
+  }
+  if (global_tiles > UINT32_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "global tile count exceeds the uint32 key range");
+  }
+  if (global_tiles > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "device tile grouping supports at most INT_MAX tile segments");
+  }
+  if (ws->tile_capacity < global_tiles) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "tile range workspace is too small for the render batch");
+  }
+  if (ws->visible_capacity <= 0) return fail(VGR_ERR_INVALID_ARGUMENT, "visible capacity must be positive");
+  if (ws->visible_capacity > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "dense depth ordering requires visible capacity to fit int32");
+  }
+  if (ws->intersection_capacity <= 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "intersection capacity must be positive");
+  }
+  if (ws->intersection_capacity > INT_MAX) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "The first renderer implementation supports at most INT_MAX intersections");
+  }
+  if (!ws->records || !ws->keys_in || !ws->keys_out || !ws->values_in || !ws->values_out ||
+      !ws->tile_starts || !ws->tile_ends || !ws->counters || !ws->scratch) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "workspace tensors must be non-null");
+  }
+  if ((reinterpret_cast<uintptr_t>(ws->records) & 15) != 0 ||
+      (reinterpret_cast<uintptr_t>(ws->scratch) & 255) != 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "records must be 16-byte aligned and scratch 256-byte aligned");
+  }
+
+  const int64_t vblocks = render_vblocks(active, scene->max_scene_gaussians);
+  const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, vblocks);
+  if (ws->scratch_bytes < layout.total) {
+    return fail(VGR_ERR_SCRATCH_TOO_SMALL,
+                "render scratch holds %lld bytes but this batch needs %lld",
+                static_cast<long long>(ws->scratch_bytes), static_cast<long long>(layout.total));
+  }
+
+  const float near_f = static_cast<float>(opt->near_plane);
+  const float far_f = static_cast<float>(opt->far_plane);
+  SortKeyMap map;
+  map.near_bits = float_bits(near_f);
+  map.depth_bits = static_cast<uint32_t>(bit_length(float_bits(far_f) - map.near_bits));
+  map.tile_count = static_cast<uint32_t>(global_tiles);
+  const int tile_bits = global_tiles > 1 ? bit_length(static_cast<uint64_t>(global_tiles - 1)) : 0;
+  map.total_bits = map.depth_bits + static_cast<uint32_t>(tile_bits);
+  const int passes = static_cast<int>((map.total_bits + kRadixBits - 1) / kRadixBits);
+  if (passes > kMaxSortPasses || passes < 1) {
+    return fail(VGR_ERR_UNSUPPORTED, "sort key of %u bits exceeds the %d-pass limit",
+                map.total_bits, kMaxSortPasses);
+  }
+
+  int sms = 0;
+  int rc = device_sms(&sms);
+  if (rc != VGR_OK) return rc;
+
+  if (opt->stage_events && opt->stage_event_count != VGR_STAGE_EVENTS) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "stage_events needs exactly %d events", VGR_STAGE_EVENTS);
+  }
+  auto mark = [&](int i) {
+    if (opt->stage_events) cudaEventRecord(static_cast<cudaEvent_t>(opt->stage_events[i]), stream);
+  };
+  mark(0);
+  unsigned char* scratch = static_cast<unsigned char*>(ws->scratch);
+  const int32_t* sorted_values = opt->sorted_buffer_hint ? ws->values_out : ws->values_in;
+  int64_t selector = 1;
+
+  if (!opt->reuse_projection) {
+    if (cudaMemsetAsync(scratch + layout.project_desc, 0, static_cast<size_t>(vblocks) * 8, stream) !=
+        cudaSuccess) {
+      return check_launch("render: clear projection descriptors", 0);
+    }
+    SetupParams sp{};
+    sp.scratch = scratch;
+    sp.layout = layout;
+    sp.counters = ws->counters;
+    sp.reset_counters = 1;
+    sp.active_ids = cams->active_camera_ids;
+    sp.active_count = active;
+    sp.batch = cams->batch;
+    sp.camera_scene_ids = cams->camera_scene_ids;
+    sp.registered_scene_ids = scene->registered_scene_ids;
+    sp.scene_offsets = scene->scene_offsets;
+    sp.scene_count = static_cast<int>(scene->scene_count);
+    sp.widths = cams->widths;
+    sp.heights = cams->heights;
+    sp.tile_offsets = cams->tile_offsets;
+    sp.pixel_offsets = cams->pixel_offsets;
+    sp.width = static_cast<int>(opt->width);
+    sp.height = static_cast<int>(opt->height);
+    sp.tile_size = ts;
+    camera_setup_kernel<<<1, 1024, 0, stream>>>(sp);
+    if ((rc = check_launch("render: camera setup")) != VGR_OK) return rc;
+    mark(1);
+
+    ProjectParams pp{};
+    pp.scratch = scratch;
+    pp.layout = layout;
+    pp.means = scene->means;
+    pp.covariances = scene->covariances;
+    pp.opacities = scene->opacities;
+    pp.features = scene->features;
+    pp.feature_width = scene->feature_width;
+    pp.viewmats = cams->viewmats;
+    pp.intrinsics = cams->intrinsics;
+    pp.env_xforms = cams->env_xforms;
+    pp.active_count = active;
+    pp.total_vblocks = vblocks;
+    pp.near_plane = near_f;
+    pp.far_plane = far_f;
+    pp.support_sigma = static_cast<float>(opt->gaussian_support_sigma);
+    pp.cov_eps = static_cast<float>(opt->covariance_epsilon);
+    pp.antialiased = opt->antialiased != 0;
+    pp.tile_size = ts;
+    pp.records = ws->records;
+    pp.visible_capacity = ws->visible_capacity;
+    pp.keys = ws->keys_in;
+    pp.values = ws->values_in;
+    pp.intersection_capacity = ws->intersection_capacity;
+    pp.tile_starts = ws->tile_starts;
+    pp.tile_ends = ws->tile_ends;
+    pp.tile_count = global_tiles;
+    pp.counters = ws->counters;
+    pp.mirror_means2d = ws->visible_means2d;
+    pp.mirror_conics = ws->visible_conics;
+    pp.mirror_depths = ws->visible_depths;
+    pp.mirror_opacities = ws->visible_opacities;
+    pp.mirror_camera_ids = ws->visible_camera_ids;
+    pp.mirror_gaussian_ids = ws->visible_gaussian_ids;
+    pp.mirror_radii = ws->visible_radii;
+    if (pp.mirror_means2d && !(pp.mirror_conics && pp.mirror_depths && pp.mirror_opacities &&
+                               pp.mirror_camera_ids && pp.mirror_gaussian_ids && pp.mirror_radii)) {
+      return fail(VGR_ERR_INVALID_ARGUMENT, "the visible-record mirrors must be all set or all null");
+    }
+    int64_t pgrid = static_cast<int64_t>(sms) * g_occ.project_blocks;
+    if (pgrid > vblocks) pgrid = vblocks;
+    if (pgrid < 1) pgrid = 1;
+    switch (opt->sh_degree) {
+      case -1: project_emit_kernel<-1><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+      case 0: project_emit_kernel<0><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+      case 1: project_emit_kernel<1><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+      case 2: project_emit_kernel<2><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+      default: project_emit_kernel<3><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+    }
+    if ((rc = check_launch("render: projection")) != VGR_OK) return rc;
+    mark(2);
+
+    SortParams so{};
+    so.scratch = scratch;
+    so.layout = layout;
+    so.counters = ws->counters;
+    so.capacity = ws->intersection_capacity;
+    so.map = map;
+    so.passes = passes;
+    int64_t hgrid = static_cast<int64_t>(sms) * 4;
+    if (hgrid > layout.max_partitions) hgrid = layout.max_partitions;
+    if (hgrid < 1) hgrid = 1;
+    so.keys_in = ws->keys_in;
+    sort_histogram_kernel<<<static_cast<unsigned>(hgrid), kSortThreads, 0, stream>>>(so);
+    if ((rc = check_launch("render: sort histogram")) != VGR_OK) return rc;
+    mark(3);
+    int64_t sgrid = static_cast<int64_t>(sms) * g_occ.sort_blocks;
+    if (sgrid > layout.max_partitions) sgrid = layout.max_partitions;
+    if (sgrid < 1) sgrid = 1;
+    uint64_t* kin = ws->keys_in;
+    uint64_t* kout = ws->keys_out;
+    int32_t* vin = ws->values_in;
+    int32_t* vout = ws->values_out;
+    for (int pass = 0; pass < passes; ++pass) {
+      so.pass = pass;
+      so.keys_in = kin;
+      so.values_in = vin;
+      so.keys_out = kout;
+      so.values_out = vout;
+      sort_onesweep_kernel<<<static_cast<unsigned>(sgrid), kSortThreads, kSortDynamicSmem, stream>>>(
+          so);
+      if ((rc = check_launch("render: sort pass")) != VGR_OK) return rc;
+      uint64_t* tk = kin; kin = kout; kout = tk;
+      int32_t* tv = vin; vin = vout; vout = tv;
+    }
+    selector = passes & 1;
+    mark(4);
+    sorted_values = vin;
+
+    RangeParams rp{};
+    rp.counters = ws->counters;
+    rp.capacity = ws->intersection_capacity;
+    rp.keys = kin;
+    rp.tile_count = global_tiles;
+    rp.tile_starts = ws->tile_starts;
+    rp.tile_ends = ws->tile_ends;
+    rp.active_tiles = ws->counters + VGR_COUNTER_ACTIVE_TILES;
+    int64_t rgrid = (ws->intersection_capacity + 255) / 256;
+    if (rgrid > static_cast<int64_t>(sms) * 8) rgrid = static_cast<int64_t>(sms) * 8;
+    tile_ranges_kernel<<<static_cast<unsigned>(rgrid), 256, 0, stream>>>(rp);
+    if ((rc = check_launch("render: tile ranges")) != VGR_OK) return rc;
+    mark(5);
+  }
+
+  for (int i = 1; i <= 5; ++i) {
+    if (opt->reuse_projection) mark(i);
+  }
+  // Compositor over every tile of every active camera.
+  const int64_t max_items =
+      ragged ? active * cams->max_tiles_per_camera : active * tiles_per_image;
+  if (max_items > 0) {
+    if (max_items > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "raster grid exceeds CUDA limit");
+    CompositeParams cp{};
+    cp.scratch = scratch;
+    cp.layout = layout;
+    cp.active_count = active;
+    cp.tiles_per_camera_hint = ragged ? 0 : tiles_per_image;
+    cp.records = static_cast<const Record*>(ws->records);
+    cp.values = sorted_values;
+    cp.tile_starts = ws->tile_starts;
+    cp.tile_ends = ws->tile_ends;
+    cp.semantic_ids = scene->semantic_ids;
+    cp.semantic_min_alpha = static_cast<float>(opt->semantic_min_alpha);
+    cp.output_srgb = opt->output_srgb != 0;
+    cp.rgb = out->rgb;
+    cp.depth = out->depth;
+    cp.alpha = out->alpha;
+    cp.semantic = out->semantic;
+    const unsigned grid = static_cast<unsigned>(max_items);
+    const bool full = opt->full_sensor_output != 0;
+    if (ts == 16) {
+      if (full) composite_kernel<16, true><<<grid, 256, 0, stream>>>(cp);
+      else composite_kernel<16, false><<<grid, 256, 0, stream>>>(cp);
+    } else if (ts == 8) {
+      if (full) composite_kernel<8, true><<<grid, 64, 0, stream>>>(cp);
+      else composite_kernel<8, false><<<grid, 64, 0, stream>>>(cp);
+    } else {
+      if (full) composite_kernel<4, true><<<grid, 32, 0, stream>>>(cp);
+      else composite_kernel<4, false><<<grid, 32, 0, stream>>>(cp);
+    }
+    if ((rc = check_launch("render: compositor")) != VGR_OK) return rc;
+  }
+  mark(6);
+  *sorted_buffer_selector = selector;
+  return VGR_OK;
+}

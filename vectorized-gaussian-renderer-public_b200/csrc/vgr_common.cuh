@@ -1,0 +1,127 @@
+// Shared device helpers of the B200 renderer.
+//
+// Arithmetic contract: every floating-point operation whose result reaches a
+// tile ID, a key, a blend weight or an output pixel is written as an explicit
+// IEEE round-to-nearest intrinsic (__fmul_rn, __fadd_rn, __fsub_rn,
+// __fmaf_rn, __fdiv_rn, __fsqrt_rn).  The compiler can therefore neither
+// contract nor approximate it, and a C restatement that performs the same
+// operations in the same order (fmaf, *, +, /, sqrtf with contraction off)
+// reproduces every bit.  exp and log are evaluated by the polynomial methods
+// below (not CUDA's math library) for the same reason.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vgr {
+
+constexpr float kAlphaThreshold = 1.0f / 255.0f;   // renderer_cuda.cu:24
+constexpr float kMaxAlpha = 0.99f;                 // renderer_cuda.cu:25
+constexpr float kTransmittanceThreshold = 1.0e-4f; // renderer_cuda.cu:23
+constexpr float kMinAntialiasCompensation = 0.005f;// renderer_cuda.cu:26
+
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+
+// exp(x) for finite x in [-87, 88]: Cody-Waite reduction x = n ln2 + r with
+// n = rint(x log2 e), r carried as f = x log2(e) - n in two fma steps, and the
+// degree-7 Taylor polynomial of 2^f = e^(f ln 2) on |f| <= 0.5 (truncation
+// error < 5e-9 relative), scaled by 2^n through the exponent field.
+__device__ __forceinline__ float vexp(float x) {
+  const float kLog2eHi = 1.44269502162933349609375f;
+  const float kLog2eLo = 1.925963033500011079e-8f;
+  const float t = fmul(x, kLog2eHi);
+  const float n = rintf(t);
+  float f = ffma(x, kLog2eHi, -n);
+  f = ffma(x, kLog2eLo, f);
+  // c_k = (ln 2)^k / k!
+  float p = 1.525273380405984e-05f;            // k = 7
+  p = ffma(p, f, 1.540353039338161e-04f);      // k = 6
+  p = ffma(p, f, 1.333355814642844e-03f);      // k = 5
+  p = ffma(p, f, 9.618129107628477e-03f);      // k = 4
+  p = ffma(p, f, 5.550410866482158e-02f);      // k = 3
+  p = ffma(p, f, 2.402265069591007e-01f);      // k = 2
+  p = ffma(p, f, 6.931471805599453e-01f);      // k = 1
+  p = ffma(p, f, 1.0f);                        // k = 0
+  const int e = static_cast<int>(n);
+  return fmul(p, __int_as_float((e + 127) << 23));
+}
+
+// ln(y) for positive normal finite y: y = m 2^e with m in [sqrt(1/2), sqrt(2)),
+// ln m = 2 atanh(s), s = (m-1)/(m+1), atanh by its odd series through s^11
+// (|s| <= 0.1716, truncation < 1e-10 relative), ln 2 split in two parts.
+__device__ __forceinline__ float vlog(float y) {
+  const int bits = __float_as_int(y);
+  int e = ((bits >> 23) & 0xff) - 127;
+  float m = __int_as_float((bits & 0x007fffff) | 0x3f800000);
+  if (m > 1.41421353816986083984375f) {
+    m = fmul(m, 0.5f);
+    e += 1;
+  }
+  const float s = fdiv(fsub(m, 1.0f), fadd(m, 1.0f));
+  const float s2 = fmul(s, s);
+  float p = 0.0909090909090909f;               // 1/11
+  p = ffma(p, s2, 0.1111111111111111f);        // 1/9
+  p = ffma(p, s2, 0.1428571428571428f);        // 1/7
+  p = ffma(p, s2, 0.2f);                       // 1/5
+  p = ffma(p, s2, 0.3333333333333333f);        // 1/3
+  p = ffma(p, s2, 1.0f);
+  const float lnm = fmul(fmul(2.0f, s), p);
+  const float fe = static_cast<float>(e);
+  const float kLn2Hi = 0.693145751953125f;
+  const float kLn2Lo = 1.428606765330187e-06f;
+  return ffma(fe, kLn2Hi, ffma(fe, kLn2Lo, lnm));
+}
+
+// sRGB transfer (renderer_cuda.cu:161-166) with pow(v, 1/2.4) as
+// vexp(vlog(v) / 2.4).
+__device__ __forceinline__ float linear_to_srgb(float v) {
+  v = fminf(fmaxf(v, 0.0f), 1.0f);
+  if (v <= 0.0031308f) {
+    return fmul(12.92f, v);
+  }
+  const float p = vexp(fmul(vlog(v), 0.4166666666666667f));
+  return fsub(fmul(1.055f, p), 0.055f);
+}
+
+// Float -> int conversions with explicit saturation, so the C restatement
+// (which has no saturating conversion) agrees for out-of-range values.
+__device__ __forceinline__ int ceil_radius(float x) {
+  return x > 0.0f ? static_cast<int>(fminf(ceilf(x), 2147483520.0f)) : 0;
+}
+__device__ __forceinline__ int floor_clamped(float x) {
+  // NaN compares false and maps to 0.
+  if (!(x == x)) return 0;
+  return static_cast<int>(floorf(fminf(fmaxf(x, -1073741824.0f), 1073741824.0f)));
+}
+__device__ __forceinline__ int ceil_clamped(float x) {
+  if (!(x == x)) return 0;
+  return static_cast<int>(ceilf(fminf(fmaxf(x, -1073741824.0f), 1073741824.0f)));
+}
+
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Bounded spin budget for decoupled look-back waits.  A wait that runs out
+// records VGR_DEVICE_ERROR_LOOKBACK in the device status word and the kernel
+// continues with a clamped result (outputs are then invalid but no access
+// leaves its buffer).
+constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr int kDeviceErrorLookback = 1;
+
+}  // namespace vgr

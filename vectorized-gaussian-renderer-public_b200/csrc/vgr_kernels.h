@@ -1,0 +1,119 @@
+// Kernel parameter blocks and kernel declarations of the camera path.
+#pragma once
+
+#include <stdint.h>
+
+#include "vgr_camera.cuh"
+
+namespace vgr {
+
+struct SetupParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  int64_t* counters;
+  int reset_counters;
+  const int64_t* active_ids;
+  int64_t active_count;
+  int64_t batch;
+  const int64_t* camera_scene_ids;
+  const int64_t* registered_scene_ids;
+  const int64_t* scene_offsets;
+  int scene_count;
+  const int32_t* widths;
+  const int32_t* heights;
+  const int64_t* tile_offsets;
+  const int64_t* pixel_offsets;
+  int width;
+  int height;
+  int tile_size;
+};
+
+struct ProjectParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  const float* means;
+  const float* covariances;
+  const float* opacities;
+  const float* features;
+  int64_t feature_width;
+  const float* viewmats;
+  const float* intrinsics;
+  const float* env_xforms;
+  int64_t active_count;
+  int64_t total_vblocks;
+  float near_plane;
+  float far_plane;
+  float support_sigma;
+  float cov_eps;
+  bool antialiased;
+  int tile_size;
+  void* records;
+  int64_t visible_capacity;
+  uint64_t* keys;
+  int32_t* values;
+  int64_t intersection_capacity;
+  int32_t* tile_starts;
+  int32_t* tile_ends;
+  int64_t tile_count;
+  int64_t* counters;
+  float* mirror_means2d;
+  float* mirror_conics;
+  float* mirror_depths;
+  float* mirror_opacities;
+  int32_t* mirror_camera_ids;
+  int32_t* mirror_gaussian_ids;
+  int32_t* mirror_radii;
+};
+
+struct SortParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  const int64_t* counters;     // counters[1] = emitted keys
+  int64_t capacity;
+  SortKeyMap map;
+  int passes;
+  int pass;
+  const uint64_t* keys_in;
+  const int32_t* values_in;
+  uint64_t* keys_out;
+  int32_t* values_out;
+};
+
+struct RangeParams {
+  const int64_t* counters;
+  int64_t capacity;
+  const uint64_t* keys;
+  int64_t tile_count;
+  int32_t* tile_starts;
+  int32_t* tile_ends;
+  int64_t* active_tiles;
+};
+
+struct CompositeParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  int64_t active_count;
+  int64_t tiles_per_camera_hint;  // >0 when every camera has this many tiles
+  const Record* records;
+  const int32_t* values;
+  const int32_t* tile_starts;
+  const int32_t* tile_ends;
+  const int64_t* semantic_ids;
+  float semantic_min_alpha;
+  bool output_srgb;
+  float* rgb;
+  float* depth;
+  float* alpha;
+  int64_t* semantic;
+};
+
+__global__ void camera_setup_kernel(SetupParams p);
+template <int kShDegree>
+__global__ void project_emit_kernel(ProjectParams p);
+__global__ void sort_histogram_kernel(SortParams p);
+__global__ void sort_onesweep_kernel(SortParams p);
+__global__ void tile_ranges_kernel(RangeParams p);
+template <int kTile, bool kFull>
+__global__ void composite_kernel(CompositeParams p);
+
+}  // namespace vgr

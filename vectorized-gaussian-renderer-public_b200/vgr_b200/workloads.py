@@ -1,0 +1,164 @@
+"""Seeded synthetic scenes and camera rigs of the benchmark workloads.
+
+No public dataset is used by the benchmark: scenes and cameras are drawn from
+the stated distributions with a CPU torch.Generator, so the CUDA path and the
+CPU oracle see bit-identical inputs.
+
+Workloads (all float32):
+  plain-10k-256   10,000 Gaussians, means U[-1,1]^3, log-scales N(-4,0.5),
+                  quaternions normalised N(0,I4) (WXYZ), opacity
+                  sigmoid(N(0,1)), RGB U[0,1], semantic U{0..15}; one pinhole
+                  256x256 camera, fx=fy=256, cx=cy=128, at (0,0,-3) looking at
+                  the origin.
+  batched-1m-sh3  1,000,000 Gaussians with means U[-5,5]^3 and degree-3
+                  spherical harmonics (48 coefficients: DC from U[0,1] colour,
+                  the rest N(0,0.2)); 64 pinhole 640x480 cameras, fx=fy=525,
+                  on a radius-8 orbit at height 1.5 with +-5 deg yaw jitter,
+                  all looking at the origin.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import torch
+
+SH_C0 = 0.28209479177387814
+
+
+@dataclass
+class SceneTensors:
+    means: torch.Tensor
+    scales: torch.Tensor
+    rotations: torch.Tensor
+    opacities: torch.Tensor
+    features: torch.Tensor
+    semantic_ids: torch.Tensor
+
+    def to(self, device: torch.device | str) -> "SceneTensors":
+        return SceneTensors(
+            **{name: getattr(self, name).to(device).contiguous() for name in self.__dataclass_fields__}
+        )
+
+    def as_kwargs(self) -> dict[str, torch.Tensor]:
+        return {name: getattr(self, name) for name in self.__dataclass_fields__}
+
+
+@dataclass
+class CameraRig:
+    viewmats: torch.Tensor  # [B,4,4] world -> OpenCV camera
+    intrinsics: torch.Tensor  # [B,3,3]
+    height: int
+    width: int
+
+    def to(self, device: torch.device | str) -> "CameraRig":
+        return CameraRig(
+            self.viewmats.to(device).contiguous(),
+            self.intrinsics.to(device).contiguous(),
+            self.height,
+            self.width,
+        )
+
+
+def synthetic_scene(
+    count: int,
+    *,
+    seed: int,
+    mean_half_extent: float = 1.0,
+    log_scale_mean: float = -4.0,
+    log_scale_std: float = 0.5,
+    sh_degree: int | None = None,
+    semantic_classes: int = 16,
+) -> SceneTensors:
+    """Scene drawn with a CPU generator (see module docstring for the laws)."""
+    gen = torch.Generator().manual_seed(seed)
+    means = (torch.rand((count, 3), generator=gen) * 2.0 - 1.0) * mean_half_extent
+    scales = torch.exp(torch.randn((count, 3), generator=gen) * log_scale_std + log_scale_mean)
+    quats = torch.randn((count, 4), generator=gen)
+    quats = quats / quats.norm(dim=1, keepdim=True).clamp_min(1e-12)
+    opacities = torch.sigmoid(torch.randn((count,), generator=gen))
+    rgb = torch.rand((count, 3), generator=gen)
+    if sh_degree is None:
+        features = rgb
+    else:
+        k = (sh_degree + 1) ** 2
+        coeffs = torch.randn((count, k, 3), generator=gen) * 0.2
+        coeffs[:, 0, :] = (rgb - 0.5) / SH_C0
+        features = coeffs.reshape(count, k * 3)
+    semantic_ids = torch.randint(0, semantic_classes, (count,), generator=gen, dtype=torch.int32)
+    return SceneTensors(
+        means=means.float().contiguous(),
+        scales=scales.float().contiguous(),
+        rotations=quats.float().contiguous(),
+        opacities=opacities.float().contiguous(),
+        features=features.float().contiguous(),
+        semantic_ids=semantic_ids.to(torch.int64).contiguous(),
+    )
+
+
+def look_at_viewmats(eyes: torch.Tensor, targets: torch.Tensor, up=(0.0, 1.0, 0.0)) -> torch.Tensor:
+    """OpenCV world->camera matrices (x right, y down, z forward), float64 math."""
+    eyes = eyes.double()
+    targets = targets.double()
+    up_t = torch.tensor(up, dtype=torch.float64).expand_as(eyes)
+    z = targets - eyes
+    z = z / z.norm(dim=1, keepdim=True)
+    y_hint = -up_t
+    x = torch.linalg.cross(y_hint, z, dim=1)
+    x = x / x.norm(dim=1, keepdim=True)
+    y = torch.linalg.cross(z, x, dim=1)
+    rot = torch.stack((x, y, z), dim=1)
+    trans = -(rot @ eyes.unsqueeze(-1)).squeeze(-1)
+    view = torch.zeros((eyes.shape[0], 4, 4), dtype=torch.float64)
+    view[:, :3, :3] = rot
+    view[:, :3, 3] = trans
+    view[:, 3, 3] = 1.0
+    return view.float().contiguous()
+
+
+def pinhole(batch: int, fx: float, fy: float, cx: float, cy: float) -> torch.Tensor:
+    k = torch.zeros((batch, 3, 3), dtype=torch.float32)
+    k[:, 0, 0] = fx
+    k[:, 1, 1] = fy
+    k[:, 0, 2] = cx
+    k[:, 1, 2] = cy
+    k[:, 2, 2] = 1.0
+    return k
+
+
+def plain_camera(height: int = 256, width: int = 256, focal: float = 256.0, distance: float = 3.0) -> CameraRig:
+    eyes = torch.tensor([[0.0, 0.0, -distance]])
+    view = look_at_viewmats(eyes, torch.zeros((1, 3)))
+    return CameraRig(view, pinhole(1, focal, focal, width / 2.0, height / 2.0), height, width)
+
+
+def orbit_cameras(
+    count: int,
+    *,
+    seed: int,
+    radius: float = 8.0,
+    height_offset: float = 1.5,
+    yaw_jitter_deg: float = 5.0,
+    width: int = 640,
+    height: int = 480,
+    focal: float = 525.0,
+) -> CameraRig:
+    gen = torch.Generator().manual_seed(seed)
+    base = torch.arange(count, dtype=torch.float64) * (2.0 * math.pi / count)
+    jitter = (torch.rand((count,), generator=gen, dtype=torch.float64) * 2.0 - 1.0) * math.radians(yaw_jitter_deg)
+    yaw = base + jitter
+    eyes = torch.stack((radius * torch.cos(yaw), torch.full_like(yaw, height_offset), radius * torch.sin(yaw)), dim=1)
+    view = look_at_viewmats(eyes, torch.zeros((count, 3), dtype=torch.float64))
+    return CameraRig(view, pinhole(count, focal, focal, width / 2.0, height / 2.0), height, width)
+
+
+def plain_workload() -> tuple[SceneTensors, CameraRig]:
+    """Plain single-camera forward render: 10k Gaussians, 256x256."""
+    return synthetic_scene(10_000, seed=0), plain_camera()
+
+
+def batched_workload(gaussians: int = 1_000_000, cameras: int = 64) -> tuple[SceneTensors, CameraRig]:
+    """Batched forward render: 1M Gaussians SH degree 3, 64 cameras 640x480."""
+    scene = synthetic_scene(gaussians, seed=1, mean_half_extent=5.0, sh_degree=3)
+    return scene, orbit_cameras(cameras, seed=2)
