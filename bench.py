@@ -65,23 +65,26 @@ def parse_args() -> argparse.Namespace:
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
     parser.add_argument("--workload", choices=("batched-1m-sh3", "plain-10k-256"), default="batched-1m-sh3")
     parser.add_argument("--cpu-sample-cameras", type=int, default=2)
+    parser.add_argument("--cameras", type=int, default=None,
+                        help="override the camera count (small profiling captures)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
     return parser.parse_args()
 
 
 # --------------------------------------------------------------------------- workloads
-def make_workload(name: str, rank: int):
+def make_workload(name: str, rank: int, cameras: int | None = None):
     from vgr_b200 import workloads
 
     if name == "plain-10k-256":
         scene, rig = workloads.plain_workload()
         return scene, rig, None, {"workload": name, "gaussians": 10_000, "cameras": 1,
                                   "height": 256, "width": 256, "tile_size": 16, "color": "rgb"}
-    scene, rig = workloads.batched_workload()
+    count = cameras or 64
+    scene, rig = workloads.batched_workload(cameras=count)
     if rank:
-        rig = workloads.orbit_cameras(64, seed=2 + rank)
-    return scene, rig, 3, {"workload": name, "gaussians": 1_000_000, "cameras": 64,
+        rig = workloads.orbit_cameras(count, seed=2 + rank)
+    return scene, rig, 3, {"workload": name, "gaussians": 1_000_000, "cameras": count,
                            "height": 480, "width": 640, "tile_size": 16, "color": "sh3"}
 
 
@@ -232,7 +235,7 @@ def run_reference(args) -> None:
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    scene, rig, sh_degree, config = make_workload(args.workload, 0)
+    scene, rig, sh_degree, config = make_workload(args.workload, 0, args.cameras)
     sample = list(range(min(args.cpu_sample_cameras, rig.viewmats.shape[0])))
     for _ in range(max(args.warmup, 0) and 1):
         time_cpu(scene, rig, sh_degree, sample[:1], 1)
@@ -298,7 +301,7 @@ def run_b200(args) -> None:
 
     from vgr_b200 import CustomCudaBackend, RendererService, _native
 
-    scene, rig, sh_degree, config = make_workload(args.workload, rank)
+    scene, rig, sh_degree, config = make_workload(args.workload, rank, args.cameras)
     batch = rig.viewmats.shape[0]
     backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=config["tile_size"])
     service = RendererService(backend, height=rig.height, width=rig.width, max_views=batch)

@@ -14,7 +14,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 PKG_ROOT = ROOT / "vectorized-gaussian-renderer-public_b200"
-for path in (str(PKG_ROOT), str(ROOT)):
+for path in (str(ROOT / "tests"), str(PKG_ROOT), str(ROOT)):
     if path not in sys.path:
         sys.path.insert(0, path)
 

@@ -1,0 +1,58 @@
+"""Seeded camera cases shared by the golden generator and the golden tests.
+
+Each case builds its scenes and cameras from fixed seeds on the CPU, so the
+fixtures only need to store outputs.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from vgr_b200.workloads import (
+    CameraRig,
+    orbit_cameras,
+    pinhole,
+    plain_workload,
+    synthetic_scene,
+)
+
+
+def _plain():
+    scene, rig = plain_workload()
+    return [(0, scene)], rig, [0]
+
+
+def _batch4():
+    scene = synthetic_scene(20_000, seed=5, mean_half_extent=1.5, log_scale_mean=-3.5)
+    rig = orbit_cameras(4, seed=3, radius=4.0, height_offset=0.8, width=96, height=80, focal=90.0)
+    return [(7, scene)], rig, [7, 7, 7, 7]
+
+
+def _ties():
+    count = 256
+    scene = synthetic_scene(count, seed=0)
+    scene.means.zero_()
+    scene.means[:, 2] = 5.0
+    scene.scales.fill_(0.03)
+    scene.rotations.zero_()
+    scene.rotations[:, 0] = 1.0
+    scene.opacities.fill_(0.2)
+    scene.features.zero_()
+    scene.features[:, 0] = torch.linspace(1.0, 0.0, count)
+    scene.features[:, 2] = torch.linspace(0.0, 1.0, count)
+    scene.semantic_ids.copy_(torch.arange(1000, 1000 + count))
+    view = torch.eye(4).repeat(2, 1, 1)
+    view[:, 2, 3] = -4.0
+    rig = CameraRig(view.contiguous(), pinhole(2, 64.0, 64.0, 32.0, 32.0), 64, 64)
+    return [(73, scene)], rig, [73, 73]
+
+
+CASES = {
+    "plain_deterministic": {"build": _plain, "options": {"deterministic": True}},
+    "plain_global_radix": {"build": _plain, "options": {"deterministic": False}},
+    "batch4_antialiased_srgb": {
+        "build": _batch4,
+        "options": {"deterministic": True, "rasterize_mode": "antialiased", "output_srgb": True},
+    },
+    "ties": {"build": _ties, "options": {"deterministic": True, "gaussian_support_sigma": 3.0}},
+}
