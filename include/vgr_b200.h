@@ -212,6 +212,28 @@ int vgr_render(const vgr_scene* scene, const vgr_cameras* cameras,
                const vgr_render_options* options, void* stream,
                int64_t* sorted_buffer_selector);
 
+/* Size of the library-owned device array used by vgr_render_static_scratch. */
+#define VGR_STATIC_SCRATCH_BYTES (16ll << 20)
+
+/* vgr_render for callers that must not allocate device memory on their
+ * render path (a plug-in whose host owns every device allocation through its
+ * own pool, a real-time loop that cannot afford allocator latency, code being
+ * recorded into a CUDA graph).  It has no counterpart in the reference.  The
+ * caller passes inputs, outputs and the record/key/value/range/counter
+ * workspace exactly as for vgr_render; workspace->scratch and scratch_bytes
+ * are ignored and a VGR_STATIC_SCRATCH_BYTES array inside the library is used
+ * instead (every GPU that loads the library keeps it until exit).  Renders
+ * that need more scratch than that (about four million tile intersections)
+ * fail with VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
+ * the array: calls ordered on one stream are fine, calls that overlap on the
+ * GPU race.  The first call on a device looks the array's address up while
+ * that device is current; make it before any stream capture. */
+int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras,
+                              const vgr_outputs* outputs,
+                              const vgr_workspace* workspace,
+                              const vgr_render_options* options, void* stream,
+                              int64_t* sorted_buffer_selector);
+
 #ifdef __cplusplus
 }
 #endif

@@ -147,6 +147,19 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
             ctypes.POINTER(_c_i64),
         ],
     ),
+    (
+        "vgr_render_static_scratch",
+        ctypes.c_int,
+        [
+            ctypes.POINTER(VgrScene),
+            ctypes.POINTER(VgrCameras),
+            ctypes.POINTER(VgrOutputs),
+            ctypes.POINTER(VgrWorkspace),
+            ctypes.POINTER(VgrRenderOptions),
+            _c_p,
+            ctypes.POINTER(_c_i64),
+        ],
+    ),
 ]
 
 _LIB: ctypes.CDLL | None = None
