@@ -8,12 +8,14 @@
 // depth = sum(w z) / alpha (or +inf), semantic = label of the largest single
 // w (the earliest wins ties) or -1 when alpha < semantic_min_alpha.
 //
-// B200 structure: one CTA per (camera, tile); records are staged in batches
-// of 256 through shared memory together with an 8-bit mask of the warps whose
-// 8x4 pixel block the record's conservative alpha footprint touches.  Each
-// warp walks only its own records with __ballot_sync over the masks, skips
-// exp for pixels beyond a per-record quadratic-form bound, and retires as a
-// unit once all of its pixels have terminated; the CTA stops staging when
+// B200 structure: one CTA per (camera, tile); each thread owns two pixels of
+// one column (rows y and y + kLaneRows) so the per-record work shared by the
+// pair (shared-memory loads, dx, a*dx*dx, 2b*dx, loop control) is paid once.
+// Records are staged in batches of 256 through shared memory together with a
+// mask of the warps whose 8x8-pixel block the record's conservative alpha
+// footprint touches; each warp walks only its records with __ballot_sync
+// over the masks, skips exp beyond a per-record quadratic-form bound, and
+// retires once all of its pixels have terminated; the CTA stops staging when
 // __syncthreads_count reports no live pixel.
 #include "vgr_kernels.h"
 
@@ -21,9 +23,10 @@ namespace vgr {
 
 template <int kTile>
 struct CompositeGeometry {
-  static constexpr int kPixels = kTile * kTile;
-  static constexpr int kBlockW = kTile < 8 ? kTile : 8;          // warp sub-block width
-  static constexpr int kBlockH = (32 / kBlockW) < kTile ? (32 / kBlockW) : kTile;
+  static constexpr int kBlockW = kTile < 8 ? kTile : 8;  // warp block width (px)
+  static constexpr int kLaneRows =
+      (32 / kBlockW) < (kTile / 2) ? (32 / kBlockW) : (kTile / 2);  // lane rows
+  static constexpr int kBlockH = 2 * kLaneRows;  // warp block height (px)
   static constexpr int kWarpsX = kTile / kBlockW;
   static constexpr int kWarpsY = kTile / kBlockH;
   static constexpr int kWarps = kWarpsX * kWarpsY;
@@ -32,14 +35,72 @@ struct CompositeGeometry {
 
 constexpr int kCompositeBatch = 256;
 
+struct PixelState {
+  float transmittance;
+  float r, g, b, depth;
+  float best_weight;
+  int64_t best_semantic;
+  bool done;
+};
+
+template <bool kFull>
+__device__ __forceinline__ void blend(PixelState& s, float q, float qmax, int j,
+                                      const float4* s_cqo, const float4* s_col,
+                                      const int64_t* s_sem) {
+  if (s.done || !(q <= qmax)) return;
+  const float power = fmul(-0.5f, q);
+  if (power > 0.0f || power < -20.0f) return;
+  const float4 cqo = s_cqo[j];
+  const float alpha = fminf(kMaxAlpha, fmul(cqo.z, vexp(power)));
+  if (!(alpha >= kAlphaThreshold)) return;
+  const float next_t = fmul(s.transmittance, fsub(1.0f, alpha));
+  if (next_t <= kTransmittanceThreshold) {
+    s.done = true;
+    return;
+  }
+  const float w = fmul(s.transmittance, alpha);
+  const float4 col = s_col[j];
+  s.r = ffma(w, col.x, s.r);
+  s.g = ffma(w, col.y, s.g);
+  s.b = ffma(w, col.z, s.b);
+  if (kFull) {
+    s.depth = ffma(w, col.w, s.depth);
+    if (w > s.best_weight) {
+      s.best_weight = w;
+      s.best_semantic = s_sem[j];
+    }
+  }
+  s.transmittance = next_t;
+}
+
+template <bool kFull>
+__device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamPlan& plan, int x,
+                                            int y, PixelState& s) {
+  const int64_t pixel = plan.pixel_base + static_cast<int64_t>(y) * plan.width + x;
+  const float out_alpha = fsub(1.0f, s.transmittance);
+  if (p.output_srgb) {
+    s.r = linear_to_srgb(s.r);
+    s.g = linear_to_srgb(s.g);
+    s.b = linear_to_srgb(s.b);
+  }
+  p.rgb[pixel * 3 + 0] = s.r;
+  p.rgb[pixel * 3 + 1] = s.g;
+  p.rgb[pixel * 3 + 2] = s.b;
+  if (kFull) {
+    p.alpha[pixel] = out_alpha;
+    p.depth[pixel] = out_alpha > 1.0e-8f ? fdiv(s.depth, out_alpha) : __int_as_float(0x7f800000);
+    p.semantic[pixel] =
+        (s.best_weight >= 0.0f && out_alpha >= p.semantic_min_alpha) ? s.best_semantic : -1;
+  }
+}
+
 template <int kTile, bool kFull>
 __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
     composite_kernel(CompositeParams p) {
   using Geo = CompositeGeometry<kTile>;
-  __shared__ float4 s_a[kCompositeBatch];
-  __shared__ float4 s_b[kCompositeBatch];
-  __shared__ float4 s_c[kCompositeBatch];
-  __shared__ float s_qmax[kCompositeBatch];
+  __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, conic_xx, 2*conic_xy
+  __shared__ float4 s_cqo[kCompositeBatch];  // conic_yy, q bound, opacity, -
+  __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
   __shared__ uint32_t s_mask[kCompositeBatch];
   __shared__ int64_t s_sem[kFull ? kCompositeBatch : 1];
 
@@ -53,7 +114,6 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
   if (item >= total) return;
   int64_t lo = 0, hi = p.active_count;  // tile_prefix[lo] <= item < tile_prefix[hi]
   {
-    // Uniform batches: direct guess first.
     const int64_t tpi = p.tiles_per_camera_hint;
     if (tpi > 0) {
       const int64_t guess = item / tpi;
@@ -80,18 +140,19 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
   const int warp_y = warp / Geo::kWarpsX;
   const int lx = lane % Geo::kBlockW;
   const int ly = lane / Geo::kBlockW;
+  const bool lane_used = ly < Geo::kLaneRows;
   const int pixel_x = tile_x * kTile + warp_x * Geo::kBlockW + lx;
-  const int pixel_y = tile_y * kTile + warp_y * Geo::kBlockH + ly;
-  const bool valid = ly < Geo::kBlockH && pixel_x < plan.width && pixel_y < plan.height;
+  const int pixel_y0 = tile_y * kTile + warp_y * Geo::kBlockH + ly;
+  const int pixel_y1 = pixel_y0 + Geo::kLaneRows;
+  const bool valid0 = lane_used && pixel_x < plan.width && pixel_y0 < plan.height;
+  const bool valid1 = lane_used && pixel_x < plan.width && pixel_y1 < plan.height;
   const float cx = fadd(static_cast<float>(pixel_x), 0.5f);
-  const float cy = fadd(static_cast<float>(pixel_y), 0.5f);
+  const float cy0 = fadd(static_cast<float>(pixel_y0), 0.5f);
+  const float cy1 = fadd(static_cast<float>(pixel_y1), 0.5f);
 
-  float transmittance = 1.0f;
-  float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, acc_depth = 0.0f;
-  float best_weight = -1.0f;
-  int64_t best_semantic = -1;
-  bool done = !valid;
-  bool warp_done = __all_sync(0xffffffffu, done);
+  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, -1, !valid0};
+  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, -1, !valid1};
+  bool warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
 
   const int64_t range_start = p.tile_starts[global_tile];
   const int64_t range_end = p.tile_ends[global_tile];
@@ -104,12 +165,12 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
       for (int j = tid; j < n; j += Geo::kThreads) {
         const int32_t v = p.values[chunk + j];
         const Record rec = p.records[v];
-        s_a[j] = rec.a;
-        s_b[j] = rec.b;
-        s_c[j] = rec.c;
-        if (kFull) s_sem[j] = p.semantic_ids[__float_as_int(rec.b.w)];
+        s_geo[j] = make_float4(rec.a.x, rec.a.y, rec.a.z, fmul(2.0f, rec.a.w));
         const float o = rec.b.y;
-        s_qmax[j] = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
+        const float qmax = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
+        s_cqo[j] = make_float4(rec.b.x, qmax, o, 0.0f);
+        s_col[j] = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
+        if (kFull) s_sem[j] = p.semantic_ids[__float_as_int(rec.b.w)];
         const __half2 box = *reinterpret_cast<const __half2*>(&rec.c.w);
         const float hx = __low2float(box);
         const float hy = __high2float(box);
@@ -134,69 +195,28 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
           while (bits) {
             const int j = base + __ffs(bits) - 1;
             bits &= bits - 1;
-            if (!done) {
-              const float4 ra = s_a[j];
-              const float conic2 = s_b[j].x;
-              const float dx = fsub(cx, ra.x);
-              const float dy = fsub(cy, ra.y);
-              const float q = ffma(fmul(conic2, dy), dy,
-                                   ffma(fmul(fmul(2.0f, ra.w), dx), dy, fmul(fmul(ra.z, dx), dx)));
-              if (q <= s_qmax[j]) {
-                const float power = fmul(-0.5f, q);
-                if (!(power > 0.0f || power < -20.0f)) {
-                  const float4 rb = s_b[j];
-                  const float alpha = fminf(kMaxAlpha, fmul(rb.y, vexp(power)));
-                  if (alpha >= kAlphaThreshold) {
-                    const float next_t = fmul(transmittance, fsub(1.0f, alpha));
-                    if (next_t <= kTransmittanceThreshold) {
-                      done = true;
-                    } else {
-                      const float w = fmul(transmittance, alpha);
-                      const float4 rc = s_c[j];
-                      acc_r = ffma(w, rc.x, acc_r);
-                      acc_g = ffma(w, rc.y, acc_g);
-                      acc_b = ffma(w, rc.z, acc_b);
-                      if (kFull) {
-                        acc_depth = ffma(w, rb.z, acc_depth);
-                        if (w > best_weight) {
-                          best_weight = w;
-                          best_semantic = s_sem[j];
-                        }
-                      }
-                      transmittance = next_t;
-                    }
-                  }
-                }
-              }
-            }
-            if (__all_sync(0xffffffffu, done)) {
-              warp_done = true;
-              break;
-            }
+            const float4 geo = s_geo[j];
+            const float cq = s_cqo[j].x;
+            const float qmax = s_cqo[j].y;
+            const float dx = fsub(cx, geo.x);
+            const float adx = fmul(fmul(geo.z, dx), dx);
+            const float bdx = fmul(geo.w, dx);
+            const float dy0 = fsub(cy0, geo.y);
+            const float dy1 = fsub(cy1, geo.y);
+            const float q0 = ffma(fmul(cq, dy0), dy0, ffma(bdx, dy0, adx));
+            const float q1 = ffma(fmul(cq, dy1), dy1, ffma(bdx, dy1, adx));
+            blend<kFull>(s0, q0, qmax, j, s_cqo, s_col, s_sem);
+            blend<kFull>(s1, q1, qmax, j, s_cqo, s_col, s_sem);
           }
+          warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
         }
       }
-      if (__syncthreads_count(!done) == 0) break;
+      if (__syncthreads_count(!(s0.done && s1.done)) == 0) break;
     }
   }
 
-  if (!valid) return;
-  const int64_t pixel = plan.pixel_base + static_cast<int64_t>(pixel_y) * plan.width + pixel_x;
-  const float out_alpha = fsub(1.0f, transmittance);
-  if (p.output_srgb) {
-    acc_r = linear_to_srgb(acc_r);
-    acc_g = linear_to_srgb(acc_g);
-    acc_b = linear_to_srgb(acc_b);
-  }
-  p.rgb[pixel * 3 + 0] = acc_r;
-  p.rgb[pixel * 3 + 1] = acc_g;
-  p.rgb[pixel * 3 + 2] = acc_b;
-  if (kFull) {
-    p.alpha[pixel] = out_alpha;
-    p.depth[pixel] = out_alpha > 1.0e-8f ? fdiv(acc_depth, out_alpha) : __int_as_float(0x7f800000);
-    p.semantic[pixel] =
-        (best_weight >= 0.0f && out_alpha >= p.semantic_min_alpha) ? best_semantic : -1;
-  }
+  if (valid0) write_pixel<kFull>(p, plan, pixel_x, pixel_y0, s0);
+  if (valid1) write_pixel<kFull>(p, plan, pixel_x, pixel_y1, s1);
 }
 
 template __global__ void composite_kernel<4, false>(CompositeParams);

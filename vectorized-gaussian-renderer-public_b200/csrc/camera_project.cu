@@ -275,10 +275,32 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
 // Real spherical harmonics through degree 3 (the basis and constants of the
 // 3D Gaussian Splatting reference implementation, as used by gsplat), view
 // direction from the camera centre to the mean in object space, +0.5 offset,
-// clamped at zero.  coeffs is [(d+1)^2, 3], coefficient-major.
-__device__ __forceinline__ void eval_sh(int degree, const float* __restrict__ coeffs,
+// clamped at zero.  coeffs is [(d+1)^2, 3], coefficient-major.  With
+// vector_loads the row is fetched as float4s (rows 16-byte aligned and padded
+// to a multiple of four floats), otherwise as scalars.
+template <int kDegree>
+__device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vector_loads,
                                         const CamConst& c, float px, float py, float pz,
                                         float* rgb) {
+  constexpr int kCount = (kDegree + 1) * (kDegree + 1);
+  constexpr int kFloats = kCount * 3;
+  constexpr int kVectors = (kFloats + 3) / 4;
+  float coeffs[kVectors * 4];
+  if (vector_loads) {
+    const float4* row4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+    for (int i = 0; i < kVectors; ++i) {
+      const float4 v = __ldg(row4 + i);
+      coeffs[4 * i + 0] = v.x;
+      coeffs[4 * i + 1] = v.y;
+      coeffs[4 * i + 2] = v.z;
+      coeffs[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kFloats; ++i) coeffs[i] = __ldg(row + i);
+  }
+  const int degree = kDegree;
   float dx = ffma(c.r[6], pz, ffma(c.r[3], py, fmul(c.r[0], px)));
   float dy = ffma(c.r[7], pz, ffma(c.r[4], py, fmul(c.r[1], px)));
   float dz = ffma(c.r[8], pz, ffma(c.r[5], py, fmul(c.r[2], px)));
@@ -317,6 +339,7 @@ __device__ __forceinline__ void eval_sh(int degree, const float* __restrict__ co
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) {
     float acc = fmul(basis[0], coeffs[ch]);
+#pragma unroll
     for (int k = 1; k < count; ++k) acc = ffma(basis[k], coeffs[k * 3 + ch], acc);
     rgb[ch] = fmaxf(fadd(acc, 0.5f), 0.0f);
   }
@@ -389,15 +412,15 @@ __device__ __forceinline__ void project_lookback(uint64_t* desc, int64_t b, uint
 }
 
 template <int kShDegree>
-__global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectParams p) {
-  __shared__ Record s_rec[kProjectChunk];
+__global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(ProjectParams p) {
+  __shared__ Record s_rec[kProjectChunk];          // by task slot
+  __shared__ uint16_t s_slot[kProjectChunk];       // rank -> task slot
   __shared__ uint32_t s_rect_min[kProjectChunk];   // min_tx | min_ty << 16
   __shared__ uint32_t s_rect_size[kProjectChunk];  // ntx | nty << 16
   __shared__ uint32_t s_prefix[kProjectChunk + 1]; // exclusive isect prefix
   __shared__ int32_t s_radii[kProjectChunk * 2];
-  __shared__ int64_t s_gid[kProjectChunk];
-  __shared__ uint32_t s_warp_vis[kProjectThreads / 32];
-  __shared__ uint64_t s_warp_isect[kProjectThreads / 32];
+  __shared__ uint32_t s_warp_vis[kProjectRounds][kProjectThreads / 32];
+  __shared__ uint64_t s_warp_isect[kProjectRounds][kProjectThreads / 32];
   __shared__ CamConst s_cam;
   __shared__ CamPlan s_plan;
   __shared__ int64_t s_vblock;
@@ -441,96 +464,114 @@ __global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectPa
     }
     __syncthreads();
 
-    uint32_t block_vis = 0;
-    uint64_t block_isect = 0;
-    if (live) {
-      const float its = 1.0f / static_cast<float>(p.tile_size);
+    // Project both rounds first (no barrier), then one block scan of
+    // (visible, tiles) over the kProjectChunk tasks in task order.
+    bool vis[kProjectRounds];
+    uint32_t ntiles[kProjectRounds], rect_min[kProjectRounds], rect_size[kProjectRounds];
+    int32_t radius_x[kProjectRounds], radius_y[kProjectRounds];
+    const float its = 1.0f / static_cast<float>(p.tile_size);
 #pragma unroll
-      for (int round = 0; round < kProjectRounds; ++round) {
-        const int64_t local = local_begin + round * kProjectThreads + tid;
-        Projected pr;
-        bool vis = false;
-        uint32_t rect_min = 0, rect_size = 0, ntiles = 0;
-        if (local < plan.g_count) {
-          vis = project_gaussian(p.means, p.covariances, p.opacities, plan.g_begin + local, s_cam,
-                                 p.near_plane, p.far_plane, p.support_sigma, p.cov_eps,
-                                 p.antialiased, &pr);
-          if (vis) {
-            const float frx = static_cast<float>(pr.radius_x);
-            const float fry = static_cast<float>(pr.radius_y);
-            const int min_tx = max(0, floor_clamped(fsub(fmul(pr.mean_x, its), fmul(frx, its))));
-            const int min_ty = max(0, floor_clamped(fsub(fmul(pr.mean_y, its), fmul(fry, its))));
-            const int max_tx =
-                min(plan.tiles_x, ceil_clamped(fadd(fmul(pr.mean_x, its), fmul(frx, its))));
-            const int max_ty =
-                min(plan.tiles_y, ceil_clamped(fadd(fmul(pr.mean_y, its), fmul(fry, its))));
-            const int ntx = max(0, max_tx - min_tx);
-            const int nty = max(0, max_ty - min_ty);
-            ntiles = static_cast<uint32_t>(ntx) * static_cast<uint32_t>(nty);
-            rect_min = static_cast<uint32_t>(min(min_tx, 65535)) |
-                       (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
-            rect_size = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
-          }
-        }
-        // Block scan of (visible, tiles) in task order.
-        uint32_t v_incl = vis ? 1u : 0u;
-        uint64_t t_incl = ntiles;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t nv = __shfl_up_sync(0xffffffffu, v_incl, o);
-          const uint64_t nt = __shfl_up_sync(0xffffffffu, t_incl, o);
-          if (lane >= o) {
-            v_incl += nv;
-            t_incl += nt;
-          }
-        }
-        if (lane == 31) {
-          s_warp_vis[warp] = v_incl;
-          s_warp_isect[warp] = t_incl;
-        }
-        __syncthreads();
-        uint32_t wv = 0;
-        uint64_t wt = 0;
-        for (int w = 0; w < warp; ++w) {
-          wv += s_warp_vis[w];
-          wt += s_warp_isect[w];
-        }
-        uint32_t rv = 0;
-        uint64_t rt = 0;
-        for (int w = 0; w < kProjectThreads / 32; ++w) {
-          rv += s_warp_vis[w];
-          rt += s_warp_isect[w];
-        }
-        if (vis) {
-          const uint32_t rank = block_vis + wv + v_incl - 1;
-          const uint64_t excl = block_isect + wt + t_incl - ntiles;
-          Record rec;
+    for (int round = 0; round < kProjectRounds; ++round) {
+      const int64_t local = local_begin + round * kProjectThreads + tid;
+      vis[round] = false;
+      ntiles[round] = 0;
+      rect_min[round] = 0;
+      rect_size[round] = 0;
+      radius_x[round] = 0;
+      radius_y[round] = 0;
+      Projected pr;
+      if (live && local < plan.g_count) {
+        const int64_t g = plan.g_begin + local;
+        vis[round] = project_gaussian(p.means, p.covariances, p.opacities, g, s_cam, p.near_plane,
+                                      p.far_plane, p.support_sigma, p.cov_eps, p.antialiased, &pr);
+        if (vis[round]) {
+          const float frx = static_cast<float>(pr.radius_x);
+          const float fry = static_cast<float>(pr.radius_y);
+          const int min_tx = max(0, floor_clamped(fsub(fmul(pr.mean_x, its), fmul(frx, its))));
+          const int min_ty = max(0, floor_clamped(fsub(fmul(pr.mean_y, its), fmul(fry, its))));
+          const int max_tx =
+              min(plan.tiles_x, ceil_clamped(fadd(fmul(pr.mean_x, its), fmul(frx, its))));
+          const int max_ty =
+              min(plan.tiles_y, ceil_clamped(fadd(fmul(pr.mean_y, its), fmul(fry, its))));
+          const int ntx = max(0, max_tx - min_tx);
+          const int nty = max(0, max_ty - min_ty);
+          ntiles[round] = static_cast<uint32_t>(ntx) * static_cast<uint32_t>(nty);
+          rect_min[round] = static_cast<uint32_t>(min(min_tx, 65535)) |
+                            (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
+          rect_size[round] = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
+          radius_x[round] = pr.radius_x;
+          radius_y[round] = pr.radius_y;
           float rgb[3];
-          const int64_t g = plan.g_begin + local;
           if (kShDegree < 0) {
             rgb[0] = p.features[g * p.feature_width + 0];
             rgb[1] = p.features[g * p.feature_width + 1];
             rgb[2] = p.features[g * p.feature_width + 2];
           } else {
-            eval_sh(kShDegree, p.features + g * p.feature_width, s_cam, pr.px, pr.py, pr.pz, rgb);
+            eval_sh<kShDegree < 0 ? 0 : kShDegree>(p.features + g * p.feature_width,
+                                                   p.vector_feature_loads, s_cam, pr.px, pr.py,
+                                                   pr.pz, rgb);
           }
-          rec.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
-          rec.b = make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(static_cast<int>(g)));
-          rec.c = make_float4(rgb[0], rgb[1], rgb[2],
-                              __uint_as_float(footprint_box(pr.opacity, pr.cov_a, pr.cov_b,
-                                                            pr.cov_c)));
-          s_rec[rank] = rec;
-          s_rect_min[rank] = rect_min;
-          s_rect_size[rank] = rect_size;
-          s_prefix[rank] = static_cast<uint32_t>(excl > 0x7fffffffull ? 0x7fffffffull : excl);
-          s_radii[rank * 2 + 0] = pr.radius_x;
-          s_radii[rank * 2 + 1] = pr.radius_y;
-          s_gid[rank] = g;
+          // Staged by task slot; the scan below maps ranks to slots.
+          Record& staged = s_rec[round * kProjectThreads + tid];
+          staged.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
+          staged.b =
+              make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(static_cast<int>(g)));
+          staged.c = make_float4(
+              rgb[0], rgb[1], rgb[2],
+              __uint_as_float(footprint_box(pr.opacity, pr.cov_a, pr.cov_b, pr.cov_c)));
         }
-        block_vis += rv;
-        block_isect += rt;
-        __syncthreads();
       }
+    }
+    uint32_t v_incl[kProjectRounds];
+    uint64_t t_incl[kProjectRounds];
+#pragma unroll
+    for (int round = 0; round < kProjectRounds; ++round) {
+      v_incl[round] = vis[round] ? 1u : 0u;
+      t_incl[round] = ntiles[round];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t nv = __shfl_up_sync(0xffffffffu, v_incl[round], o);
+        const uint64_t nt = __shfl_up_sync(0xffffffffu, t_incl[round], o);
+        if (lane >= o) {
+          v_incl[round] += nv;
+          t_incl[round] += nt;
+        }
+      }
+      if (lane == 31) {
+        s_warp_vis[round][warp] = v_incl[round];
+        s_warp_isect[round][warp] = t_incl[round];
+      }
+    }
+    __syncthreads();
+    uint32_t block_vis = 0;
+    uint64_t block_isect = 0;
+#pragma unroll
+    for (int round = 0; round < kProjectRounds; ++round) {
+      uint32_t wv = 0, rv = 0;
+      uint64_t wt = 0, rt = 0;
+#pragma unroll
+      for (int w = 0; w < kProjectThreads / 32; ++w) {
+        const uint32_t sv = s_warp_vis[round][w];
+        const uint64_t st = s_warp_isect[round][w];
+        if (w < warp) {
+          wv += sv;
+          wt += st;
+        }
+        rv += sv;
+        rt += st;
+      }
+      if (vis[round]) {
+        const uint32_t rank = block_vis + wv + v_incl[round] - 1;
+        const uint64_t excl = block_isect + wt + t_incl[round] - ntiles[round];
+        s_slot[rank] = static_cast<uint16_t>(round * kProjectThreads + tid);
+        s_rect_min[rank] = rect_min[round];
+        s_rect_size[rank] = rect_size[round];
+        s_prefix[rank] = static_cast<uint32_t>(excl > 0x7fffffffull ? 0x7fffffffull : excl);
+        s_radii[rank * 2 + 0] = radius_x[round];
+        s_radii[rank * 2 + 1] = radius_y[round];
+      }
+      block_vis += rv;
+      block_isect += rt;
     }
     if (tid == 0) {
       s_nvis = block_vis;
@@ -582,14 +623,15 @@ __global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectPa
       float4* dst = reinterpret_cast<float4*>(p.records);
       const float4* src = reinterpret_cast<const float4*>(s_rec);
       for (uint32_t i = tid; i < nvis * 3; i += kProjectThreads) {
-        const uint64_t r = base_vis + i / 3;
-        if (r < vcap) dst[r * 3 + (i % 3)] = src[i];
+        const uint32_t rank = i / 3;
+        const uint64_t r = base_vis + rank;
+        if (r < vcap) dst[r * 3 + (i - rank * 3)] = src[s_slot[rank] * 3 + (i - rank * 3)];
       }
       if (p.mirror_means2d) {
         for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
           const uint64_t r = base_vis + i;
           if (r >= vcap) continue;
-          const Record rec = s_rec[i];
+          const Record rec = s_rec[s_slot[i]];
           p.mirror_means2d[r * 2 + 0] = rec.a.x;
           p.mirror_means2d[r * 2 + 1] = rec.a.y;
           p.mirror_conics[r * 3 + 0] = rec.a.z;
@@ -598,7 +640,7 @@ __global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectPa
           p.mirror_depths[r] = rec.b.z;
           p.mirror_opacities[r] = rec.b.y;
           p.mirror_camera_ids[r] = plan.camera;
-          p.mirror_gaussian_ids[r] = static_cast<int32_t>(s_gid[i]);
+          p.mirror_gaussian_ids[r] = __float_as_int(rec.b.w);
           p.mirror_radii[r * 2 + 0] = s_radii[i * 2 + 0];
           p.mirror_radii[r * 2 + 1] = s_radii[i * 2 + 1];
         }
@@ -632,7 +674,7 @@ __global__ void __launch_bounds__(kProjectThreads) project_emit_kernel(ProjectPa
         if (r < vcap) {
           const uint64_t tile = static_cast<uint64_t>(plan.tile_base) +
                                 static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
-          key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[i].b.z));
+          key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[s_slot[i]].b.z));
           value = static_cast<int32_t>(r);
         }
         p.keys[base_isect + j] = key;

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(SortParams
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(SortParams p) {
+__global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(SortParams p) {
   constexpr int kWarps = kSortThreads / 32;
   __shared__ uint32_t s_warp_hist[kWarps][kRadixBins];
   extern __shared__ __align__(16) unsigned char s_dynamic[];
@@ -116,33 +116,33 @@ __global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(SortParams 
     if (part >= parts) break;
     const int64_t begin = part * kSortTile;
 
+    // Items in (warp, k, lane) order; digit and in-warp rank packed as
+    // digit << 16 | rank (digit 0x1ff marks an item past the end).
     uint64_t keys[kSortItems];
     int32_t vals[kSortItems];
-    uint32_t digits[kSortItems];
-    uint32_t ranks[kSortItems];
-    const uint32_t lt = lanemask_lt();
+    uint32_t dr[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
       const int64_t idx = begin + warp * (kSortItems * 32) + k * 32 + lane;
       const bool valid = idx < n;
       keys[k] = valid ? p.keys_in[idx] : 0ull;
       vals[k] = valid ? p.values_in[idx] : 0;
-      digits[k] = valid
-          ? static_cast<uint32_t>((composite_key(keys[k], p.map) >> shift) & (kRadixBins - 1))
-          : (kRadixBins + lane);  // unique per lane: matches nothing valid
     }
-    // Stable warp-local ranking, item order = (warp, k, lane).
+    const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
-      const uint32_t d = digits[k];
+      const int64_t idx = begin + warp * (kSortItems * 32) + k * 32 + lane;
+      const bool valid = idx < n;
+      const uint32_t d = valid
+          ? static_cast<uint32_t>((composite_key(keys[k], p.map) >> shift) & (kRadixBins - 1))
+          : (kRadixBins + lane);  // unique per lane: matches nothing valid
       const uint32_t peers = __match_any_sync(0xffffffffu, d);
-      const bool valid = d < kRadixBins;
       uint32_t old = 0;
       if (valid) old = s_warp_hist[warp][d];
       __syncwarp();
       if (valid && lane == (__ffs(peers) - 1)) s_warp_hist[warp][d] = old + __popc(peers);
       __syncwarp();
-      ranks[k] = old + __popc(peers & lt);
+      dr[k] = valid ? ((d << 16) | (old + __popc(peers & lt))) : (0x1ffu << 16);
     }
     __syncthreads();
     // Per digit: exclusive prefix across warps and the partition total.
@@ -200,9 +200,9 @@ __global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(SortParams 
     // Reorder the partition by digit in shared memory.
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
-      const uint32_t dk = digits[k];
+      const uint32_t dk = dr[k] >> 16;
       if (dk < kRadixBins) {
-        const uint32_t pos = s_digit_start[dk] + s_warp_hist[warp][dk] + ranks[k];
+        const uint32_t pos = s_digit_start[dk] + s_warp_hist[warp][dk] + (dr[k] & 0xffffu);
         s_keys[pos] = keys[k];
         s_vals[pos] = vals[k];
       }

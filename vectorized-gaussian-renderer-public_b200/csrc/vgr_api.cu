@@ -418,6 +418,8 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     pp.opacities = scene->opacities;
     pp.features = scene->features;
     pp.feature_width = scene->feature_width;
+    pp.vector_feature_loads = (reinterpret_cast<uintptr_t>(scene->features) & 15) == 0 &&
+                              (scene->feature_width & 3) == 0;
     pp.viewmats = cams->viewmats;
     pp.intrinsics = cams->intrinsics;
     pp.env_xforms = cams->env_xforms;
@@ -541,14 +543,14 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     const unsigned grid = static_cast<unsigned>(max_items);
     const bool full = opt->full_sensor_output != 0;
     if (ts == 16) {
-      if (full) composite_kernel<16, true><<<grid, 256, 0, stream>>>(cp);
-      else composite_kernel<16, false><<<grid, 256, 0, stream>>>(cp);
+      if (full) composite_kernel<16, true><<<grid, composite_threads(16), 0, stream>>>(cp);
+      else composite_kernel<16, false><<<grid, composite_threads(16), 0, stream>>>(cp);
     } else if (ts == 8) {
-      if (full) composite_kernel<8, true><<<grid, 64, 0, stream>>>(cp);
-      else composite_kernel<8, false><<<grid, 64, 0, stream>>>(cp);
+      if (full) composite_kernel<8, true><<<grid, composite_threads(8), 0, stream>>>(cp);
+      else composite_kernel<8, false><<<grid, composite_threads(8), 0, stream>>>(cp);
     } else {
-      if (full) composite_kernel<4, true><<<grid, 32, 0, stream>>>(cp);
-      else composite_kernel<4, false><<<grid, 32, 0, stream>>>(cp);
+      if (full) composite_kernel<4, true><<<grid, composite_threads(4), 0, stream>>>(cp);
+      else composite_kernel<4, false><<<grid, composite_threads(4), 0, stream>>>(cp);
     }
     if ((rc = check_launch("render: compositor")) != VGR_OK) return rc;
   }

@@ -36,6 +36,7 @@ struct ProjectParams {
   const float* opacities;
   const float* features;
   int64_t feature_width;
+  bool vector_feature_loads;  // rows 16-byte aligned and a multiple of 4 floats
   const float* viewmats;
   const float* intrinsics;
   const float* env_xforms;
@@ -115,5 +116,8 @@ __global__ void sort_onesweep_kernel(SortParams p);
 __global__ void tile_ranges_kernel(RangeParams p);
 template <int kTile, bool kFull>
 __global__ void composite_kernel(CompositeParams p);
+
+// Threads per compositor CTA (two pixels per thread, 8x8-pixel warp blocks).
+constexpr int composite_threads(int tile) { return tile >= 16 ? 128 : 32; }
 
 }  // namespace vgr
