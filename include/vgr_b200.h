@@ -234,6 +234,96 @@ int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras
                               const vgr_render_options* options, void* stream,
                               int64_t* sorted_buffer_selector);
 
+/* ------------------------------------------------------------------ LiDAR */
+
+/* Caller-owned Gaussian LiDAR scene (lidar_scene.py:13-96): WXYZ rotations,
+ * activated scales/opacity; reflectivity and surface_confidence may be NULL
+ * (constant fallback reflectivity, confidence 1). */
+typedef struct vgr_lidar_scene {
+  const float* means;              /* [G,3] */
+  const float* scales;             /* [G,3] */
+  const float* rotations;          /* [G,4] WXYZ */
+  const float* opacities;          /* [G] */
+  const int64_t* semantic_ids;     /* [G] */
+  const float* reflectivity;       /* [G] or NULL */
+  const float* surface_confidence; /* [G] or NULL */
+  int64_t count;                   /* G */
+} vgr_lidar_scene;
+
+/* Shared sensor-local rays against per-sensor scenes
+ * (lidar_renderer.cpp:133-210 inputs[6]). */
+typedef struct vgr_lidar_inputs {
+  const float* ray_directions;      /* [R,3] unit, sensor frame */
+  int64_t rays;                     /* R */
+  const void* time_offsets;         /* [R] int32 or int64 */
+  int32_t time_offsets_are_int64;
+  const float* sensor_to_world;     /* [B,4,4] */
+  const float* scene_to_world;      /* [B,4,4] */
+  const int64_t* scene_ids;         /* [B] */
+  int64_t batch;                    /* B */
+  const int64_t* active_sensor_ids; /* [A] strictly increasing, or NULL (all) */
+  int64_t active_count;
+} vgr_lidar_inputs;
+
+/* outputs[7] of the reference: every element is rewritten each call. */
+typedef struct vgr_lidar_outputs {
+  float* range_m;            /* [B,R,K] (+inf when no return) */
+  float* position_world_m;   /* [B,R,K,3] */
+  float* intensity;          /* [B,R,K] */
+  int64_t* semantic_id;      /* [B,R,K] (-1 when no return) */
+  uint8_t* valid;            /* [B,R,K] bool */
+  int64_t* time_offset_ns;   /* [B,R,K] */
+  int32_t* return_count;     /* [B,R] */
+} vgr_lidar_outputs;
+
+typedef struct vgr_lidar_options {
+  int32_t returns;           /* 1 or 2 */
+  int32_t semantic_slots;    /* 1..32 */
+  double near_plane_m;
+  double far_plane_m;
+  double support_sigma;
+  double detection_threshold;
+  double planarity_ratio_max;
+  double min_incidence_cos;
+  double cluster_abs_m;
+  double cluster_relative;
+  double fallback_reflectivity;
+  double direction_norm_tolerance;
+} vgr_lidar_options;
+
+/* Counter slots, same order as the reference LIDAR_COUNTER_NAMES
+ * (cuda_lidar_backend.py:19-32). */
+#define VGR_LIDAR_COUNTERS 12
+/* One scene descriptor occupies at most one reference [S,14] int64 row. */
+#define VGR_LIDAR_DESCRIPTOR_BYTES 112
+
+/* Replaces sort_temp_bytes (lidar_renderer.cpp:62-65,
+ * lidar_renderer_cuda.cu:853-868): bytes of the per-scene acceleration
+ * buffer (surfel records, LBVH nodes and the build's sort scratch). */
+int64_t vgr_lidar_sort_temp_bytes(int64_t num_items, int32_t packet_size);
+
+/* Replaces build_scene_lbvh (lidar_renderer.cpp:67-108,
+ * lidar_renderer_cuda.cu:870-929): Morton sort of the planar surfels, packet
+ * leaves, Karras radix tree and bottom-up box refit, into accel. */
+int vgr_lidar_build_scene_lbvh(const vgr_lidar_scene* scene, int32_t packet_size,
+                               double support_sigma, double planarity_ratio_max,
+                               void* accel, int64_t accel_bytes, void* stream);
+
+/* Replaces pack_scene_descriptor (lidar_renderer.cpp:110-131,
+ * lidar_renderer_cuda.cu:931-959): writes descriptor slot `slot` of a device
+ * table of VGR_LIDAR_DESCRIPTOR_BYTES-byte rows. */
+int vgr_lidar_pack_scene_descriptor(void* descriptors, int64_t descriptor_capacity,
+                                    int64_t slot, int64_t scene_id, const void* accel,
+                                    int64_t gaussian_count, int32_t packet_size,
+                                    void* stream);
+
+/* Replaces render_lidar (lidar_renderer.cpp:133-210,
+ * lidar_renderer_cuda.cu:961-1051): no-hit clear, first-return tracing of
+ * every (active sensor, ray), device counters[VGR_LIDAR_COUNTERS]. */
+int vgr_render_lidar(const void* descriptors, int64_t scene_count,
+                     const vgr_lidar_inputs* inputs, const vgr_lidar_outputs* outputs,
+                     int64_t* counters, const vgr_lidar_options* options, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

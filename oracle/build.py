@@ -1,6 +1,7 @@
 """Build the CPU parity oracles (test infrastructure only).
 
   liboracle_camera.so  <- oracle/camera_oracle.c (gcc, IEEE float, no contraction)
+  liboracle_lidar.so   <- oracle/lidar_oracle.c (gcc, float64)
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
 these libraries; the renderer itself never does.
@@ -32,7 +33,10 @@ def _stale(target: Path, source: Path) -> bool:
 
 def build(force: bool = False) -> list[Path]:
     outputs = []
-    for source, target in ((HERE / "camera_oracle.c", HERE / "liboracle_camera.so"),):
+    for source, target in (
+        (HERE / "camera_oracle.c", HERE / "liboracle_camera.so"),
+        (HERE / "lidar_oracle.c", HERE / "liboracle_lidar.so"),
+    ):
         if force or _stale(target, source):
             cmd = ["gcc", *FLAGS, str(source), "-o", str(target), "-lm"]
             result = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,56 @@
+"""The CPU camera oracle against golden vectors of the reference's own CUDA build.
+
+tests/golden/camera_*.npz were produced on a B200 by
+tests/golden/make_reference_golden.py from the reference extension compiled
+from its sources (oracle/build_ref.py).  The oracle (and, transitively, the
+CUDA path, which is bit-exact with the oracle) must reproduce the
+reference's frame counters and per-tile intersection counts exactly, RGB and
+alpha within 1e-4, depth within 1e-4 relative, and semantic labels; the
+sorted per-tile lists must hold the same Gaussians in the same order except
+where two depths within a float ulp swap (the reference computes depth with
+--use_fast_math contraction, the oracle with plain IEEE operations).
+"""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from golden.cases import CASES
+from helpers import render_oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_cuda_build(name):
+    golden = np.load(GOLDEN / f"camera_{name}.npz")
+    scenes, rig, scene_ids = CASES[name]["build"]()
+    got = render_oracle(scenes, rig, scene_ids, with_tiles=True, **CASES[name]["options"])
+
+    counters = golden["counters"]
+    assert got.visible == int(counters[0])
+    assert got.intersections == int(counters[1])
+    assert got.active_tiles == int(counters[4])
+    np.testing.assert_array_equal(got.tile_counts, golden["tile_counts"])
+
+    assert np.abs(got.rgb - golden["rgb"]).max() <= 1e-4
+    assert np.abs(got.alpha - golden["alpha"]).max() <= 1e-4
+    np.testing.assert_array_equal(np.isinf(got.depth), np.isinf(golden["depth"]))
+    covered = (golden["alpha"] > 1e-3) & np.isfinite(golden["depth"])
+    rel = np.abs(got.depth - golden["depth"])[covered] / np.abs(golden["depth"][covered])
+    assert rel.max() <= 1e-4
+    assert (got.semantic == golden["semantic"]).mean() >= 0.999
+
+    ref_ids = golden["sorted_gaussian_ids"]
+    ids = got.sorted_gaussian_ids
+    assert ids.shape == ref_ids.shape
+    starts = np.concatenate([[0], np.cumsum(golden["tile_counts"])])
+    for tile in range(len(starts) - 1):
+        a = ids[starts[tile] : starts[tile + 1]]
+        b = ref_ids[starts[tile] : starts[tile + 1]]
+        np.testing.assert_array_equal(np.sort(a), np.sort(b))
+    differing = np.count_nonzero(ids != ref_ids)
+    assert differing <= max(2, ids.size // 1000), differing

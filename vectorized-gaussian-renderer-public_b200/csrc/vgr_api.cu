@@ -355,7 +355,7 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
 
   const float near_f = static_cast<float>(opt->near_plane);
   const float far_f = static_cast<float>(opt->far_plane);
-  SortKeyMap map;
+  SortKeyMap map{};
   map.near_bits = float_bits(near_f);
   map.depth_bits = static_cast<uint32_t>(bit_length(float_bits(far_f) - map.near_bits));
   map.tile_count = static_cast<uint32_t>(global_tiles);

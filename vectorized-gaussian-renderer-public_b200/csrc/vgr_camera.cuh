@@ -110,9 +110,11 @@ struct SortKeyMap {
   uint32_t depth_bits;   // bit width of (far_bits - near_bits)
   uint32_t total_bits;   // tile bits + depth bits
   uint32_t tile_count;   // global tiles
+  uint32_t raw;          // nonzero: digits come from the key itself (LBVH Morton sort)
 };
 
 __device__ __forceinline__ uint64_t composite_key(uint64_t key, const SortKeyMap& m) {
+  if (m.raw) return key;
   const uint32_t tile = static_cast<uint32_t>(key >> 32);
   if (tile >= m.tile_count) {
     return ~0ull;

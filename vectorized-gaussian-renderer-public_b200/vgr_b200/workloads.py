@@ -153,6 +153,85 @@ def orbit_cameras(
     return CameraRig(view, pinhole(count, focal, focal, width / 2.0, height / 2.0), height, width)
 
 
+@dataclass
+class LidarWorkload:
+    means: torch.Tensor
+    scales: torch.Tensor
+    rotations: torch.Tensor
+    opacities: torch.Tensor
+    semantic_ids: torch.Tensor
+    reflectivity: torch.Tensor
+    ray_directions: torch.Tensor  # [R,3] sensor frame
+    time_offsets_ns: torch.Tensor  # [R] int64
+    sensor_to_world: torch.Tensor  # [B,4,4]
+
+    def scene_kwargs(self, device) -> dict[str, torch.Tensor]:
+        return {
+            name: getattr(self, name).to(device).contiguous()
+            for name in ("means", "scales", "rotations", "opacities", "semantic_ids", "reflectivity")
+        }
+
+
+def spinning_lidar_rays(beams: int = 128, azimuths: int = 2048, low_deg: float = -25.0,
+                        high_deg: float = 15.0) -> tuple[torch.Tensor, torch.Tensor]:
+    """Unit rays of a spinning LiDAR: beams evenly spaced in elevation, azimuth-major order."""
+    elev = torch.linspace(math.radians(low_deg), math.radians(high_deg), beams, dtype=torch.float64)
+    azim = torch.arange(azimuths, dtype=torch.float64) * (2.0 * math.pi / azimuths)
+    a, e = torch.meshgrid(azim, elev, indexing="ij")
+    dirs = torch.stack((torch.cos(e) * torch.cos(a), torch.cos(e) * torch.sin(a), torch.sin(e)), dim=-1)
+    dirs = dirs.reshape(-1, 3)
+    dirs = dirs / dirs.norm(dim=1, keepdim=True)
+    # One revolution in 100 ms, azimuth-major.
+    times = (torch.arange(azimuths, dtype=torch.int64) * (100_000_000 // azimuths)).repeat_interleave(beams)
+    return dirs.float().contiguous(), times.contiguous()
+
+
+def lidar_workload(gaussians: int = 2_000_000, sensors: int = 64, beams: int = 128,
+                   azimuths: int = 2048, seed: int = 5) -> LidarWorkload:
+    """Gaussian LiDAR tracing: Gaussians in a 40 x 40 x 6 m box, log-scales
+    N(-3, 0.5), reflectivity U[0,1], semantic U{0..15}; spinning sensors of
+    `beams` x `azimuths` rays at random positions 1-2 m above the floor."""
+    gen = torch.Generator().manual_seed(seed)
+    lo = torch.tensor([-20.0, -20.0, 0.0], dtype=torch.float64)
+    ext = torch.tensor([40.0, 40.0, 6.0], dtype=torch.float64)
+    means = lo + torch.rand((gaussians, 3), generator=gen, dtype=torch.float64) * ext
+    scales = torch.exp(torch.randn((gaussians, 3), generator=gen) * 0.5 - 3.0)
+    quats = torch.randn((gaussians, 4), generator=gen)
+    quats = quats / quats.norm(dim=1, keepdim=True)
+    opacities = torch.sigmoid(torch.randn((gaussians,), generator=gen))
+    reflectivity = torch.rand((gaussians,), generator=gen)
+    semantic = torch.randint(0, 16, (gaussians,), generator=gen, dtype=torch.int64)
+    dirs, times = spinning_lidar_rays(beams, azimuths)
+    pos = torch.stack(
+        (
+            torch.rand((sensors,), generator=gen, dtype=torch.float64) * 36.0 - 18.0,
+            torch.rand((sensors,), generator=gen, dtype=torch.float64) * 36.0 - 18.0,
+            1.0 + torch.rand((sensors,), generator=gen, dtype=torch.float64),
+        ),
+        dim=1,
+    )
+    yaw = torch.rand((sensors,), generator=gen, dtype=torch.float64) * 2.0 * math.pi
+    xform = torch.zeros((sensors, 4, 4), dtype=torch.float64)
+    xform[:, 0, 0] = torch.cos(yaw)
+    xform[:, 0, 1] = -torch.sin(yaw)
+    xform[:, 1, 0] = torch.sin(yaw)
+    xform[:, 1, 1] = torch.cos(yaw)
+    xform[:, 2, 2] = 1.0
+    xform[:, :3, 3] = pos
+    xform[:, 3, 3] = 1.0
+    return LidarWorkload(
+        means=means.float().contiguous(),
+        scales=scales.float().contiguous(),
+        rotations=quats.float().contiguous(),
+        opacities=opacities.float().contiguous(),
+        semantic_ids=semantic.contiguous(),
+        reflectivity=reflectivity.float().contiguous(),
+        ray_directions=dirs,
+        time_offsets_ns=times,
+        sensor_to_world=xform.float().contiguous(),
+    )
+
+
 def plain_workload() -> tuple[SceneTensors, CameraRig]:
     """Plain single-camera forward render: 10k Gaussians, 256x256."""
     return synthetic_scene(10_000, seed=0), plain_camera()
