@@ -69,6 +69,8 @@ def parse_args() -> argparse.Namespace:
                         help="override the camera count (small profiling captures)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--lidar-steps", type=int, default=5,
+                        help="LiDAR frames timed after the camera workload (0: skip)")
     return parser.parse_args()
 
 
@@ -261,6 +263,17 @@ def run_reference(args) -> None:
                          "sample": sample_desc},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.lidar_steps > 0:
+        from vgr_b200 import workloads
+
+        cfg = LIDAR_CONFIG
+        work = workloads.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
+        rays_per_s, lidar_threads, lidar_sample = lidar_cpu_sample(work)
+        line["lidar"] = {
+            "metric": LIDAR_METRIC, "value": round(rays_per_s, 1), "unit": "rays/s", "config": cfg,
+            "cpu_baseline": {"value": round(rays_per_s, 1), "unit": "rays/s", "cores": lidar_threads,
+                             "kind": "port", "sample": lidar_sample},
+        }
     print(json.dumps(line), flush=True)
 
 
@@ -284,6 +297,151 @@ def stage_bytes(counters: dict, scene, rig, passes: int, sh_degree) -> dict[str,
         "tile_ranges": i * 8,
         "composite": i * (4 + 48 + 8) + p * 28,
     }
+
+
+# --------------------------------------------------------------------------- LiDAR
+LIDAR_METRIC = "rays/s, LBVH rebuilt every frame"
+LIDAR_CONFIG = {"workload": "lidar-2m-64x128x2048", "gaussians": 2_000_000, "sensors": 64, "beams": 128,
+                "azimuths": 2048, "returns": 1, "far_plane_m": 80.0, "packet": 8,
+                "motion": "5% of means moved by N(0, 0.05) m before each frame's rebuild"}
+
+
+def lidar_moved_means(means: torch.Tensor, seed: int) -> torch.Tensor:
+    """``means`` with a seeded 5% subset moved by N(0, 0.05) m."""
+    gen = torch.Generator().manual_seed(seed)
+    count = means.shape[0]
+    pick = torch.randperm(count, generator=gen)[: count // 20]
+    moved = means.clone()
+    moved[pick] += torch.randn((pick.numel(), 3), generator=gen) * 0.05
+    return moved.contiguous()
+
+
+def lidar_cpu_sample(work, rays_stride: int = 256, threads: int | None = None) -> tuple[float, int, str]:
+    """Rays/s of the LiDAR CPU oracle on sensor 0 and every ``rays_stride``-th ray."""
+    from oracle import lidar as ol
+
+    threads = threads or os.cpu_count() or 1
+    dirs = work.ray_directions.double().numpy()[::rays_stride]
+    times = work.time_offsets_ns.numpy()[::rays_stride]
+    scene = {
+        "means": work.means.double().numpy(), "scales": work.scales.double().numpy(),
+        "rotations": work.rotations.double().numpy(), "opacities": work.opacities.double().numpy(),
+        "semantic_ids": work.semantic_ids.numpy(), "reflectivity": work.reflectivity.double().numpy(),
+        "surface_confidence": None,
+    }
+    config = ol.LidarConfig(far_plane_m=LIDAR_CONFIG["far_plane_m"])
+    sensors = work.sensor_to_world.double().numpy()[:1]
+    start = time.perf_counter()
+    ol.render({0: scene}, dirs, times, sensors, np.zeros(1, dtype=np.int64), returns=1, config=config,
+              threads=threads)
+    seconds = time.perf_counter() - start
+    rays = dirs.shape[0]
+    return rays / seconds, threads, f"sensor 0, {rays} of {work.ray_directions.shape[0]} rays, full 2M scene"
+
+
+def run_lidar(args, device, world: int, with_cpu: bool) -> dict:
+    """Gaussian LiDAR frames: rebuild the LBVH from moved means, then trace
+    every ray of every sensor (first return)."""
+    from vgr_b200 import workloads
+    from vgr_b200.cuda_lidar_backend import CudaLidarBackend
+    from vgr_b200.lidar_service import GaussianLidarService
+
+    cfg = LIDAR_CONFIG
+    work = workloads.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
+    sensors = cfg["sensors"]
+    rays = work.ray_directions.shape[0]
+    backend = CudaLidarBackend(far_plane_m=cfg["far_plane_m"], packet_size=cfg["packet"])
+    service = GaussianLidarService(backend, max_sensors=sensors, max_rays=rays, returns=cfg["returns"])
+    service.initialize(stage=None, device=device)
+    scene = work.scene_kwargs(device)
+    means = scene["means"]
+    service.load_scene(0, **scene)
+    moved = [lidar_moved_means(work.means, 100 + k).to(device) for k in range(2)]
+    dirs = work.ray_directions.to(device)
+    times = work.time_offsets_ns.to(device)
+    poses = work.sensor_to_world.to(device)
+    scene_ids = torch.zeros((sensors,), dtype=torch.int64, device=device)
+    outputs = service.render_lidar(dirs, times, poses, scene_ids)
+
+    def frame(k: int) -> None:
+        means.copy_(moved[k % 2], non_blocking=True)
+        backend.rebuild_scene(0)
+
+    for k in range(max(args.warmup, 3)):
+        frame(k)
+        service.render_lidar(dirs, times, poses, scene_ids, outputs=outputs)
+    torch.cuda.synchronize(device)
+    counters0 = backend.check_errors()
+    steps = max(args.lidar_steps, 1)
+    stream = torch.cuda.current_stream(device)
+    marks = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize(device)
+    for k in range(steps):
+        marks[k][0].record(stream)
+        frame(k + 1)
+        marks[k][1].record(stream)
+        service.render_lidar(dirs, times, poses, scene_ids, outputs=outputs)
+        marks[k][2].record(stream)
+    torch.cuda.synchronize(device)
+    counters = backend.check_errors()
+    total_ms = max_over_ranks(marks[0][0].elapsed_time(marks[-1][2]), world, device)
+    build_ms = statistics.fmean(m[0].elapsed_time(m[1]) for m in marks)
+    trace_ms = statistics.fmean(m[1].elapsed_time(m[2]) for m in marks)
+    surfels = backend.surfel_count(0)
+    traced = sensors * rays
+    value = world * traced * steps / (total_ms / 1e3)
+
+    # End to end: poses from pinned host memory, every output back to pinned host memory.
+    host_poses = work.sensor_to_world.pin_memory()
+    host_out = {k: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for k, t in outputs.items()}
+    d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+    e_steps = max(2, min(steps, 5))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(e_steps):
+        poses.copy_(host_poses, non_blocking=True)
+        frame(k)
+        service.render_lidar(dirs, times, poses, scene_ids, outputs=outputs)
+        for name, t in outputs.items():
+            host_out[name].copy_(t, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+
+    leaves = -(-surfels // cfg["packet"])
+    out_bytes = traced * (cfg["returns"] * (4 + 12 + 4 + 8 + 1 + 8) + 4)
+    trace_bytes = traced * 12 + out_bytes + surfels * (80 + 8) + max(leaves - 1, 1) * 64
+    peak, peak_kind = measured_peaks()
+    result = {
+        "metric": LIDAR_METRIC,
+        "value": round(value, 1),
+        "unit": "rays/s",
+        "steps": steps,
+        "ms_per_frame": round(total_ms / steps, 4),
+        "build_ms": round(build_ms, 4),
+        "trace_ms": round(trace_ms, 4),
+        "config": {**cfg, "rays_per_frame": traced, "planar_surfels": surfels,
+                   "returns_found_per_frame": (counters["returns"] - counters0["returns"]) // steps},
+        "e2e": {"value": round(world * traced * e_steps / (e_ms / 1e3), 1), "unit": "rays/s",
+                "h2d_bytes_per_step": host_poses.numel() * 4, "d2h_bytes_per_step": d2h, "steps": e_steps},
+        "roofline": {
+            "bound": "hbm", "kernel": "lidar_trace_kernel (+ output clear)",
+            "achieved": round(trace_bytes / (trace_ms / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(trace_bytes / (trace_ms / 1e3) / 1e9 / peak, 4),
+            "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None, "algorithmic_bytes": int(trace_bytes),
+        },
+        "node_visits_per_ray": round((counters["node_visits"] - counters0["node_visits"]) / (steps * traced), 2),
+        "leaf_tests_per_ray": round((counters["leaf_tests"] - counters0["leaf_tests"]) / (steps * traced), 2),
+        "cpu_baseline": None,
+    }
+    service.shutdown()
+    if with_cpu:
+        cpu, threads, sample = lidar_cpu_sample(work)
+        result["cpu_baseline"] = {"value": round(cpu, 1), "unit": "rays/s", "cores": threads, "kind": "port",
+                                  "sample": sample}
+    return result
 
 
 def run_b200(args) -> None:
@@ -431,6 +589,10 @@ def run_b200(args) -> None:
             "sample": f"{len(sample)} of {batch} cameras ({len(sample) * rig.height * rig.width} px), full scene, 1 render",
         }
 
+    lidar = None
+    if args.lidar_steps > 0:
+        lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -455,6 +617,7 @@ def run_b200(args) -> None:
             "cpu_baseline": cpu_baseline,
             "clocks": clocks,
             "capacity_check": {k: check[k] for k in ("visible_overflow", "intersection_overflow")},
+            "lidar": lidar,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -258,6 +258,12 @@ class CudaLidarBackend:
             raise LidarTraversalError(f"Gaussian LiDAR device errors: {errors}.")
         return counters
 
+    def surfel_count(self, scene_id: int) -> int:
+        """Planar surfels of the scene's current build (the device-computed
+        count in the acceleration header; synchronises)."""
+        accel = self._scenes[scene_id].accel
+        return int(accel[:4].view(torch.int32).item())
+
     @property
     def bvh_bytes(self) -> int:
         return sum(acc.bvh_bytes for acc in self._scenes.values())
