@@ -45,13 +45,13 @@ import torch  # noqa: E402
 
 METRIC = "Mpix/s ragged batch + fwd+bwd ms/iter, chosen vs plain form at 1e-4 RGB err"
 UNIT = "Mpix/s"
-STAGES = ("setup", "project_emit", "sort_histogram", "sort_passes", "tile_ranges", "composite")
+STAGES = ("setup", "project_emit", "tile_scan", "bucket_scatter", "tile_sort", "composite")
 KERNEL_NAMES = {
     "setup": "camera_setup_kernel",
     "project_emit": "project_emit_kernel",
-    "sort_histogram": "sort_histogram_kernel",
-    "sort_passes": "sort_onesweep_kernel",
-    "tile_ranges": "tile_ranges_kernel",
+    "tile_scan": "tile_scan_kernel",
+    "bucket_scatter": "bucket_scatter_kernel",
+    "tile_sort": "tile_sort_kernel",
     "composite": "composite_kernel",
 }
 FALLBACK_HBM_GBS = 6650.0
@@ -277,10 +277,11 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def stage_bytes(counters: dict, scene, rig, passes: int, sh_degree) -> dict[str, float]:
+def stage_bytes(counters: dict, scene, rig, tiles: int, sh_degree) -> dict[str, float]:
     """Algorithmic bytes per launch of each stage.
 
-    G Gaussians, B cameras, V visible records, I tile intersections, P pixels.
+    G Gaussians, B cameras, V visible records, I tile intersections, T tiles,
+    P pixels.
     """
     g = scene.means.shape[0]
     b = rig.viewmats.shape[0]
@@ -292,9 +293,9 @@ def stage_bytes(counters: dict, scene, rig, passes: int, sh_degree) -> dict[str,
     return {
         "setup": b * (64 + 36 + 64 + 8) + b * 56,
         "project_emit": scene_read + v * color + v * 48 + i * 12,
-        "sort_histogram": i * 8,
-        "sort_passes": passes * i * 24,
-        "tile_ranges": i * 8,
+        "tile_scan": tiles * (4 + 8),
+        "bucket_scatter": i * (12 + 8),
+        "tile_sort": i * (8 + 12),
         "composite": i * (4 + 48 + 8) + p * 28,
     }
 
@@ -551,14 +552,8 @@ def run_b200(args) -> None:
         }
 
     # Roofline of the dominant stage.
-    from vgr_b200.cuda_backend import _emitted_sort_key_end_bit  # noqa: F401
-
-    near_bits = np.float32(backend.near_plane).view(np.uint32)
-    far_bits = np.float32(backend.far_plane).view(np.uint32)
     tiles = batch * math.ceil(rig.height / config["tile_size"]) * math.ceil(rig.width / config["tile_size"])
-    key_bits = int(far_bits - near_bits).bit_length() + (tiles - 1).bit_length()
-    passes = math.ceil(key_bits / 8)
-    bytes_per_stage = stage_bytes(counters, scene, rig, passes, sh_degree)
+    bytes_per_stage = stage_bytes(counters, scene, rig, tiles, sh_degree)
     dominant = max(stage_avg, key=stage_avg.get)
     peak, peak_kind = measured_peaks()
     traffic_table = recorded_traffic(config["workload"])

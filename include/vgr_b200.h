@@ -222,9 +222,11 @@ int vgr_render(const vgr_scene* scene, const vgr_cameras* cameras,
  * caller passes inputs, outputs and the record/key/value/range/counter
  * workspace exactly as for vgr_render; workspace->scratch and scratch_bytes
  * are ignored and a VGR_STATIC_SCRATCH_BYTES array inside the library is used
- * instead (every GPU that loads the library keeps it until exit).  Renders
- * that need more scratch than that (about four million tile intersections)
- * fail with VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
+ * instead (every GPU that loads the library keeps it until exit).  The
+ * scratch grows with the projection work (8 bytes per 512 (camera, Gaussian)
+ * tasks, 64 bytes per active camera), not with the intersections: renders of
+ * more than about 2^31 tasks (e.g. 64 cameras x 16M Gaussians) fail with
+ * VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
  * the array: calls ordered on one stream are fine, calls that overlap on the
  * GPU race.  The first call on a device looks the array's address up while
  * that device is current; make it before any stream capture. */

@@ -174,3 +174,48 @@ def test_everything_culled_and_empty_tiles():
     assert torch.all(gpu.outputs["alpha"] == 0)
     assert torch.all(torch.isinf(gpu.outputs["depth"]))
     assert torch.all(gpu.outputs["semantic_id"] == -1)
+
+
+def _dense_cluster_rig():
+    eyes = torch.tensor([[0.0, 0.0, -3.0]])
+    view = look_at_viewmats(eyes, torch.zeros((1, 3)))
+    return CameraRig(view, pinhole(1, 256.0, 256.0, 64.0, 64.0), 128, 128)
+
+
+def test_buckets_above_shared_memory_capacity_bitwise():
+    # A tight cluster puts tens of thousands of keys into a handful of tiles,
+    # which the tile sort orders in chunks through global memory.
+    scene = synthetic_scene(30_000, seed=61, mean_half_extent=0.04, log_scale_mean=-5.0)
+    rig = _dense_cluster_rig()
+    gpu = render_gpu([(0, scene)], rig, [0])
+    cpu = render_oracle([(0, scene)], rig, [0], with_tiles=True)
+    assert cpu.tile_counts.max() > 4096
+    _compare(gpu, cpu)
+    assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
+
+
+def test_large_bucket_of_equal_depths_follows_gaussian_id():
+    count = 6_000
+    scene = synthetic_scene(count, seed=62, log_scale_mean=-5.5)
+    scene.means[:, :2] = (torch.rand((count, 2), generator=torch.Generator().manual_seed(3)) - 0.5) * 0.02
+    scene.means[:, 2] = 0.0
+    rig = _dense_cluster_rig()
+    gpu = render_gpu([(0, scene)], rig, [0])
+    cpu = render_oracle([(0, scene)], rig, [0], with_tiles=True)
+    assert cpu.tile_counts.max() > 4096
+    _compare(gpu, cpu)
+    assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
+
+
+def test_partial_depth_ties_in_shared_memory_buckets():
+    # Half of the Gaussians share one of three depths, the rest are spread:
+    # buckets below the shared-memory capacity take the tie re-sort.
+    count = 3_000
+    scene = synthetic_scene(count, seed=63, mean_half_extent=0.05, log_scale_mean=-5.0)
+    scene.means[::2, 2] = torch.tensor([-0.01, 0.0, 0.01]).repeat(count // 6 + 1)[: (count + 1) // 2]
+    rig = _dense_cluster_rig()
+    gpu = render_gpu([(0, scene)], rig, [0])
+    cpu = render_oracle([(0, scene)], rig, [0], with_tiles=True)
+    assert 1 < cpu.tile_counts.max() <= 4096
+    _compare(gpu, cpu)
+    assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")

@@ -40,7 +40,7 @@ def _setup():
     return device, rig, backend
 
 
-def _structs(device, rig, backend, intersection_capacity=None):
+def _structs(device, rig, backend, intersection_capacity=None, max_scene_gaussians=None):
     packed = backend._packed_scene
     ws = backend.workspace
     batch = rig.viewmats.shape[0]
@@ -77,7 +77,7 @@ def _structs(device, rig, backend, intersection_capacity=None):
         scene_offsets=packed["scene_offsets"].data_ptr(),
         scene_count=1,
         gaussian_count=packed["means"].shape[0],
-        max_scene_gaussians=packed["means"].shape[0],
+        max_scene_gaussians=max_scene_gaussians or packed["means"].shape[0],
     )
     cams = _native.VgrCameras(
         viewmats=viewmats.data_ptr(),
@@ -165,8 +165,9 @@ def test_static_scratch_matches_vgr_render_twice_in_a_row():
 def test_static_scratch_refuses_oversized_render():
     device, rig, backend = _setup()
     lib = _native.load_library()
-    # 20M intersections need ~80 MB of sort look-back descriptors.
-    structs = _structs(device, rig, backend, intersection_capacity=20_000_000)
+    # A scene bound of 2^31 - 1 Gaussians needs 4.2M projection look-back
+    # descriptors per camera, far past the 16 MiB array.
+    structs = _structs(device, rig, backend, max_scene_gaussians=2**31 - 1)
     structs[5]["counters"].fill_(-1)
     code, _ = _call(lib.vgr_render_static_scratch, device, structs)
     assert code == _native.VGR_ERR_SCRATCH_TOO_SMALL

@@ -1,0 +1,533 @@
+// Tile-bucket sort of the tile intersections and the tile ranges.
+//
+// The reference orders the 64-bit keys (global tile << 32 | float bits of
+// depth) with a host count read plus CUB DeviceRadixSort
+// (src/isaacsim_gaussian_renderer/native/renderer_cuda.cu:3215-3269), or in
+// its deterministic mode with count/scan/scatter/segmented sort
+// (:1831-1906, :1944-1971, :3288-3381), then derives the tile ranges
+// (:1908-1942).  Both produce the order (tile, depth bits, Gaussian id).
+//
+// Here the tile is never a radix digit.  The projection kernel counts each
+// tile's keys while it emits them, so after one scan of the counts every
+// tile's range [start, end) is known before any key moves:
+//   tile_scan_kernel      counts -> starts, ends (= scatter cursors), active
+//                         tile count and the bucket total;
+//   bucket_scatter_kernel one read of the emitted keys, each (depth bits,
+//                         record index) pair claims a slot of its tile's
+//                         bucket with an atomic cursor;
+//   tile_sort_kernel      one CTA per tile orders its bucket by (depth bits,
+//                         record index) - in shared memory when it holds at
+//                         most kTileSortCap pairs, else in chunks through
+//                         global memory - and writes the sorted keys and
+//                         record indices.
+// Within a tile the record index increases with the Gaussian id (records are
+// compacted in Gaussian order per camera), so (depth bits, record) is the
+// reference order, and it is a total order: the arbitrary order in which the
+// atomic cursors fill a bucket does not reach the result, and no step of the
+// tile sort needs to be stable.
+//
+// Traffic per key: 12 bytes read and 8 written by the scatter, 8 read and 12
+// written by the tile sort, against 24 bytes per radix pass (6 passes for a
+// 44-bit key at 64 cameras of 640x480) of the global sort.
+#include "../../include/vgr_b200.h"
+#include "vgr_kernels.h"
+
+namespace vgr {
+namespace {
+
+constexpr int kTsWarps = kTileSortThreads / 32;
+constexpr uint32_t kNoDigit = 0xffffu;
+static_assert(kTileSortThreads == kRadixBins, "one digit per thread in the digit scans");
+static_assert(kTileSortCap <= 65536, "ranks are packed in 16 bits");
+
+struct RankSmem {
+  uint32_t warp_hist[kTsWarps][kRadixBins];
+  uint32_t digit_start[kRadixBins];
+  uint32_t scan[kTsWarps];
+};
+
+// Digit of one LSD pass over a bucket entry (depth bits << 32 | record
+// index, so that integer order is the reference order), relative to the
+// tile's minimum of the word.
+struct PassDigit {
+  int use_record;
+  uint32_t base;
+  int shift;
+  __device__ __forceinline__ uint32_t operator()(uint64_t v) const {
+    const uint32_t word = use_record ? static_cast<uint32_t>(v) : static_cast<uint32_t>(v >> 32);
+    return ((word - base) >> shift) & (kRadixBins - 1);
+  }
+};
+
+__device__ __forceinline__ int bit_length_u32(uint32_t v) { return v ? 32 - __clz(v) : 0; }
+
+// Stable rank of one chunk of m items held warp-blocked in registers: item k
+// of lane l in warp w is chunk element (w * K + k) * 32 + l.  On return
+// warp_hist[w][d] is the count of digit d in warps < w, digit_start[d] the
+// count of digits < d, dr[k] = digit << 16 | rank among the warp's earlier
+// items of that digit, and the result is this thread's digit total.
+// warp_hist must be zero on entry.
+template <int kItems>
+__device__ __forceinline__ uint32_t rank_chunk(const uint64_t (&it)[kItems], uint32_t (&dr)[kItems],
+                                               int K, int m, PassDigit dig, RankSmem& s) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (k >= K) break;
+    const int idx = (warp * K + k) * 32 + lane;
+    const bool valid = idx < m;
+    const uint32_t d = valid ? dig(it[k]) : (kRadixBins + lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t old = 0;
+    if (valid) old = s.warp_hist[warp][d];
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) s.warp_hist[warp][d] = old + __popc(peers);
+    __syncwarp();
+    dr[k] = valid ? ((d << 16) | (old + __popc(peers & lt))) : (kNoDigit << 16);
+  }
+  __syncthreads();
+  const int d = tid;
+  uint32_t total = 0;
+#pragma unroll
+  for (int w = 0; w < kTsWarps; ++w) {
+    const uint32_t t = s.warp_hist[w][d];
+    s.warp_hist[w][d] = total;
+    total += t;
+  }
+  uint32_t incl = total;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s.scan[warp] = incl;
+  __syncthreads();
+  uint32_t wp = 0;
+#pragma unroll
+  for (int w = 0; w < kTsWarps; ++w) wp += w < warp ? s.scan[w] : 0u;
+  s.digit_start[d] = wp + incl - total;
+  __syncthreads();
+  return total;
+}
+
+// Block-wide min/max of four words; every thread gets the result.
+__device__ __forceinline__ void block_minmax(uint32_t& dmin, uint32_t& dmax, uint32_t& rmin,
+                                             uint32_t& rmax, uint32_t (*s)[kTsWarps]) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  dmin = __reduce_min_sync(0xffffffffu, dmin);
+  dmax = __reduce_max_sync(0xffffffffu, dmax);
+  rmin = __reduce_min_sync(0xffffffffu, rmin);
+  rmax = __reduce_max_sync(0xffffffffu, rmax);
+  if (lane == 0) {
+    s[0][warp] = dmin;
+    s[1][warp] = dmax;
+    s[2][warp] = rmin;
+    s[3][warp] = rmax;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int w = 0; w < kTsWarps; ++w) {
+    dmin = min(dmin, s[0][w]);
+    dmax = max(dmax, s[1][w]);
+    rmin = min(rmin, s[2][w]);
+    rmax = max(rmax, s[3][w]);
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+// One CTA: counts -> exclusive starts, cursors, active tiles, bucket total.
+__global__ void __launch_bounds__(kTileScanThreads) tile_scan_kernel(BucketParams p) {
+  __shared__ uint32_t s_warp[kTileScanThreads / 32];
+  __shared__ uint32_t s_carry;
+  __shared__ uint32_t s_active;
+  ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  if (tid == 0) {
+    s_carry = 0;
+    s_active = 0;
+  }
+  __syncthreads();
+  const uint32_t* counts = reinterpret_cast<const uint32_t*>(p.tile_ends);
+  const int64_t tiles = p.tile_count;
+  uint32_t active = 0;
+  for (int64_t base = 0; base < tiles; base += kTileScanThreads * kTileScanItems) {
+    const int64_t first = base + static_cast<int64_t>(tid) * kTileScanItems;
+    uint32_t c[kTileScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kTileScanItems; ++k) {
+      c[k] = first + k < tiles ? counts[first + k] : 0u;
+      sum += c[k];
+      active += c[k] != 0u ? 1u : 0u;
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t v = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+      }
+      s_warp[lane] = v;
+    }
+    __syncthreads();
+    uint32_t prefix = s_carry + (warp > 0 ? s_warp[warp - 1] : 0u) + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kTileScanItems; ++k) {
+      if (first + k < tiles) {
+        p.tile_starts[first + k] = static_cast<int32_t>(prefix);
+        p.tile_ends[first + k] = static_cast<int32_t>(prefix);
+      }
+      prefix += c[k];
+    }
+    __syncthreads();
+    if (tid == kTileScanThreads - 1) s_carry = prefix;
+    __syncthreads();
+  }
+  active = __reduce_add_sync(0xffffffffu, active);
+  if (lane == 0 && active) atomicAdd(&s_active, active);
+  __syncthreads();
+  if (tid == 0) {
+    header->bucket_total = s_carry;
+    p.counters[VGR_COUNTER_ACTIVE_TILES] = static_cast<int64_t>(s_active);
+  }
+}
+
+// Each emitted key claims a slot in its tile's bucket; keys whose tile is out
+// of range (records past the visible capacity) go after the buckets.  A
+// thread claims the slots of kBatch keys before it stores any of them, so
+// its cursor atomics are in flight together.
+__global__ void __launch_bounds__(256) bucket_scatter_kernel(BucketParams p) {
+  constexpr int kBatch = 8;
+  ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
+  int64_t n = p.counters[1];
+  if (n > p.capacity) n = p.capacity;
+  if (n < 0) n = 0;
+  const uint32_t bucket_total = header->bucket_total;
+  uint32_t* cursors = reinterpret_cast<uint32_t*>(p.tile_ends);
+  const uint64_t tiles = static_cast<uint64_t>(p.tile_count);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * kBatch;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x * kBatch + threadIdx.x; base < n;
+       base += stride) {
+    uint64_t key[kBatch];
+    int32_t value[kBatch];
+    uint64_t pos[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int64_t i = base + b * static_cast<int64_t>(blockDim.x);
+      key[b] = i < n ? p.keys_in[i] : ~0ull;
+      value[b] = i < n ? p.values_in[i] : 0;
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int64_t i = base + b * static_cast<int64_t>(blockDim.x);
+      const uint64_t tile = key[b] >> 32;
+      pos[b] = ~0ull;
+      if (i < n) {
+        pos[b] = tile < tiles
+                     ? static_cast<uint64_t>(atomicAdd(cursors + tile, 1u))
+                     : static_cast<uint64_t>(bucket_total) + atomicAdd(&header->tail_cursor, 1u);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      if (pos[b] >= static_cast<uint64_t>(n)) continue;
+      if ((key[b] >> 32) < tiles) {
+        p.keys_out[pos[b]] = (key[b] << 32) | static_cast<uint32_t>(value[b]);
+      } else {
+        p.keys_out[pos[b]] = ~0ull;
+        p.values_out[pos[b]] = value[b];
+      }
+    }
+  }
+}
+
+// One CTA per tile: order the bucket by (depth bits, record index).
+//
+// Buckets of at most kTileSortCap entries stay in shared memory.  The common
+// path splits them by the top kSplitBits bits of the tile's depth range with
+// shared-memory counters (any order within a split is fine: every split is
+// then insertion-sorted by the full 64-bit entry by the thread that owns it),
+// which costs one pass and a handful of barriers.  A bucket whose largest
+// split exceeds kMaxSplit (many equal or nearly equal depths) is sorted by
+// stable LSD passes over the record word and then the depth word instead;
+// so is every bucket above kTileSortCap, in chunks through global memory.
+__global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketParams p) {
+  constexpr int kSplitBits = 11;
+  constexpr int kSplits = 1 << kSplitBits;
+  constexpr int kSplitsPerThread = kSplits / kTileSortThreads;
+  constexpr uint32_t kMaxSplit = 48;
+  static_assert(kSplitsPerThread == 8, "two uint4 loads of split counters per thread");
+  __shared__ __align__(16) uint64_t s_items[kTileSortCap];
+  __shared__ __align__(16) union {
+    RankSmem rank;
+    uint32_t split[kSplits];
+  } s_u;
+  __shared__ uint32_t s_base[kRadixBins];
+  __shared__ uint32_t s_minmax[4][kTsWarps];
+  __shared__ uint32_t s_scan[kTsWarps];
+  __shared__ uint32_t s_big[kTsWarps];
+
+  const int64_t tile = blockIdx.x;
+  const int64_t start = p.tile_starts[tile];
+  const int64_t end = p.tile_ends[tile];
+  if (start < 0 || end > p.capacity || end - start <= 0) return;
+  const int n = static_cast<int>(end - start);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const uint64_t key_tile = static_cast<uint64_t>(tile) << 32;
+  uint64_t* bucket = p.keys_out + start;
+
+  if (n == 1) {
+    if (tid == 0) {
+      const uint64_t v = bucket[0];
+      p.keys_out[start] = key_tile | (v >> 32);
+      p.values_out[start] = static_cast<int32_t>(static_cast<uint32_t>(v));
+    }
+    return;
+  }
+
+  uint64_t it[kTileSortItems];
+  uint32_t dr[kTileSortItems];
+  uint32_t dmin = 0xffffffffu, dmax = 0u, rmin = 0xffffffffu, rmax = 0u;
+
+  if (n <= kTileSortCap) {
+    // ------------------------------------------------ split + insertion sort
+    const int K = (n + kTileSortThreads - 1) / kTileSortThreads;
+#pragma unroll
+    for (int k = 0; k < kTileSortItems; ++k) {
+      if (k >= K) break;
+      const int i = k * kTileSortThreads + tid;
+      if (i < n) {
+        it[k] = bucket[i];
+        const uint32_t dw = static_cast<uint32_t>(it[k] >> 32);
+        const uint32_t rw = static_cast<uint32_t>(it[k]);
+        dmin = min(dmin, dw);
+        dmax = max(dmax, dw);
+        rmin = min(rmin, rw);
+        rmax = max(rmax, rw);
+      }
+    }
+    for (int b = tid; b < kSplits; b += kTileSortThreads) s_u.split[b] = 0u;
+    block_minmax(dmin, dmax, rmin, rmax, s_minmax);
+    const int range_bits = bit_length_u32(dmax - dmin);
+    const int shift = range_bits > kSplitBits ? range_bits - kSplitBits : 0;
+#pragma unroll
+    for (int k = 0; k < kTileSortItems; ++k) {
+      if (k >= K) break;
+      if (k * kTileSortThreads + tid < n) {
+        const uint32_t sp = (static_cast<uint32_t>(it[k] >> 32) - dmin) >> shift;
+        dr[k] = (sp << 16) | atomicAdd(&s_u.split[sp], 1u);
+      }
+    }
+    __syncthreads();
+    // Exclusive offsets of the splits in place; thread t owns splits
+    // [8t, 8t + 8).  Also the largest split.
+    uint32_t c[kSplitsPerThread];
+    {
+      const uint4 lo = reinterpret_cast<const uint4*>(s_u.split)[tid * 2];
+      const uint4 hi = reinterpret_cast<const uint4*>(s_u.split)[tid * 2 + 1];
+      c[0] = lo.x; c[1] = lo.y; c[2] = lo.z; c[3] = lo.w;
+      c[4] = hi.x; c[5] = hi.y; c[6] = hi.z; c[7] = hi.w;
+    }
+    uint32_t sum = 0, big = 0;
+#pragma unroll
+    for (int j = 0; j < kSplitsPerThread; ++j) {
+      sum += c[j];
+      big = max(big, c[j]);
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    big = __reduce_max_sync(0xffffffffu, big);
+    if (lane == 31) s_scan[warp] = incl;
+    if (lane == 0) s_big[warp] = big;
+    __syncthreads();
+    uint32_t prefix = incl - sum;
+#pragma unroll
+    for (int w = 0; w < kTsWarps; ++w) {
+      prefix += w < warp ? s_scan[w] : 0u;
+      big = max(big, s_big[w]);
+    }
+    if (big <= kMaxSplit) {
+      uint32_t off[kSplitsPerThread];
+#pragma unroll
+      for (int j = 0; j < kSplitsPerThread; ++j) {
+        off[j] = prefix;
+        prefix += c[j];
+      }
+      __syncthreads();  // every thread has read its counters
+      reinterpret_cast<uint4*>(s_u.split)[tid * 2] = make_uint4(off[0], off[1], off[2], off[3]);
+      reinterpret_cast<uint4*>(s_u.split)[tid * 2 + 1] = make_uint4(off[4], off[5], off[6], off[7]);
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kTileSortItems; ++k) {
+        if (k >= K) break;
+        if (k * kTileSortThreads + tid < n) {
+          s_items[s_u.split[dr[k] >> 16] + (dr[k] & 0xffffu)] = it[k];
+        }
+      }
+      __syncthreads();
+      // Insertion sort of the owned splits by the full entry.
+#pragma unroll
+      for (int j = 0; j < kSplitsPerThread; ++j) {
+        const int split = tid * kSplitsPerThread + j;
+        const int lo = static_cast<int>(s_u.split[split]);
+        const int hi = split + 1 < kSplits ? static_cast<int>(s_u.split[split + 1]) : n;
+        for (int a = lo + 1; a < hi; ++a) {
+          const uint64_t v = s_items[a];
+          int b = a - 1;
+          while (b >= lo && s_items[b] > v) {
+            s_items[b + 1] = s_items[b];
+            --b;
+          }
+          s_items[b + 1] = v;
+        }
+      }
+      __syncthreads();
+    } else {
+      // ------------------------------------------- stable LSD in shared memory
+      // Items are re-read warp-blocked (element (w * K + k) * 32 + l) for the
+      // stable ranking.
+      __syncthreads();  // the split counters share storage with the rank state
+      for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
+        (&s_u.rank.warp_hist[0][0])[i] = 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < kTileSortItems; ++k) {
+        if (k >= K) break;
+        const int idx = (warp * K + k) * 32 + lane;
+        if (idx < n) it[k] = bucket[idx];
+      }
+      __syncthreads();
+      const int passes_d = (range_bits + kRadixBits - 1) / kRadixBits;
+      const int passes_r = (bit_length_u32(rmax - rmin) + kRadixBits - 1) / kRadixBits;
+      for (int q = 0; q < passes_r + passes_d; ++q) {
+        const PassDigit dig = q < passes_r ? PassDigit{1, rmin, q * kRadixBits}
+                                           : PassDigit{0, dmin, (q - passes_r) * kRadixBits};
+        rank_chunk(it, dr, K, n, dig, s_u.rank);
+#pragma unroll
+        for (int k = 0; k < kTileSortItems; ++k) {
+          if (k >= K) break;
+          const uint32_t d = dr[k] >> 16;
+          if (d != kNoDigit) {
+            s_items[s_u.rank.digit_start[d] + s_u.rank.warp_hist[warp][d] + (dr[k] & 0xffffu)] = it[k];
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kTileSortItems; ++k) {
+          if (k >= K) break;
+          const int idx = (warp * K + k) * 32 + lane;
+          if (idx < n) it[k] = s_items[idx];
+        }
+#pragma unroll
+        for (int w = 0; w < kTsWarps; ++w) s_u.rank.warp_hist[w][tid] = 0u;
+        __syncthreads();
+      }
+    }
+    for (int i = tid; i < n; i += kTileSortThreads) {
+      const uint64_t v = s_items[i];
+      p.keys_out[start + i] = key_tile | (v >> 32);
+      p.values_out[start + i] = static_cast<int32_t>(static_cast<uint32_t>(v));
+    }
+    return;
+  }
+
+  // ------------------------------------------------------------ large buckets
+  // Stable chunked LSD over the full entry through global memory,
+  // ping-ponging between the bucket and the same range of the temp buffer.
+  constexpr int kChunkItems = 8;
+  constexpr int kChunk = kTileSortThreads * kChunkItems;
+  for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
+    (&s_u.rank.warp_hist[0][0])[i] = 0u;
+  }
+  for (int i = tid; i < n; i += kTileSortThreads) {
+    const uint64_t v = bucket[i];
+    const uint32_t dw = static_cast<uint32_t>(v >> 32);
+    const uint32_t rw = static_cast<uint32_t>(v);
+    dmin = min(dmin, dw);
+    dmax = max(dmax, dw);
+    rmin = min(rmin, rw);
+    rmax = max(rmax, rw);
+  }
+  block_minmax(dmin, dmax, rmin, rmax, s_minmax);
+  const int passes_d = (bit_length_u32(dmax - dmin) + kRadixBits - 1) / kRadixBits;
+  const int passes_r = (bit_length_u32(rmax - rmin) + kRadixBits - 1) / kRadixBits;
+  uint64_t* src = bucket;
+  uint64_t* dst = p.temp + start;
+  for (int q = 0; q < passes_r + passes_d; ++q) {
+    const PassDigit dig = q < passes_r ? PassDigit{1, rmin, q * kRadixBits}
+                                       : PassDigit{0, dmin, (q - passes_r) * kRadixBits};
+    s_base[tid] = 0u;
+    __syncthreads();
+    for (int i = tid; i < n; i += kTileSortThreads) atomicAdd(&s_base[dig(src[i])], 1u);
+    __syncthreads();
+    {
+      const uint32_t v = s_base[tid];
+      uint32_t incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) s_scan[warp] = incl;
+      __syncthreads();
+      uint32_t wp = 0;
+#pragma unroll
+      for (int w = 0; w < kTsWarps; ++w) wp += w < warp ? s_scan[w] : 0u;
+      s_base[tid] = wp + incl - v;
+      __syncthreads();
+    }
+    for (int cb = 0; cb < n; cb += kChunk) {
+      const int m = n - cb < kChunk ? n - cb : kChunk;
+      uint64_t ci[kChunkItems];
+      uint32_t cr[kChunkItems];
+#pragma unroll
+      for (int k = 0; k < kChunkItems; ++k) {
+        const int idx = (warp * kChunkItems + k) * 32 + lane;
+        ci[k] = idx < m ? src[cb + idx] : 0ull;
+      }
+      const uint32_t total = rank_chunk(ci, cr, kChunkItems, m, dig, s_u.rank);
+#pragma unroll
+      for (int k = 0; k < kChunkItems; ++k) {
+        const uint32_t d = cr[k] >> 16;
+        if (d != kNoDigit) dst[s_base[d] + s_u.rank.warp_hist[warp][d] + (cr[k] & 0xffffu)] = ci[k];
+      }
+      __syncthreads();
+      s_base[tid] += total;
+#pragma unroll
+      for (int w = 0; w < kTsWarps; ++w) s_u.rank.warp_hist[w][tid] = 0u;
+      __syncthreads();
+    }
+    uint64_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  for (int i = tid; i < n; i += kTileSortThreads) {
+    const uint64_t v = src[i];
+    p.keys_out[start + i] = key_tile | (v >> 32);
+    p.values_out[start + i] = static_cast<int32_t>(static_cast<uint32_t>(v));
+  }
+}
+
+}  // namespace vgr

@@ -8,8 +8,9 @@
 // records and their tile intersections in task order through a decoupled
 // look-back prefix (so the visible list and the key list are deterministic,
 // ascending Gaussian id within each camera), and emits the keys cooperatively
-// from shared memory so every store is coalesced.  There is no host round
-// trip: the emitted count stays on the device for the sort.
+// from shared memory so every store is coalesced, counting each tile's keys
+// for the bucket sort.  There is no host round trip: the emitted count stays
+// on the device for the sort.
 #include "vgr_camera.cuh"
 #include "vgr_kernels.h"
 
@@ -435,13 +436,6 @@ __global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(Projec
   const int lane = tid & 31;
   const int warp = tid >> 5;
 
-  // Clear the tile ranges of this frame (written later by the range kernel).
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; i < p.tile_count;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    p.tile_starts[i] = 0;
-    p.tile_ends[i] = 0;
-  }
-
   const int64_t total_vblocks = p.total_vblocks;
   while (true) {
     if (tid == 0) s_vblock = atomicAdd(&header->project_queue, 1u);
@@ -676,6 +670,10 @@ __global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(Projec
                                 static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
           key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[s_slot[i]].b.z));
           value = static_cast<int32_t>(r);
+          // Bucket size for the tile sort (a tile past the batch's range - a
+          // caller's inconsistent ragged offsets - is left to the scatter's
+          // overflow tail).
+          if (tile < static_cast<uint64_t>(p.tile_count)) atomicAdd(p.tile_counts + tile, 1u);
         }
         p.keys[base_isect + j] = key;
         p.values[base_isect + j] = value;

@@ -1,20 +1,15 @@
-// Device-bounded stable LSD radix sort of the tile-intersection keys, and the
-// tile-range pass.
+// Device-bounded stable LSD radix sort (onesweep) of 64-bit keys with int32
+// values, used by the LBVH build to order surfels along the Morton curve.
 //
-// Replaces the reference's host count read plus CUB DeviceRadixSort
-// (src/isaacsim_gaussian_renderer/native/renderer_cuda.cu:3215-3269) and its
-// deterministic count/scan/scatter/segmented-sort path (:1831-1906,
-// :1944-1971, :3288-3381).  The emitted count is read on the device, so the
-// frame has no host synchronisation and can be captured in a CUDA graph.
-// Keys are sorted on the composite (tile, depth_bits - near_bits) digits
-// (see SortKeyMap) with one upfront histogram launch for all passes and one
-// onesweep launch per 8-bit digit: each partition of kSortTile keys ranks its
-// keys stably with warp match/ballot, publishes per-digit counts, resolves
-// its global offsets by decoupled look-back over earlier partitions and
-// scatters through shared memory so that stores are coalesced.  Because the
-// emitter writes keys in ascending Gaussian id within each camera and every
-// pass is stable, the result is the reference's deterministic order
-// (tile, depth bits, Gaussian id) in both of its modes.
+// The emitted count is read on the device, so a sort needs no host
+// synchronisation and can be captured in a CUDA graph.  One histogram launch
+// covers every pass; each onesweep launch handles one 8-bit digit: a
+// partition of kSortTile keys ranks its keys stably with warp match/ballot,
+// publishes per-digit counts, resolves its global offsets by decoupled
+// look-back over earlier partitions and scatters through shared memory so
+// that stores are coalesced.  Keys are either used as they are
+// (SortKeyMap.raw) or mapped to the composite (tile, depth_bits - near_bits)
+// digits of the tile-intersection keys.
 #include "vgr_kernels.h"
 
 namespace vgr {
@@ -221,33 +216,6 @@ __global__ void __launch_bounds__(kSortThreads, 3) sort_onesweep_kernel(SortPara
       }
     }
     __syncthreads();
-  }
-}
-
-// Tile [start, end) ranges from the sorted keys (renderer_cuda.cu:1908-1942).
-__global__ void __launch_bounds__(256) tile_ranges_kernel(RangeParams p) {
-  int64_t n = p.counters[1];
-  if (n > p.capacity) n = p.capacity;
-  if (n < 0) n = 0;
-  uint32_t local_active = 0;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t tile = static_cast<int64_t>(p.keys[i] >> 32);
-    if (tile >= p.tile_count) continue;
-    const bool begins = i == 0 || static_cast<int64_t>(p.keys[i - 1] >> 32) != tile;
-    const bool ends = i + 1 == n || static_cast<int64_t>(p.keys[i + 1] >> 32) != tile;
-    if (begins) p.tile_starts[tile] = static_cast<int32_t>(i);
-    if (ends) {
-      p.tile_ends[tile] = static_cast<int32_t>(i + 1);
-      ++local_active;
-    }
-  }
-  // Warp-aggregated active-tile count.
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) local_active += __shfl_xor_sync(0xffffffffu, local_active, o);
-  if ((threadIdx.x & 31) == 0 && local_active) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(p.active_tiles),
-              static_cast<unsigned long long>(local_active));
   }
 }
 

@@ -27,24 +27,8 @@ struct OccupancyCache {
   int device = -1;
   int sms = 0;
   int project_blocks = 0;
-  int sort_blocks = 0;
 };
 thread_local OccupancyCache g_occ;
-
-int bit_length(uint64_t v) {
-  int bits = 0;
-  while (v) {
-    ++bits;
-    v >>= 1;
-  }
-  return bits;
-}
-
-uint32_t float_bits(float f) {
-  uint32_t u;
-  std::memcpy(&u, &f, 4);
-  return u;
-}
 
 }  // namespace
 
@@ -78,12 +62,11 @@ int device_sms(int* sms) {
     }
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3>,
                                                   kProjectThreads, 0);
+    // The onesweep partition (LBVH Morton sort) needs more than the default
+    // 48 KB of dynamic shared memory.
     cudaFuncSetAttribute(sort_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kSortDynamicSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.sort_blocks, sort_onesweep_kernel,
-                                                  kSortThreads, kSortDynamicSmem);
     if (g_occ.project_blocks < 1) g_occ.project_blocks = 1;
-    if (g_occ.sort_blocks < 1) g_occ.sort_blocks = 1;
     cudaGetLastError();
   }
   *sms = g_occ.sms;
@@ -114,7 +97,7 @@ extern "C" int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
   }
   const int64_t vblocks = (max_projection_tasks + kProjectChunk - 1) / kProjectChunk +
                           max_active_cameras;
-  return make_scratch_layout(intersection_capacity, max_active_cameras, vblocks).total;
+  return make_scratch_layout(intersection_capacity, max_active_cameras, vblocks, false).total;
 }
 
 // Scratch for a drop-in caller that only knows (items, segments): active
@@ -346,7 +329,7 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
   }
 
   const int64_t vblocks = render_vblocks(active, scene->max_scene_gaussians);
-  const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, vblocks);
+  const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, vblocks, false);
   if (ws->scratch_bytes < layout.total) {
     return fail(VGR_ERR_SCRATCH_TOO_SMALL,
                 "render scratch holds %lld bytes but this batch needs %lld",
@@ -355,17 +338,6 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
 
   const float near_f = static_cast<float>(opt->near_plane);
   const float far_f = static_cast<float>(opt->far_plane);
-  SortKeyMap map{};
-  map.near_bits = float_bits(near_f);
-  map.depth_bits = static_cast<uint32_t>(bit_length(float_bits(far_f) - map.near_bits));
-  map.tile_count = static_cast<uint32_t>(global_tiles);
-  const int tile_bits = global_tiles > 1 ? bit_length(static_cast<uint64_t>(global_tiles - 1)) : 0;
-  map.total_bits = map.depth_bits + static_cast<uint32_t>(tile_bits);
-  const int passes = static_cast<int>((map.total_bits + kRadixBits - 1) / kRadixBits);
-  if (passes > kMaxSortPasses || passes < 1) {
-    return fail(VGR_ERR_UNSUPPORTED, "sort key of %u bits exceeds the %d-pass limit",
-                map.total_bits, kMaxSortPasses);
-  }
 
   int sms = 0;
   int rc = device_sms(&sms);
@@ -386,6 +358,10 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     if (cudaMemsetAsync(scratch + layout.project_desc, 0, static_cast<size_t>(vblocks) * 8, stream) !=
         cudaSuccess) {
       return check_launch("render: clear projection descriptors", 0);
+    }
+    if (global_tiles > 0 &&
+        cudaMemsetAsync(ws->tile_ends, 0, static_cast<size_t>(global_tiles) * 4, stream) != cudaSuccess) {
+      return check_launch("render: clear tile counts", 0);
     }
     SetupParams sp{};
     sp.scratch = scratch;
@@ -436,8 +412,7 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     pp.keys = ws->keys_in;
     pp.values = ws->values_in;
     pp.intersection_capacity = ws->intersection_capacity;
-    pp.tile_starts = ws->tile_starts;
-    pp.tile_ends = ws->tile_ends;
+    pp.tile_counts = reinterpret_cast<uint32_t*>(ws->tile_ends);
     pp.tile_count = global_tiles;
     pp.counters = ws->counters;
     pp.mirror_means2d = ws->visible_means2d;
@@ -464,55 +439,32 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     if ((rc = check_launch("render: projection")) != VGR_OK) return rc;
     mark(2);
 
-    SortParams so{};
-    so.scratch = scratch;
-    so.layout = layout;
-    so.counters = ws->counters;
-    so.capacity = ws->intersection_capacity;
-    so.map = map;
-    so.passes = passes;
-    int64_t hgrid = static_cast<int64_t>(sms) * 4;
-    if (hgrid > layout.max_partitions) hgrid = layout.max_partitions;
-    if (hgrid < 1) hgrid = 1;
-    so.keys_in = ws->keys_in;
-    sort_histogram_kernel<<<static_cast<unsigned>(hgrid), kSortThreads, 0, stream>>>(so);
-    if ((rc = check_launch("render: sort histogram")) != VGR_OK) return rc;
+    BucketParams bp{};
+    bp.scratch = scratch;
+    bp.layout = layout;
+    bp.counters = ws->counters;
+    bp.capacity = ws->intersection_capacity;
+    bp.tile_count = global_tiles;
+    bp.keys_in = ws->keys_in;
+    bp.values_in = ws->values_in;
+    bp.keys_out = ws->keys_out;
+    bp.values_out = ws->values_out;
+    bp.temp = ws->keys_in;
+    bp.tile_starts = ws->tile_starts;
+    bp.tile_ends = ws->tile_ends;
+    tile_scan_kernel<<<1, kTileScanThreads, 0, stream>>>(bp);
+    if ((rc = check_launch("render: tile scan")) != VGR_OK) return rc;
     mark(3);
-    int64_t sgrid = static_cast<int64_t>(sms) * g_occ.sort_blocks;
-    if (sgrid > layout.max_partitions) sgrid = layout.max_partitions;
+    int64_t sgrid = (ws->intersection_capacity + 2047) / 2048;
+    if (sgrid > static_cast<int64_t>(sms) * 8) sgrid = static_cast<int64_t>(sms) * 8;
     if (sgrid < 1) sgrid = 1;
-    uint64_t* kin = ws->keys_in;
-    uint64_t* kout = ws->keys_out;
-    int32_t* vin = ws->values_in;
-    int32_t* vout = ws->values_out;
-    for (int pass = 0; pass < passes; ++pass) {
-      so.pass = pass;
-      so.keys_in = kin;
-      so.values_in = vin;
-      so.keys_out = kout;
-      so.values_out = vout;
-      sort_onesweep_kernel<<<static_cast<unsigned>(sgrid), kSortThreads, kSortDynamicSmem, stream>>>(
-          so);
-      if ((rc = check_launch("render: sort pass")) != VGR_OK) return rc;
-      uint64_t* tk = kin; kin = kout; kout = tk;
-      int32_t* tv = vin; vin = vout; vout = tv;
-    }
-    selector = passes & 1;
+    bucket_scatter_kernel<<<static_cast<unsigned>(sgrid), 256, 0, stream>>>(bp);
+    if ((rc = check_launch("render: bucket scatter")) != VGR_OK) return rc;
     mark(4);
-    sorted_values = vin;
-
-    RangeParams rp{};
-    rp.counters = ws->counters;
-    rp.capacity = ws->intersection_capacity;
-    rp.keys = kin;
-    rp.tile_count = global_tiles;
-    rp.tile_starts = ws->tile_starts;
-    rp.tile_ends = ws->tile_ends;
-    rp.active_tiles = ws->counters + VGR_COUNTER_ACTIVE_TILES;
-    int64_t rgrid = (ws->intersection_capacity + 255) / 256;
-    if (rgrid > static_cast<int64_t>(sms) * 8) rgrid = static_cast<int64_t>(sms) * 8;
-    tile_ranges_kernel<<<static_cast<unsigned>(rgrid), 256, 0, stream>>>(rp);
-    if ((rc = check_launch("render: tile ranges")) != VGR_OK) return rc;
+    tile_sort_kernel<<<static_cast<unsigned>(global_tiles), kTileSortThreads, 0, stream>>>(bp);
+    if ((rc = check_launch("render: tile sort")) != VGR_OK) return rc;
+    selector = 1;
+    sorted_values = ws->values_out;
     mark(5);
   }
 

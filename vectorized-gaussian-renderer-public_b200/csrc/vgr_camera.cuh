@@ -38,7 +38,9 @@ struct ScratchHeader {
   uint32_t composite_queue;    // work-item ticket of the persistent compositor
   uint32_t sort_queue[8];      // partition ticket per radix pass
   uint32_t ranges_done;
-  uint32_t pad1[19];
+  uint32_t bucket_total;       // keys placed in tile buckets (tile_scan_kernel)
+  uint32_t tail_cursor;        // overflow-sentinel keys placed after the buckets
+  uint32_t pad1[17];
 };
 static_assert(sizeof(ScratchHeader) == 128, "ScratchHeader layout");
 
@@ -54,6 +56,15 @@ constexpr int kRadixBins = 1 << kRadixBits;
 // Dynamic shared memory of one onesweep CTA: the partition's keys and values.
 constexpr int kSortDynamicSmem = kSortTile * (8 + 4);
 constexpr int kMaxSortPasses = 8;
+
+// Tile-bucket sort: one CTA per tile orders the tile's (depth, record) pairs
+// in shared memory when they fit (kTileSortCap), else in chunks through global
+// memory.
+constexpr int kTileSortThreads = 256;
+constexpr int kTileSortItems = 12;
+constexpr int kTileSortCap = kTileSortThreads * kTileSortItems;
+constexpr int kTileScanThreads = 1024;
+constexpr int kTileScanItems = 16;
 
 // Projection look-back descriptor: flag (2 bits) | visible (31) | isects (31).
 constexpr uint64_t kDescAggregate = 1ull << 62;
@@ -77,9 +88,12 @@ struct ScratchLayout {
   int64_t max_partitions;
 };
 
+// onesweep_descriptors: reserve the per-partition look-back descriptors of
+// the global onesweep sort (the LBVH Morton sort); the camera path sorts in
+// tile buckets and needs none.
 __host__ __device__ inline ScratchLayout make_scratch_layout(
     int64_t intersection_capacity, int64_t max_active_cameras,
-    int64_t max_vblocks) {
+    int64_t max_vblocks, bool onesweep_descriptors) {
   ScratchLayout l{};
   int64_t off = 0;
   l.header = off;
@@ -94,7 +108,8 @@ __host__ __device__ inline ScratchLayout make_scratch_layout(
   l.sort_hist = off;
   off = align_up(off + kMaxSortPasses * kRadixBins * 4, 256);
   l.sort_desc = off;
-  l.max_partitions = (intersection_capacity + kSortTile - 1) / kSortTile;
+  l.max_partitions =
+      onesweep_descriptors ? (intersection_capacity + kSortTile - 1) / kSortTile : 0;
   off = align_up(off + static_cast<int64_t>(kMaxSortPasses) * l.max_partitions * kRadixBins * 8, 256);
   l.total = off;
   return l;

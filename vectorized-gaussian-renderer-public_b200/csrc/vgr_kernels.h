@@ -53,8 +53,7 @@ struct ProjectParams {
   uint64_t* keys;
   int32_t* values;
   int64_t intersection_capacity;
-  int32_t* tile_starts;
-  int32_t* tile_ends;
+  uint32_t* tile_counts;       // per-tile key counts (zeroed before the launch)
   int64_t tile_count;
   int64_t* counters;
   float* mirror_means2d;
@@ -80,14 +79,22 @@ struct SortParams {
   int32_t* values_out;
 };
 
-struct RangeParams {
-  const int64_t* counters;
-  int64_t capacity;
-  const uint64_t* keys;
-  int64_t tile_count;
+
+// Tile-bucket sort of the emitted intersections.  tile_ends holds per-tile
+// key counts after projection, then scatter cursors, then range ends.
+struct BucketParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  int64_t* counters;           // [1] emitted keys in, [4] active tiles out
+  int64_t capacity;            // intersection capacity
+  int64_t tile_count;          // global tiles
+  const uint64_t* keys_in;     // emission order: tile << 32 | depth bits
+  const int32_t* values_in;    // record index per key
+  uint64_t* keys_out;          // bucketed (depth bits | record << 32), then sorted keys
+  int32_t* values_out;         // sorted record indices
+  uint64_t* temp;              // ping-pong space for tiles above kTileSortCap
   int32_t* tile_starts;
   int32_t* tile_ends;
-  int64_t* active_tiles;
 };
 
 struct CompositeParams {
@@ -113,7 +120,9 @@ template <int kShDegree>
 __global__ void project_emit_kernel(ProjectParams p);
 __global__ void sort_histogram_kernel(SortParams p);
 __global__ void sort_onesweep_kernel(SortParams p);
-__global__ void tile_ranges_kernel(RangeParams p);
+__global__ void tile_scan_kernel(BucketParams p);
+__global__ void bucket_scatter_kernel(BucketParams p);
+__global__ void tile_sort_kernel(BucketParams p);
 template <int kTile, bool kFull>
 __global__ void composite_kernel(CompositeParams p);
 

@@ -8,19 +8,20 @@
 // being captured into a CUDA graph, where a fresh cudaMalloc is not an
 // operation the capture can record.  Such a caller can still hand over the
 // buffers it already owns (inputs, outputs and the record/key/value/range
-// workspace), but has nowhere to get the look-back descriptors, digit
-// histograms and per-camera plans from.  Those fit in a fixed array that the
-// library carries itself.
+// workspace), but has nowhere to get the projection look-back descriptors,
+// queue tickets and per-camera plans from.  Those fit in a fixed array that
+// the library carries itself.
 //
 // Limits and rules:
 //  * The array is VGR_STATIC_SCRATCH_BYTES (16 MiB).  Every GPU on which the
-//    library is loaded holds it until the process exits.  A render whose
-//    scratch would exceed it (roughly more than four million tile
-//    intersections, or very large camera/Gaussian task counts) is rejected
-//    with VGR_ERR_SCRATCH_TOO_SMALL before anything is launched.
+//    library is loaded holds it until the process exits.  The scratch grows
+//    with the projection tasks (8 bytes per 512 (camera, Gaussian) pairs) and
+//    the active cameras, not with the intersections; a render past about 2^31
+//    tasks is rejected with VGR_ERR_SCRATCH_TOO_SMALL before anything is
+//    launched.
 //  * Every call on a device shares the one array, and it keeps the previous
 //    call's contents.  vgr_render clears everything that must start at zero
-//    (counters, queue tickets, histograms, look-back descriptors) on the
+//    (counters, queue tickets, tile counts, look-back descriptors) on the
 //    stream, so back-to-back calls on one stream are correct; calls whose
 //    work overlaps on the GPU (different streams, or different host threads
 //    without ordering) race on the array and produce wrong results.
