@@ -16,7 +16,8 @@
 // footprint touches; each warp walks only its records with __ballot_sync
 // over the masks, skips exp beyond a per-record quadratic-form bound, and
 // retires once all of its pixels have terminated; the CTA stops staging when
-// __syncthreads_count reports no live pixel.
+// __syncthreads_count reports no live pixel.  The semantic label is resolved
+// once per pixel at the end from the sorted position of its largest weight.
 #include "vgr_kernels.h"
 
 namespace vgr {
@@ -35,31 +36,35 @@ struct CompositeGeometry {
 
 constexpr int kCompositeBatch = 256;
 
+// Per-pixel accumulation.  A pixel that terminates gets a NaN row coordinate,
+// so every later power evaluates to NaN and fails the range test: the hot
+// path never tests `done`, which only drives the warp and CTA exits.
 struct PixelState {
   float transmittance;
   float r, g, b, depth;
   float best_weight;
-  int64_t best_semantic;
+  int32_t best_pos;  // sorted position of the largest single weight
   bool done;
 };
 
+// One record on one pixel.  power = -q/2 evaluated from conic terms scaled by
+// -1/2 (exact: scaling by a power of two commutes with rounding), lo =
+// max(-qmax/2, -20) merges the conservative q bound with the reference's
+// power >= -20 cut, so the test below is the reference's
+// `power <= 0 && power >= -20` restricted to records that can reach 1/255.
 template <bool kFull>
-__device__ __forceinline__ void blend(PixelState& s, float q, float qmax, int j,
-                                      const float4* s_cqo, const float4* s_col,
-                                      const int64_t* s_sem) {
-  if (s.done || !(q <= qmax)) return;
-  const float power = fmul(-0.5f, q);
-  if (power > 0.0f || power < -20.0f) return;
-  const float4 cqo = s_cqo[j];
-  const float alpha = fminf(kMaxAlpha, fmul(cqo.z, vexp(power)));
+__device__ __forceinline__ void blend(PixelState& s, float& cy, float power, float lo, float o,
+                                      int32_t pos, const float4& col) {
+  if (!(power >= lo && power <= 0.0f)) return;
+  const float alpha = fminf(kMaxAlpha, fmul(o, vexp(power)));
   if (!(alpha >= kAlphaThreshold)) return;
   const float next_t = fmul(s.transmittance, fsub(1.0f, alpha));
   if (next_t <= kTransmittanceThreshold) {
     s.done = true;
+    cy = __int_as_float(0x7fc00000);
     return;
   }
   const float w = fmul(s.transmittance, alpha);
-  const float4 col = s_col[j];
   s.r = ffma(w, col.x, s.r);
   s.g = ffma(w, col.y, s.g);
   s.b = ffma(w, col.z, s.b);
@@ -67,7 +72,7 @@ __device__ __forceinline__ void blend(PixelState& s, float q, float qmax, int j,
     s.depth = ffma(w, col.w, s.depth);
     if (w > s.best_weight) {
       s.best_weight = w;
-      s.best_semantic = s_sem[j];
+      s.best_pos = pos;
     }
   }
   s.transmittance = next_t;
@@ -89,20 +94,24 @@ __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamP
   if (kFull) {
     p.alpha[pixel] = out_alpha;
     p.depth[pixel] = out_alpha > 1.0e-8f ? fdiv(s.depth, out_alpha) : __int_as_float(0x7f800000);
-    p.semantic[pixel] =
-        (s.best_weight >= 0.0f && out_alpha >= p.semantic_min_alpha) ? s.best_semantic : -1;
+    int64_t semantic = -1;
+    if (s.best_weight >= 0.0f && out_alpha >= p.semantic_min_alpha) {
+      const Record& rec = p.records[p.values[s.best_pos]];
+      semantic = p.semantic_ids[__float_as_int(rec.b.w)];
+    }
+    p.semantic[pixel] = semantic;
   }
 }
 
 template <int kTile, bool kFull>
-__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
+__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
+                                  2048 / CompositeGeometry<kTile>::kThreads / 2)
     composite_kernel(CompositeParams p) {
   using Geo = CompositeGeometry<kTile>;
-  __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, conic_xx, 2*conic_xy
-  __shared__ float4 s_cqo[kCompositeBatch];  // conic_yy, q bound, opacity, -
+  __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
+  __shared__ float4 s_cpo[kCompositeBatch];  // -conic_yy/2, lo, opacity, -
   __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
   __shared__ uint32_t s_mask[kCompositeBatch];
-  __shared__ int64_t s_sem[kFull ? kCompositeBatch : 1];
 
   const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
   const int64_t* tile_prefix = reinterpret_cast<const int64_t*>(p.scratch + p.layout.tile_prefix);
@@ -146,12 +155,13 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
   const int pixel_y1 = pixel_y0 + Geo::kLaneRows;
   const bool valid0 = lane_used && pixel_x < plan.width && pixel_y0 < plan.height;
   const bool valid1 = lane_used && pixel_x < plan.width && pixel_y1 < plan.height;
+  const float kNaN = __int_as_float(0x7fc00000);
   const float cx = fadd(static_cast<float>(pixel_x), 0.5f);
-  const float cy0 = fadd(static_cast<float>(pixel_y0), 0.5f);
-  const float cy1 = fadd(static_cast<float>(pixel_y1), 0.5f);
+  float cy0 = valid0 ? fadd(static_cast<float>(pixel_y0), 0.5f) : kNaN;
+  float cy1 = valid1 ? fadd(static_cast<float>(pixel_y1), 0.5f) : kNaN;
 
-  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, -1, !valid0};
-  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, -1, !valid1};
+  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, !valid0};
+  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, !valid1};
   bool warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
 
   const int64_t range_start = p.tile_starts[global_tile];
@@ -165,12 +175,11 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
       for (int j = tid; j < n; j += Geo::kThreads) {
         const int32_t v = p.values[chunk + j];
         const Record rec = p.records[v];
-        s_geo[j] = make_float4(rec.a.x, rec.a.y, rec.a.z, fmul(2.0f, rec.a.w));
+        s_geo[j] = make_float4(rec.a.x, rec.a.y, fmul(-0.5f, rec.a.z), -rec.a.w);
         const float o = rec.b.y;
         const float qmax = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
-        s_cqo[j] = make_float4(rec.b.x, qmax, o, 0.0f);
+        s_cpo[j] = make_float4(fmul(-0.5f, rec.b.x), fmaxf(fmul(-0.5f, qmax), -20.0f), o, 0.0f);
         s_col[j] = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
-        if (kFull) s_sem[j] = p.semantic_ids[__float_as_int(rec.b.w)];
         const __half2 box = *reinterpret_cast<const __half2*>(&rec.c.w);
         const float hx = __low2float(box);
         const float hy = __high2float(box);
@@ -189,6 +198,7 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
       }
       __syncthreads();
       if (!warp_done) {
+        const int32_t chunk_pos = static_cast<int32_t>(chunk);
         for (int base = 0; base < n && !warp_done; base += 32) {
           const uint32_t m = (base + lane < n) ? s_mask[base + lane] : 0u;
           uint32_t bits = __ballot_sync(0xffffffffu, (m >> warp) & 1u);
@@ -196,17 +206,21 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
             const int j = base + __ffs(bits) - 1;
             bits &= bits - 1;
             const float4 geo = s_geo[j];
-            const float cq = s_cqo[j].x;
-            const float qmax = s_cqo[j].y;
+            const float4 cpo = s_cpo[j];
             const float dx = fsub(cx, geo.x);
             const float adx = fmul(fmul(geo.z, dx), dx);
             const float bdx = fmul(geo.w, dx);
             const float dy0 = fsub(cy0, geo.y);
             const float dy1 = fsub(cy1, geo.y);
-            const float q0 = ffma(fmul(cq, dy0), dy0, ffma(bdx, dy0, adx));
-            const float q1 = ffma(fmul(cq, dy1), dy1, ffma(bdx, dy1, adx));
-            blend<kFull>(s0, q0, qmax, j, s_cqo, s_col, s_sem);
-            blend<kFull>(s1, q1, qmax, j, s_cqo, s_col, s_sem);
+            const float p0 = ffma(fmul(cpo.x, dy0), dy0, ffma(bdx, dy0, adx));
+            const float p1 = ffma(fmul(cpo.x, dy1), dy1, ffma(bdx, dy1, adx));
+            const bool in0 = p0 >= cpo.y && p0 <= 0.0f;
+            const bool in1 = p1 >= cpo.y && p1 <= 0.0f;
+            if (in0 || in1) {
+              const float4 col = s_col[j];
+              blend<kFull>(s0, cy0, p0, cpo.y, cpo.z, chunk_pos + j, col);
+              blend<kFull>(s1, cy1, p1, cpo.y, cpo.z, chunk_pos + j, col);
+            }
           }
           warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
         }

@@ -30,12 +30,17 @@ __device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
 // exp(x) for finite x in [-87, 88]: Cody-Waite reduction x = n ln2 + r with
 // n = rint(x log2 e), r carried as f = x log2(e) - n in two fma steps, and the
 // degree-7 Taylor polynomial of 2^f = e^(f ln 2) on |f| <= 0.5 (truncation
-// error < 5e-9 relative), scaled by 2^n through the exponent field.
+// error < 5e-9 relative), scaled by 2^n through the exponent field.  The
+// rounding to an integer adds and subtracts 1.5 * 2^23 (round-to-nearest-even,
+// exact for |t| < 2^22, so identical to rint), and n's integer value is read
+// from the bits of the sum: all on the FMA and integer pipes.
 __device__ __forceinline__ float vexp(float x) {
   const float kLog2eHi = 1.44269502162933349609375f;
   const float kLog2eLo = 1.925963033500011079e-8f;
+  const float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
   const float t = fmul(x, kLog2eHi);
-  const float n = rintf(t);
+  const float tm = fadd(t, kRoundMagic);
+  const float n = fsub(tm, kRoundMagic);
   float f = ffma(x, kLog2eHi, -n);
   f = ffma(x, kLog2eLo, f);
   // c_k = (ln 2)^k / k!
@@ -47,7 +52,7 @@ __device__ __forceinline__ float vexp(float x) {
   p = ffma(p, f, 2.402265069591007e-01f);      // k = 2
   p = ffma(p, f, 6.931471805599453e-01f);      // k = 1
   p = ffma(p, f, 1.0f);                        // k = 0
-  const int e = static_cast<int>(n);
+  const int e = __float_as_int(tm) - 0x4b400000;  // bits of 1.5 * 2^23
   return fmul(p, __int_as_float((e + 127) << 23));
 }
 
