@@ -136,7 +136,6 @@ __device__ __forceinline__ void block_minmax(uint32_t& dmin, uint32_t& dmax, uin
     rmin = min(rmin, s[2][w]);
     rmax = max(rmax, s[3][w]);
   }
-  __syncthreads();
 }
 
 }  // namespace
@@ -278,6 +277,7 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
     RankSmem rank;
     uint32_t split[kSplits];
   } s_u;
+  __shared__ __align__(16) uint32_t s_off[kSplits];
   __shared__ uint32_t s_base[kRadixBins];
   __shared__ uint32_t s_minmax[4][kTsWarps];
   __shared__ uint32_t s_scan[kTsWarps];
@@ -375,15 +375,14 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
         off[j] = prefix;
         prefix += c[j];
       }
-      __syncthreads();  // every thread has read its counters
-      reinterpret_cast<uint4*>(s_u.split)[tid * 2] = make_uint4(off[0], off[1], off[2], off[3]);
-      reinterpret_cast<uint4*>(s_u.split)[tid * 2 + 1] = make_uint4(off[4], off[5], off[6], off[7]);
+      reinterpret_cast<uint4*>(s_off)[tid * 2] = make_uint4(off[0], off[1], off[2], off[3]);
+      reinterpret_cast<uint4*>(s_off)[tid * 2 + 1] = make_uint4(off[4], off[5], off[6], off[7]);
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < kTileSortItems; ++k) {
         if (k >= K) break;
         if (k * kTileSortThreads + tid < n) {
-          s_items[s_u.split[dr[k] >> 16] + (dr[k] & 0xffffu)] = it[k];
+          s_items[s_off[dr[k] >> 16] + (dr[k] & 0xffffu)] = it[k];
         }
       }
       __syncthreads();
@@ -391,8 +390,8 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
 #pragma unroll
       for (int j = 0; j < kSplitsPerThread; ++j) {
         const int split = tid * kSplitsPerThread + j;
-        const int lo = static_cast<int>(s_u.split[split]);
-        const int hi = split + 1 < kSplits ? static_cast<int>(s_u.split[split + 1]) : n;
+        const int lo = static_cast<int>(s_off[split]);
+        const int hi = split + 1 < kSplits ? static_cast<int>(s_off[split + 1]) : n;
         for (int a = lo + 1; a < hi; ++a) {
           const uint64_t v = s_items[a];
           int b = a - 1;

@@ -17,15 +17,62 @@
 namespace vgr {
 
 // ---------------------------------------------------------------------------
-// Camera setup: one CTA builds the per-active-camera plans, the exclusive
-// prefix of tiles over active cameras (the compositor's work list), and
-// zeroes counters and queue tickets so the frame needs no host memset.
+// Per-camera constants of the projection, computed once per active slot by
+// the setup kernel.  R = view_rotation * env_rotation and
+// t = view_rotation * env_t + view_t, so camera-space p = R m + t.
+// ---------------------------------------------------------------------------
+struct __align__(16) CamConst {
+  float r[9];
+  float t[3];
+  float fx, fy, cx, cy;
+  float lim_xp, lim_xn, lim_yp, lim_yn;
+  float width, height;
+};
+static_assert(sizeof(CamConst) == 96, "CamConst is twelve 8-byte words");
+
+__device__ __forceinline__ void make_cam_const(const float* view, const float* env,
+                                               const float* intr, int width, int height,
+                                               CamConst* c) {
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col) {
+      c->r[row * 3 + col] =
+          ffma(view[row * 4 + 2], env[8 + col],
+               ffma(view[row * 4 + 1], env[4 + col], fmul(view[row * 4 + 0], env[col])));
+    }
+    c->t[row] = ffma(view[row * 4 + 2], env[11],
+                     ffma(view[row * 4 + 1], env[7],
+                          ffma(view[row * 4 + 0], env[3], view[row * 4 + 3])));
+  }
+  c->fx = intr[0];
+  c->fy = intr[4];
+  c->cx = intr[2];
+  c->cy = intr[5];
+  const float w = static_cast<float>(width);
+  const float h = static_cast<float>(height);
+  c->width = w;
+  c->height = h;
+  const float tan_x = fdiv(fmul(0.5f, w), c->fx);
+  const float tan_y = fdiv(fmul(0.5f, h), c->fy);
+  c->lim_xp = ffma(0.3f, tan_x, fdiv(fsub(w, c->cx), c->fx));
+  c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
+  c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
+  c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
+}
+
+// ---------------------------------------------------------------------------
+// Camera setup: one CTA builds the per-active-camera plans and projection
+// constants, the exclusive prefix of tiles over active cameras (the
+// compositor's work list), and zeroes counters and queue tickets so the frame
+// needs no host memset.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) camera_setup_kernel(SetupParams p) {
   __shared__ int64_t s_warp_sums[32];
   __shared__ int64_t s_carry;
   ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
   CamPlan* plans = reinterpret_cast<CamPlan*>(p.scratch + p.layout.plans);
+  CamConst* cam_consts = reinterpret_cast<CamConst*>(p.scratch + p.layout.cam_consts);
   int64_t* tile_prefix = reinterpret_cast<int64_t*>(p.scratch + p.layout.tile_prefix);
   const int tid = threadIdx.x;
   if (tid < 32) {
@@ -88,6 +135,8 @@ __global__ void __launch_bounds__(1024) camera_setup_kernel(SetupParams p) {
           plan.pixel_base = static_cast<int64_t>(cam) * plan.width * plan.height;
         }
         tiles = static_cast<int64_t>(plan.tiles_x) * plan.tiles_y;
+        make_cam_const(p.viewmats + cam * 16, p.env_xforms + cam * 16, p.intrinsics + cam * 9,
+                       plan.width, plan.height, cam_consts + a);
       }
       plans[a] = plan;
     }
@@ -120,50 +169,6 @@ __global__ void __launch_bounds__(1024) camera_setup_kernel(SetupParams p) {
     __syncthreads();
   }
   if (tid == 0) tile_prefix[p.active_count] = s_carry;
-}
-
-// ---------------------------------------------------------------------------
-// Per-camera constants of the projection, computed once per virtual block.
-// R = view_rotation * env_rotation and t = view_rotation * env_t + view_t,
-// so camera-space p = R m + t.
-// ---------------------------------------------------------------------------
-struct CamConst {
-  float r[9];
-  float t[3];
-  float fx, fy, cx, cy;
-  float lim_xp, lim_xn, lim_yp, lim_yn;
-  float width, height;
-};
-
-__device__ __forceinline__ void make_cam_const(const float* view, const float* env,
-                                               const float* intr, int width, int height,
-                                               CamConst* c) {
-#pragma unroll
-  for (int row = 0; row < 3; ++row) {
-#pragma unroll
-    for (int col = 0; col < 3; ++col) {
-      c->r[row * 3 + col] =
-          ffma(view[row * 4 + 2], env[8 + col],
-               ffma(view[row * 4 + 1], env[4 + col], fmul(view[row * 4 + 0], env[col])));
-    }
-    c->t[row] = ffma(view[row * 4 + 2], env[11],
-                     ffma(view[row * 4 + 1], env[7],
-                          ffma(view[row * 4 + 0], env[3], view[row * 4 + 3])));
-  }
-  c->fx = intr[0];
-  c->fy = intr[4];
-  c->cx = intr[2];
-  c->cy = intr[5];
-  const float w = static_cast<float>(width);
-  const float h = static_cast<float>(height);
-  c->width = w;
-  c->height = h;
-  const float tan_x = fdiv(fmul(0.5f, w), c->fx);
-  const float tan_y = fdiv(fmul(0.5f, h), c->fy);
-  c->lim_xp = ffma(0.3f, tan_x, fdiv(fsub(w, c->cx), c->fx));
-  c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
-  c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
-  c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
 }
 
 struct Projected {
@@ -286,22 +291,6 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vect
   constexpr int kCount = (kDegree + 1) * (kDegree + 1);
   constexpr int kFloats = kCount * 3;
   constexpr int kVectors = (kFloats + 3) / 4;
-  float coeffs[kVectors * 4];
-  if (vector_loads) {
-    const float4* row4 = reinterpret_cast<const float4*>(row);
-#pragma unroll
-    for (int i = 0; i < kVectors; ++i) {
-      const float4 v = __ldg(row4 + i);
-      coeffs[4 * i + 0] = v.x;
-      coeffs[4 * i + 1] = v.y;
-      coeffs[4 * i + 2] = v.z;
-      coeffs[4 * i + 3] = v.w;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < kFloats; ++i) coeffs[i] = __ldg(row + i);
-  }
-  const int degree = kDegree;
   float dx = ffma(c.r[6], pz, ffma(c.r[3], py, fmul(c.r[0], px)));
   float dy = ffma(c.r[7], pz, ffma(c.r[4], py, fmul(c.r[1], px)));
   float dz = ffma(c.r[8], pz, ffma(c.r[5], py, fmul(c.r[2], px)));
@@ -309,24 +298,21 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vect
   const float x = fmul(dx, inv), y = fmul(dy, inv), z = fmul(dz, inv);
   float basis[16];
   basis[0] = 0.28209479177387814f;
-  int count = 1;
-  if (degree >= 1) {
+  if (kDegree >= 1) {
     basis[1] = fmul(-0.4886025119029199f, y);
     basis[2] = fmul(0.4886025119029199f, z);
     basis[3] = fmul(-0.4886025119029199f, x);
-    count = 4;
   }
   const float xx = fmul(x, x), yy = fmul(y, y), zz = fmul(z, z);
   const float xy = fmul(x, y), yz = fmul(y, z), xz = fmul(x, z);
-  if (degree >= 2) {
+  if (kDegree >= 2) {
     basis[4] = fmul(1.0925484305920792f, xy);
     basis[5] = fmul(-1.0925484305920792f, yz);
     basis[6] = fmul(0.31539156525252005f, fsub(fsub(fmul(2.0f, zz), xx), yy));
     basis[7] = fmul(-1.0925484305920792f, xz);
     basis[8] = fmul(0.5462742152960396f, fsub(xx, yy));
-    count = 9;
   }
-  if (degree >= 3) {
+  if (kDegree >= 3) {
     basis[9] = fmul(fmul(-0.5900435899266435f, y), fsub(fmul(3.0f, xx), yy));
     basis[10] = fmul(fmul(2.890611442640554f, xy), z);
     basis[11] = fmul(fmul(-0.4570457994644658f, y), fsub(fsub(fmul(4.0f, zz), xx), yy));
@@ -335,15 +321,33 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vect
     basis[13] = fmul(fmul(-0.4570457994644658f, x), fsub(fsub(fmul(4.0f, zz), xx), yy));
     basis[14] = fmul(fmul(1.445305721320277f, z), fsub(xx, yy));
     basis[15] = fmul(fmul(-0.5900435899266435f, x), fsub(xx, fmul(3.0f, yy)));
-    count = 16;
+  }
+  // Coefficients are consumed as they arrive: float f of the row is channel
+  // f % 3 of coefficient f / 3, and each channel's terms are added in
+  // ascending coefficient order (the same sum as a per-channel loop).
+  float acc[3] = {0.0f, 0.0f, 0.0f};
+  auto take = [&](int f, float v) {
+    const int k = f / 3;
+    const int ch = f - 3 * k;
+    if (k >= kCount) return;
+    acc[ch] = k == 0 ? fmul(basis[0], v) : ffma(basis[k], v, acc[ch]);
+  };
+  if (vector_loads) {
+    const float4* row4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+    for (int i = 0; i < kVectors; ++i) {
+      const float4 v = __ldg(row4 + i);
+      take(4 * i + 0, v.x);
+      take(4 * i + 1, v.y);
+      take(4 * i + 2, v.z);
+      take(4 * i + 3, v.w);
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < kFloats; ++f) take(f, __ldg(row + f));
   }
 #pragma unroll
-  for (int ch = 0; ch < 3; ++ch) {
-    float acc = fmul(basis[0], coeffs[ch]);
-#pragma unroll
-    for (int k = 1; k < count; ++k) acc = ffma(basis[k], coeffs[k * 3 + ch], acc);
-    rgb[ch] = fmaxf(fadd(acc, 0.5f), 0.0f);
-  }
+  for (int ch = 0; ch < 3; ++ch) rgb[ch] = fmaxf(fadd(acc[ch], 0.5f), 0.0f);
 }
 
 // Conservative half-extents (pixels) of the region where a record can reach
@@ -413,7 +417,7 @@ __device__ __forceinline__ void project_lookback(uint64_t* desc, int64_t b, uint
 }
 
 template <int kShDegree>
-__global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(ProjectParams p) {
+__global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
   __shared__ uint16_t s_slot[kProjectChunk];       // rank -> task slot
   __shared__ uint32_t s_rect_min[kProjectChunk];   // min_tx | min_ty << 16
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(Projec
   __shared__ uint32_t s_warp_vis[kProjectRounds][kProjectThreads / 32];
   __shared__ uint64_t s_warp_isect[kProjectRounds][kProjectThreads / 32];
   __shared__ CamConst s_cam;
-  __shared__ CamPlan s_plan;
+  __shared__ __align__(8) CamPlan s_plan;
   __shared__ int64_t s_vblock;
   __shared__ uint64_t s_base_vis, s_base_isect;
   __shared__ uint32_t s_nvis;
@@ -431,6 +435,7 @@ __global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(Projec
 
   ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
   const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
+  const CamConst* cam_consts = reinterpret_cast<const CamConst*>(p.scratch + p.layout.cam_consts);
   uint64_t* desc = reinterpret_cast<uint64_t*>(p.scratch + p.layout.project_desc);
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -438,25 +443,31 @@ __global__ void __launch_bounds__(kProjectThreads, 3) project_emit_kernel(Projec
 
   const int64_t total_vblocks = p.total_vblocks;
   while (true) {
-    if (tid == 0) s_vblock = atomicAdd(&header->project_queue, 1u);
+    // Warp 0 takes the ticket and stages the slot's plan (7 words) and
+    // projection constants (12 words) with one load per lane.
+    if (warp == 0) {
+      int64_t ticket = 0;
+      if (lane == 0) ticket = atomicAdd(&header->project_queue, 1u);
+      ticket = __shfl_sync(0xffffffffu, ticket, 0);
+      if (ticket < total_vblocks) {
+        const int64_t slot = ticket % p.active_count;
+        if (lane < 7) {
+          reinterpret_cast<uint64_t*>(&s_plan)[lane] =
+              reinterpret_cast<const uint64_t*>(plans + slot)[lane];
+        } else if (lane < 19) {
+          reinterpret_cast<uint64_t*>(&s_cam)[lane - 7] =
+              reinterpret_cast<const uint64_t*>(cam_consts + slot)[lane - 7];
+        }
+      }
+      if (lane == 0) s_vblock = ticket;
+    }
     __syncthreads();
     const int64_t b = s_vblock;
     if (b >= total_vblocks) break;
     const int64_t chunk = b / p.active_count;
-    const int64_t slot = b - chunk * p.active_count;
-    if (tid == 0) {
-      s_plan = plans[slot];
-    }
-    __syncthreads();
     const CamPlan plan = s_plan;
     const int64_t local_begin = chunk * kProjectChunk;
     const bool live = plan.camera >= 0 && plan.scene_slot >= 0 && local_begin < plan.g_count;
-    if (live && tid == 0) {
-      const int cam = plan.camera;
-      make_cam_const(p.viewmats + cam * 16, p.env_xforms + cam * 16, p.intrinsics + cam * 9,
-                     plan.width, plan.height, &s_cam);
-    }
-    __syncthreads();
 
     // Project both rounds first (no barrier), then one block scan of
     // (visible, tiles) over the kProjectChunk tasks in task order.

@@ -382,6 +382,9 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     sp.width = static_cast<int>(opt->width);
     sp.height = static_cast<int>(opt->height);
     sp.tile_size = ts;
+    sp.viewmats = cams->viewmats;
+    sp.intrinsics = cams->intrinsics;
+    sp.env_xforms = cams->env_xforms;
     camera_setup_kernel<<<1, 1024, 0, stream>>>(sp);
     if ((rc = check_launch("render: camera setup")) != VGR_OK) return rc;
     mark(1);

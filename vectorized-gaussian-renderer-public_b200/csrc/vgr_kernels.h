@@ -26,6 +26,9 @@ struct SetupParams {
   int width;
   int height;
   int tile_size;
+  const float* viewmats;
+  const float* intrinsics;
+  const float* env_xforms;
 };
 
 struct ProjectParams {
