@@ -219,3 +219,14 @@ def test_partial_depth_ties_in_shared_memory_buckets():
     assert 1 < cpu.tile_counts.max() <= 4096
     _compare(gpu, cpu)
     assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
+
+
+def test_large_tile_grid_bitwise():
+    # 19,200 4x4-pixel tiles over four 320x240 cameras.
+    scene = synthetic_scene(20_000, seed=71, mean_half_extent=1.5, log_scale_mean=-3.5)
+    rig = orbit_cameras(4, seed=12, radius=4.0, height_offset=0.8, width=320, height=240, focal=260.0)
+    gpu = render_gpu([(2, scene)], rig, [2] * 4, tile_size=4)
+    cpu = render_oracle([(2, scene)], rig, [2] * 4, tile_size=4, with_tiles=True)
+    assert cpu.tile_counts.size >= 4096
+    _compare(gpu, cpu)
+    assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
