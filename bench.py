@@ -71,6 +71,8 @@ def parse_args() -> argparse.Namespace:
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--lidar-steps", type=int, default=5,
                         help="LiDAR frames timed after the camera workload (0: skip)")
+    parser.add_argument("--lidar-sensors", type=int, default=None,
+                        help="override the LiDAR sensor count (small profiling captures)")
     return parser.parse_args()
 
 
@@ -347,7 +349,9 @@ def run_lidar(args, device, world: int, with_cpu: bool) -> dict:
     from vgr_b200.cuda_lidar_backend import CudaLidarBackend
     from vgr_b200.lidar_service import GaussianLidarService
 
-    cfg = LIDAR_CONFIG
+    cfg = dict(LIDAR_CONFIG)
+    if args.lidar_sensors:
+        cfg["sensors"] = args.lidar_sensors
     work = workloads.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
     sensors = cfg["sensors"]
     rays = work.ray_directions.shape[0]
