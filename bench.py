@@ -571,6 +571,10 @@ def run_b200(args) -> None:
         "frac": round(achieved / peak, 4),
         "peak_source": f"hbm_gbs of {peak_kind}",
         "traffic": traffic_table.get(KERNEL_NAMES[dominant]),
+        "traffic_source": traffic_table.get("_source"),
+        # Fraction of peak instruction issue from the committed ncu capture: the compositor
+        # is issue-bound, so this, not the HBM fraction, is its binding roofline.
+        "issue_active_ncu": traffic_table.get("_issue_active", {}).get(KERNEL_NAMES[dominant]),
         "algorithmic_bytes": int(bytes_per_stage[dominant]),
         "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
         "stage_frac_of_measured_hbm": {
