@@ -50,7 +50,7 @@ struct __align__(16) Surfel {
   float4 n;   // normal xyz, surface confidence
   float4 a0;  // tangent axis 0 xyz, scale 0
   float4 a1;  // tangent axis 1 xyz, scale 1
-  float4 e;   // reflectivity, -, -, -
+  float4 e;   // reflectivity, max(scale0, scale1)^2, -, -
 };
 static_assert(sizeof(Surfel) == 80, "Surfel layout");
 
@@ -247,7 +247,8 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_gather_kernel(BuildParams
   s.n = make_float4(axes[n].x, axes[n].y, axes[n].z, p.confidence ? p.confidence[g] : 1.0f);
   s.a0 = make_float4(axes[t0].x, axes[t0].y, axes[t0].z, sc[t0]);
   s.a1 = make_float4(axes[t1].x, axes[t1].y, axes[t1].z, sc[t1]);
-  s.e = make_float4(p.reflectivity ? p.reflectivity[g] : -1.0f, 0.0f, 0.0f, 0.0f);
+  const float smax = fmaxf(sc[t0], sc[t1]);
+  s.e = make_float4(p.reflectivity ? p.reflectivity[g] : -1.0f, smax * smax, 0.0f, 0.0f);
   surfels[i] = s;
   sem[i] = p.semantics[g];
 }
@@ -429,61 +430,66 @@ __global__ void lidar_end_kernel(int64_t* counters) {
   atomicAdd(reinterpret_cast<unsigned long long*>(counters + kCallsCompleted), 1ull);
 }
 
+// Ray in the scene frame.  inv = 1/d per axis and ood = o * inv, so a slab
+// bound is one fma; an axis with d == 0 gives infinite (or NaN) bounds, which
+// the min/max below ignore, so such a box is kept (conservatively) rather
+// than culled.  inv_dd = 1/|d|^2 for the surfel distance pre-test.
 struct Ray {
-  float3 o, d, inv;
-  bool par_x, par_y, par_z;  // |d| < 1e-12 on that axis
+  float3 o, d, inv, ood;
+  float inv_dd;
 };
 
-__device__ __forceinline__ bool slab_axis(float lo, float hi, float o, float d, float inv, bool par,
-                                          float* t0, float* t1) {
-  if (par) return !(o < lo || o > hi);
-  float a = (lo - o) * inv;
-  float b = (hi - o) * inv;
-  if (a > b) {
-    const float t = a;
-    a = b;
-    b = t;
-  }
-  *t0 = fmaxf(*t0, a);
-  *t1 = fminf(*t1, b);
-  return !(*t0 > *t1);
-}
-
-// Slab test of one box against [tmin, tmax] (reference :329-363); empty
-// boxes (lo > hi) never hit.
+// Slab test of one box against [tmin, tmax] (reference :329-363), branch
+// free; empty boxes (lo > hi) never hit.  *entry = where the ray enters.
 __device__ __forceinline__ bool hit_box(const Ray& r, float lx, float ly, float lz, float hx,
                                         float hy, float hz, float tmin, float tmax, float* entry) {
-  if (lx > hx) return false;
-  float t0 = tmin, t1 = tmax;
-  if (!slab_axis(lx, hx, r.o.x, r.d.x, r.inv.x, r.par_x, &t0, &t1)) return false;
-  if (!slab_axis(ly, hy, r.o.y, r.d.y, r.inv.y, r.par_y, &t0, &t1)) return false;
-  if (!slab_axis(lz, hz, r.o.z, r.d.z, r.inv.z, r.par_z, &t0, &t1)) return false;
+  const float ax = fmaf(lx, r.inv.x, -r.ood.x), bx = fmaf(hx, r.inv.x, -r.ood.x);
+  const float ay = fmaf(ly, r.inv.y, -r.ood.y), by = fmaf(hy, r.inv.y, -r.ood.y);
+  const float az = fmaf(lz, r.inv.z, -r.ood.z), bz = fmaf(hz, r.inv.z, -r.ood.z);
+  const float t0 = fmaxf(fmaxf(tmin, fminf(ax, bx)), fmaxf(fminf(ay, by), fminf(az, bz)));
+  const float t1 = fminf(fminf(tmax, fmaxf(ax, bx)), fminf(fmaxf(ay, by), fmaxf(az, bz)));
   *entry = t0;
-  return true;
+  return t0 <= t1 && lx <= hx;
 }
 
 struct Candidate {
   float t, weight, intensity;
 };
 
-__device__ __forceinline__ bool evaluate(const Surfel& s, const Ray& r, const TraceParams& p,
+// Candidate test of one surfel (reference :383-421).  A conservative
+// pre-test comes first: an accepted hit point lies in the surfel's tangent
+// plane with tangent coordinates (u, v), u^2 + v^2 <= q_max, so within
+// sqrt(q_max) * max(scale0, scale1) of the mean, and the ray must pass at
+// least that close (distance from the cross product, which does not cancel).
+// Only surfels that pass it load their frame and take the exact test.
+__device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const TraceParams& p,
                                          Candidate* c) {
-  const float denom = s.n.x * r.d.x + s.n.y * r.d.y + s.n.z * r.d.z;
+  const float4 m = __ldg(&sp->m);
+  const float4 e = __ldg(&sp->e);
+  const float3 dm = make_float3(m.x - r.o.x, m.y - r.o.y, m.z - r.o.z);
+  const float cx = dm.y * r.d.z - dm.z * r.d.y;
+  const float cy = dm.z * r.d.x - dm.x * r.d.z;
+  const float cz = dm.x * r.d.y - dm.y * r.d.x;
+  const float dist2 = (cx * cx + cy * cy + cz * cz) * r.inv_dd;
+  if (!(dist2 <= p.q_max * e.y * 1.001f + 1.0e-5f)) return false;
+  const float4 n = __ldg(&sp->n);
+  const float denom = n.x * r.d.x + n.y * r.d.y + n.z * r.d.z;
   const float incidence = fabsf(denom);
   if (incidence < p.min_cos) return false;
-  const float3 dm = make_float3(s.m.x - r.o.x, s.m.y - r.o.y, s.m.z - r.o.z);
-  const float t = (s.n.x * dm.x + s.n.y * dm.y + s.n.z * dm.z) / denom;
+  const float t = (n.x * dm.x + n.y * dm.y + n.z * dm.z) / denom;
   if (!(t >= p.near_plane && t <= p.far_plane)) return false;
-  const float3 diff = make_float3(r.o.x + r.d.x * t - s.m.x, r.o.y + r.d.y * t - s.m.y,
-                                  r.o.z + r.d.z * t - s.m.z);
-  const float u = (diff.x * s.a0.x + diff.y * s.a0.y + diff.z * s.a0.z) / s.a0.w;
-  const float v = (diff.x * s.a1.x + diff.y * s.a1.y + diff.z * s.a1.z) / s.a1.w;
+  const float4 a0 = __ldg(&sp->a0);
+  const float4 a1 = __ldg(&sp->a1);
+  const float3 diff = make_float3(r.o.x + r.d.x * t - m.x, r.o.y + r.d.y * t - m.y,
+                                  r.o.z + r.d.z * t - m.z);
+  const float u = (diff.x * a0.x + diff.y * a0.y + diff.z * a0.z) / a0.w;
+  const float v = (diff.x * a1.x + diff.y * a1.y + diff.z * a1.z) / a1.w;
   const float q = u * u + v * v;
   if (!(q <= p.q_max)) return false;
   const float support = expf(-0.5f * q);
-  const float weight = s.m.w * support * s.n.w;
+  const float weight = m.w * support * n.w;
   if (!(weight >= p.threshold) || !isfinite(weight)) return false;
-  const float refl = s.e.x >= 0.0f ? s.e.x : p.fallback_reflectivity;
+  const float refl = e.x >= 0.0f ? e.x : p.fallback_reflectivity;
   c->t = t;
   c->weight = weight;
   c->intensity = fminf(fmaxf(refl * support * incidence, 0.0f), 1.0f);
@@ -615,10 +621,9 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_trace_kernel(TraceParams 
         r.d = make_float3(xt[0] * wd.x + xt[4] * wd.y + xt[8] * wd.z,
                           xt[1] * wd.x + xt[5] * wd.y + xt[9] * wd.z,
                           xt[2] * wd.x + xt[6] * wd.y + xt[10] * wd.z);
-        r.par_x = fabsf(r.d.x) < 1.0e-12f;
-        r.par_y = fabsf(r.d.y) < 1.0e-12f;
-        r.par_z = fabsf(r.d.z) < 1.0e-12f;
         r.inv = make_float3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+        r.ood = make_float3(r.o.x * r.inv.x, r.o.y * r.inv.y, r.o.z * r.inv.z);
+        r.inv_dd = 1.0f / (r.d.x * r.d.x + r.d.y * r.d.y + r.d.z * r.d.z);
         const LidarDescriptor sc = *scene;
         const int m = sc.header->surfel_count;
         const int leaves = (m + sc.packet - 1) / sc.packet;
@@ -634,7 +639,7 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_trace_kernel(TraceParams 
             for (int i = begin; i < end; ++i) {
               ++st.tests;
               Candidate c;
-              if (evaluate(sc.surfels[i], r, p, &c)) {
+              if (evaluate(sc.surfels + i, r, p, &c)) {
                 ++st.candidates;
                 if (c.t > previous_end && (!found || c.t < best)) {
                   best = c.t;
@@ -660,7 +665,7 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_trace_kernel(TraceParams 
             for (int i = begin; i < end; ++i) {
               ++st.tests;
               Candidate c;
-              if (!evaluate(sc.surfels[i], r, p, &c) || c.t < first_t || c.t > cluster_end) continue;
+              if (!evaluate(sc.surfels + i, r, p, &c) || c.t < first_t || c.t > cluster_end) continue;
               total_w += static_cast<double>(c.weight);
               weighted_t += static_cast<double>(c.weight) * c.t;
               weighted_i += static_cast<double>(c.weight) * c.intensity;
