@@ -43,6 +43,7 @@ namespace {
 constexpr int kLidarThreads = 256;
 constexpr int kMaxStack = 64;
 constexpr int kMaxSemanticSlots = 32;
+constexpr int kMaxCluster = 16;  // candidates kept per cluster window in one traversal
 constexpr uint32_t kNonPlanarKey = 1u << 30;
 
 struct __align__(16) Surfel {
@@ -630,65 +631,102 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_trace_kernel(TraceParams 
         float previous_end = p.near_plane - 1.0e-6f;
         const int64_t base = (sensor * p.rays + ray) * p.returns;
         for (int k = 0; k < p.returns; ++k) {
-          // Nearest candidate beyond the previous cluster.
+          // One traversal finds the nearest candidate beyond the previous
+          // cluster and keeps the candidates inside its cluster window
+          // [best, best + max(abs, rel * best)]: the window only shrinks as
+          // best does, so nodes beyond the current window are pruned and a
+          // candidate dropped from the list can never re-enter the final
+          // window.  If more than kMaxCluster candidates fall inside the
+          // window at once, a second traversal gathers the cluster.
           float best = p.far_plane;
+          float window = p.far_plane;
           bool found = false;
-          traverse(sc, leaves, r, p.near_plane, &best, st, [&](int leaf) {
+          int listed = 0;
+          bool list_full = false;
+          int32_t list_idx[kMaxCluster];
+          float list_t[kMaxCluster];
+          traverse(sc, leaves, r, p.near_plane, &window, st, [&](int leaf) {
             const int begin = leaf * sc.packet;
             const int end = min(begin + sc.packet, m);
             for (int i = begin; i < end; ++i) {
               ++st.tests;
               Candidate c;
-              if (evaluate(sc.surfels + i, r, p, &c)) {
-                ++st.candidates;
-                if (c.t > previous_end && (!found || c.t < best)) {
-                  best = c.t;
-                  found = true;
+              if (!evaluate(sc.surfels + i, r, p, &c)) continue;
+              ++st.candidates;
+              if (!(c.t > previous_end) || c.t > window) continue;
+              if (!found || c.t < best) {
+                best = c.t;
+                found = true;
+                window = fminf(p.far_plane, best + fmaxf(p.cluster_abs, p.cluster_rel * best));
+                int kept = 0;
+                for (int q = 0; q < listed; ++q) {
+                  if (list_t[q] <= window) {
+                    list_t[kept] = list_t[q];
+                    list_idx[kept] = list_idx[q];
+                    ++kept;
+                  }
                 }
+                listed = kept;
+              }
+              if (listed < kMaxCluster) {
+                list_t[listed] = c.t;
+                list_idx[listed] = i;
+                ++listed;
+              } else {
+                list_full = true;
               }
             }
           });
           if (st.overflow || !found) break;
           const float first_t = best;
-          const float cluster_end =
-              fminf(p.far_plane, first_t + fmaxf(p.cluster_abs, p.cluster_rel * first_t));
+          const float cluster_end = window;
           // Cluster reduction in double precision.
           int64_t labels[kMaxSemanticSlots];
           double label_w[kMaxSemanticSlots];
           int nl = 0;
           bool overflow = false;
           double total_w = 0.0, weighted_t = 0.0, weighted_i = 0.0;
-          float window_end = cluster_end;
-          traverse(sc, leaves, r, first_t, &window_end, st, [&](int leaf) {
-            const int begin = leaf * sc.packet;
-            const int end = min(begin + sc.packet, m);
-            for (int i = begin; i < end; ++i) {
-              ++st.tests;
-              Candidate c;
-              if (!evaluate(sc.surfels + i, r, p, &c) || c.t < first_t || c.t > cluster_end) continue;
-              total_w += static_cast<double>(c.weight);
-              weighted_t += static_cast<double>(c.weight) * c.t;
-              weighted_i += static_cast<double>(c.weight) * c.intensity;
-              const int64_t label = sc.semantics[i];
-              int slot = -1;
-              for (int q = 0; q < nl; ++q) {
-                if (labels[q] == label) {
-                  slot = q;
-                  break;
-                }
+          auto accumulate = [&](int i, const Candidate& c) {
+            total_w += static_cast<double>(c.weight);
+            weighted_t += static_cast<double>(c.weight) * c.t;
+            weighted_i += static_cast<double>(c.weight) * c.intensity;
+            const int64_t label = sc.semantics[i];
+            int slot = -1;
+            for (int q = 0; q < nl; ++q) {
+              if (labels[q] == label) {
+                slot = q;
+                break;
               }
-              if (slot < 0) {
-                if (nl >= p.semantic_slots) {
-                  overflow = true;
-                } else {
-                  slot = nl++;
-                  labels[slot] = label;
-                  label_w[slot] = 0.0;
-                }
-              }
-              if (slot >= 0) label_w[slot] += static_cast<double>(c.weight);
             }
-          });
+            if (slot < 0) {
+              if (nl >= p.semantic_slots) {
+                overflow = true;
+              } else {
+                slot = nl++;
+                labels[slot] = label;
+                label_w[slot] = 0.0;
+              }
+            }
+            if (slot >= 0) label_w[slot] += static_cast<double>(c.weight);
+          };
+          if (!list_full) {
+            for (int q = 0; q < listed; ++q) {
+              Candidate c;
+              if (evaluate(sc.surfels + list_idx[q], r, p, &c)) accumulate(list_idx[q], c);
+            }
+          } else {
+            float window_end = cluster_end;
+            traverse(sc, leaves, r, first_t, &window_end, st, [&](int leaf) {
+              const int begin = leaf * sc.packet;
+              const int end = min(begin + sc.packet, m);
+              for (int i = begin; i < end; ++i) {
+                ++st.tests;
+                Candidate c;
+                if (!evaluate(sc.surfels + i, r, p, &c) || c.t < first_t || c.t > cluster_end) continue;
+                accumulate(i, c);
+              }
+            });
+          }
           if (st.overflow) break;
           if (overflow) {
             sem_overflow = 1u;
