@@ -73,6 +73,10 @@ def parse_args() -> argparse.Namespace:
                         help="LiDAR frames timed after the camera workload (0: skip)")
     parser.add_argument("--lidar-sensors", type=int, default=None,
                         help="override the LiDAR sensor count (small profiling captures)")
+    parser.add_argument("--ragged-frames", type=int, default=20,
+                        help="frames of the ragged-batch workload (0: skip)")
+    parser.add_argument("--ragged-scale", type=float, default=1.0,
+                        help="scale scene sizes and camera counts of the ragged workload")
     return parser.parse_args()
 
 
@@ -449,6 +453,121 @@ def run_lidar(args, device, world: int, with_cpu: bool) -> dict:
     return result
 
 
+# --------------------------------------------------------------------------- ragged batch
+RAGGED_METRIC = "Mpix/s, ragged batch (one submission, CUDA graph) vs plain form (one render per resolution)"
+
+
+def run_ragged(args, device, world: int) -> dict:
+    """eight scenes (100k..3M Gaussians, SH3), 1,024 cameras
+    of mixed resolutions, a pose sequence.  The ragged form renders each frame
+    as one submission replayed from a CUDA graph; the plain form renders the
+    same frame through RendererService, one call per resolution (the fewest
+    calls the plain form allows: every scene can share a call)."""
+    from vgr_b200 import CustomCudaBackend, RendererService, workloads
+    from vgr_b200.ragged import RaggedBatch, autotune_tile_size
+
+    frames = max(args.ragged_frames, 2)
+    work = workloads.ragged_workload(frames=frames, scale=args.ragged_scale)
+    batch = len(work.heights)
+    pixels = sum(h * w for h, w in zip(work.heights, work.widths))
+    scene_ids = work.scene_ids.to(device)
+    intr = work.intrinsics.to(device)
+    poses = work.viewmats.to(device)
+
+    backend = CustomCudaBackend(sh_degree=3, output_srgb=False)
+    holder = RendererService(backend, height=16, width=16, max_views=1)
+    holder.initialize(stage=None, device=device)
+    for sid, scene in work.scenes:
+        holder.load_scene(sid, **scene.to(device).as_kwargs())
+    ragged = RaggedBatch(backend, work.heights, work.widths)
+    outputs = ragged.outputs()
+    view = poses[0].clone()
+    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16))
+    counters = ragged.calibrate(view, intr, scene_ids, outputs)
+    graph = ragged.capture(view, intr, scene_ids, outputs)
+    stream = torch.cuda.current_stream(device)
+    for k in range(min(3, frames)):
+        view.copy_(poses[k])
+        graph.replay()
+    torch.cuda.synchronize(device)
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(frames):
+        view.copy_(poses[k])
+        graph.replay()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    ragged_ms = max_over_ranks(start.elapsed_time(stop), world, device) / frames
+    check = ragged.check()
+    last = {name: t.clone() for name, t in outputs.items()}
+
+    # Plain form: one RendererService per resolution, all scenes registered.
+    groups: dict[tuple[int, int], list[int]] = {}
+    for c, hw in enumerate(zip(work.heights, work.widths)):
+        groups.setdefault(hw, []).append(c)
+    plain = []
+    for (h, w), cams in groups.items():
+        idx = torch.tensor(cams, device=device)
+        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=tile)
+        svc = RendererService(b, height=h, width=w, max_views=len(cams))
+        svc.initialize(stage=None, device=device)
+        for sid, scene in work.scenes:
+            svc.load_scene(sid, **scene.to(device).as_kwargs())
+        group_poses = poses[:, idx].contiguous()
+        group_intr = intr[idx].contiguous()
+        group_ids = scene_ids[idx].contiguous()
+        out = svc.prepare_outputs(len(cams))
+        svc.render(group_poses[0], group_intr, group_ids, outputs=out)
+        b.adaptive_capacity = False
+        plain.append((svc, b, group_poses, group_intr, group_ids, out, cams))
+    for k in range(min(3, frames)):
+        for svc, _, gp, gi, gs, out, _ in plain:
+            svc.render(gp[k], gi, gs, outputs=out)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    start.record(stream)
+    for k in range(frames):
+        for svc, _, gp, gi, gs, out, _ in plain:
+            svc.render(gp[k], gi, gs, outputs=out)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    plain_ms = max_over_ranks(start.elapsed_time(stop), world, device) / frames
+    overflow = any(b.check_capacity()["intersection_overflow"] or b.check_capacity()["visible_overflow"]
+                   for _, b, *_ in plain)
+    # Same last frame both ways: the per-camera images must agree.
+    max_abs = 0.0
+    for *_, out, cams in plain:
+        for j, c in enumerate(cams):
+            diff = (ragged.view(last, "rgb", c) - out["rgb"][j]).abs().max().item()
+            max_abs = max(max_abs, diff)
+    ragged_value = world * pixels / (ragged_ms / 1e3) / 1e6
+    plain_value = world * pixels / (plain_ms / 1e3) / 1e6
+    result = {
+        "metric": RAGGED_METRIC,
+        "value": round(ragged_value, 3),
+        "unit": "Mpix/s",
+        "frames": frames,
+        "ms_per_frame": round(ragged_ms, 3),
+        "plain_form_value": round(plain_value, 3),
+        "plain_form_ms_per_frame": round(plain_ms, 3),
+        "plain_form_calls_per_frame": len(plain),
+        "speedup_vs_plain": round(ragged_value / plain_value, 3),
+        "rgb_max_abs_vs_plain": max_abs,
+        "tile_size": tile,
+        "cuda_graph": True,
+        "config": {"workload": "ragged-8scenes-1024cams", "scene_gaussians": [s.means.shape[0] for _, s in work.scenes],
+                   "cameras": batch, "pixels_per_frame": pixels, "resolutions": sorted(groups),
+                   "visible_records": counters["visible_gaussians"],
+                   "tile_intersections": counters["tile_intersections"],
+                   "capacity_overflow": bool(check["visible_overflow"] or check["intersection_overflow"] or overflow)},
+    }
+    for svc, *_ in plain:
+        svc.shutdown()
+    holder.shutdown()
+    return result
+
+
 def run_b200(args) -> None:
     world, rank, local = dist_setup()
     if not torch.cuda.is_available():
@@ -592,6 +711,10 @@ def run_b200(args) -> None:
             "sample": f"{len(sample)} of {batch} cameras ({len(sample) * rig.height * rig.width} px), full scene, 1 render",
         }
 
+    ragged = None
+    if args.ragged_frames > 0:
+        ragged = run_ragged(args, device, world)
+
     lidar = None
     if args.lidar_steps > 0:
         lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
@@ -620,6 +743,7 @@ def run_b200(args) -> None:
             "cpu_baseline": cpu_baseline,
             "clocks": clocks,
             "capacity_check": {k: check[k] for k in ("visible_overflow", "intersection_overflow")},
+            "ragged": ragged,
             "lidar": lidar,
         }
         print(json.dumps(line), flush=True)

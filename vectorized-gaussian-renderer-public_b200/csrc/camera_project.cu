@@ -468,6 +468,14 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
     const CamPlan plan = s_plan;
     const int64_t local_begin = chunk * kProjectChunk;
     const bool live = plan.camera >= 0 && plan.scene_slot >= 0 && local_begin < plan.g_count;
+    if (!live && b != total_vblocks - 1) {
+      // A virtual block past its camera's scene (ragged scene sizes) or of an
+      // invalid camera adds nothing: publish its zero aggregate and move on
+      // (the last block still runs the look-back, as it owns the totals).
+      if (tid == 0) st_release_u64(desc + b, (b == 0 ? kDescInclusive : kDescAggregate));
+      __syncthreads();
+      continue;
+    }
 
     // Project both rounds first (no barrier), then one block scan of
     // (visible, tiles) over the kProjectChunk tasks in task order.

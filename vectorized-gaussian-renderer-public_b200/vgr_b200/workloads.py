@@ -241,3 +241,57 @@ def batched_workload(gaussians: int = 1_000_000, cameras: int = 64) -> tuple[Sce
     """Batched forward render: 1M Gaussians SH degree 3, 64 cameras 640x480."""
     scene = synthetic_scene(gaussians, seed=1, mean_half_extent=5.0, sh_degree=3)
     return scene, orbit_cameras(cameras, seed=2)
+
+
+# --------------------------------------------------------------------------- ragged batch
+RAGGED_SCENE_SIZES = (100_000, 250_000, 500_000, 750_000, 1_000_000, 1_500_000, 2_000_000, 3_000_000)
+RAGGED_CAMERAS_PER_SCENE = (32, 64, 96, 128, 128, 160, 160, 256)
+RAGGED_RESOLUTIONS = ((128, 128), (120, 160), (240, 320))  # (height, width)
+
+
+@dataclass
+class RaggedWorkload:
+    scenes: list[tuple[int, SceneTensors]]
+    scene_ids: torch.Tensor  # [B] int64, cameras grouped by scene
+    heights: list[int]
+    widths: list[int]
+    viewmats: torch.Tensor  # [F, B, 4, 4] per-frame world -> OpenCV camera
+    intrinsics: torch.Tensor  # [B, 3, 3]
+
+
+def ragged_workload(frames: int = 100, *, seed: int = 7, scale: float = 1.0) -> RaggedWorkload:
+    """Ragged batch: eight scenes of 100k..3M Gaussians (distributions of the
+    batched workload: means U[-5,5]^3, SH degree 3), 1,024 cameras split
+    32..256 per scene, each at a resolution drawn from 128x128 / 160x120 /
+    320x240, fx = fy = 0.75 W; poses at random positions inside the scene
+    bounds, yaw U[0, 2pi), pitch U[-15, 15] deg; each frame moves every
+    camera by N(0, 0.01) per axis and turns it by N(0, 0.5 deg).  ``scale``
+    shrinks scene sizes and camera counts for small checks."""
+    gen = torch.Generator().manual_seed(seed)
+    scenes = []
+    counts = []
+    for k, (size, cams) in enumerate(zip(RAGGED_SCENE_SIZES, RAGGED_CAMERAS_PER_SCENE)):
+        scenes.append((k, synthetic_scene(max(int(size * scale), 1), seed=100 + k, mean_half_extent=5.0,
+                                          sh_degree=3)))
+        counts.append(max(int(round(cams * scale)), 1))
+    batch = sum(counts)
+    scene_ids = torch.cat([torch.full((c,), k, dtype=torch.int64) for k, c in enumerate(counts)])
+    choice = torch.randint(0, len(RAGGED_RESOLUTIONS), (batch,), generator=gen)
+    heights = [RAGGED_RESOLUTIONS[int(i)][0] for i in choice]
+    widths = [RAGGED_RESOLUTIONS[int(i)][1] for i in choice]
+    pos = (torch.rand((batch, 3), generator=gen, dtype=torch.float64) * 2.0 - 1.0) * 5.0
+    yaw = torch.rand((batch,), generator=gen, dtype=torch.float64) * 2.0 * math.pi
+    pitch = (torch.rand((batch,), generator=gen, dtype=torch.float64) * 2.0 - 1.0) * math.radians(15.0)
+    views = []
+    for _ in range(frames):
+        direction = torch.stack(
+            (torch.cos(pitch) * torch.cos(yaw), torch.sin(pitch), torch.cos(pitch) * torch.sin(yaw)), dim=1
+        )
+        views.append(look_at_viewmats(pos, pos + direction))
+        pos = pos + torch.randn((batch, 3), generator=gen, dtype=torch.float64) * 0.01
+        yaw = yaw + torch.randn((batch,), generator=gen, dtype=torch.float64) * math.radians(0.5)
+    intr = torch.zeros((batch, 3, 3), dtype=torch.float32)
+    for c in range(batch):
+        w, h = widths[c], heights[c]
+        intr[c] = pinhole(1, 0.75 * w, 0.75 * w, w / 2.0, h / 2.0)[0]
+    return RaggedWorkload(scenes, scene_ids, heights, widths, torch.stack(views).contiguous(), intr)
