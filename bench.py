@@ -500,6 +500,13 @@ def run_ragged(args, device, world: int) -> dict:
     torch.cuda.synchronize(device)
     ragged_ms = max_over_ranks(start.elapsed_time(stop), world, device) / frames
     check = ragged.check()
+    # Stage breakdown of one frame outside the graph (live CUDA events).
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(STAGES) + 1)]
+    ragged.set_stage_events(marks)
+    ragged.render(view, intr, scene_ids, outputs)
+    ragged.set_stage_events(None)
+    torch.cuda.synchronize(device)
+    ragged_stages = {name: round(marks[k].elapsed_time(marks[k + 1]), 3) for k, name in enumerate(STAGES)}
     last = {name: t.clone() for name, t in outputs.items()}
 
     # Plain form: one RendererService per resolution, all scenes registered.
@@ -555,6 +562,8 @@ def run_ragged(args, device, world: int) -> dict:
         "speedup_vs_plain": round(ragged_value / plain_value, 3),
         "rgb_max_abs_vs_plain": max_abs,
         "tile_size": tile,
+        "autotune_ms": {str(k): round(v, 3) for k, v in ragged.autotune_ms.items()},
+        "stage_ms": ragged_stages,
         "cuda_graph": True,
         "config": {"workload": "ragged-8scenes-1024cams", "scene_gaussians": [s.means.shape[0] for _, s in work.scenes],
                    "cameras": batch, "pixels_per_frame": pixels, "resolutions": sorted(groups),

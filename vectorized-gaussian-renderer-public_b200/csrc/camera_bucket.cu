@@ -17,9 +17,10 @@
 //                         bucket with an atomic cursor;
 //   tile_sort_kernel      one CTA per tile orders its bucket by (depth bits,
 //                         record index) - in shared memory when it holds at
-//                         most kTileSortCap pairs, else in chunks through
-//                         global memory - and writes the sorted keys and
-//                         record indices.
+//                         most kTileSortCap pairs, else split by depth
+//                         through global memory into runs sorted in shared
+//                         memory - and writes the sorted keys and record
+//                         indices.
 // Within a tile the record index increases with the Gaussian id (records are
 // compacted in Gaussian order per camera), so (depth bits, record) is the
 // reference order, and it is a total order: the arbitrary order in which the
@@ -264,8 +265,10 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(BucketParams p) {
 // then insertion-sorted by the full 64-bit entry by the thread that owns it),
 // which costs one pass and a handful of barriers.  A bucket whose largest
 // split exceeds kMaxSplit (many equal or nearly equal depths) is sorted by
-// stable LSD passes over the record word and then the depth word instead;
-// so is every bucket above kTileSortCap, in chunks through global memory.
+// stable LSD passes over the record word and then the depth word instead.
+// Buckets above kTileSortCap are split the same way through global memory
+// into runs that fit in shared memory; only a single split above
+// kTileSortCap takes chunked LSD passes through global memory.
 __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketParams p) {
   constexpr int kSplitBits = 11;
   constexpr int kSplits = 1 << kSplitBits;
@@ -306,6 +309,62 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
   uint64_t it[kTileSortItems];
   uint32_t dr[kTileSortItems];
   uint32_t dmin = 0xffffffffu, dmax = 0u, rmin = 0xffffffffu, rmax = 0u;
+
+  // Stable LSD over the full entry (record word, then depth word) of
+  // count <= kTileSortCap entries read from src, leaving them sorted in
+  // s_items.  Items are held warp-blocked (element (w * K + k) * 32 + l) for
+  // the stable ranking; s_u.rank must be free (not holding split counters).
+  auto lsd_run = [&](const uint64_t* src, int count) {
+    const int K = (count + kTileSortThreads - 1) / kTileSortThreads;
+    for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
+      (&s_u.rank.warp_hist[0][0])[i] = 0u;
+    }
+    uint32_t dl = 0xffffffffu, dh = 0u, rl = 0xffffffffu, rh = 0u;
+#pragma unroll
+    for (int k = 0; k < kTileSortItems; ++k) {
+      if (k >= K) break;
+      const int idx = (warp * K + k) * 32 + lane;
+      if (idx < count) {
+        it[k] = src[idx];
+        dl = min(dl, static_cast<uint32_t>(it[k] >> 32));
+        dh = max(dh, static_cast<uint32_t>(it[k] >> 32));
+        rl = min(rl, static_cast<uint32_t>(it[k]));
+        rh = max(rh, static_cast<uint32_t>(it[k]));
+      }
+    }
+    block_minmax(dl, dh, rl, rh, s_minmax);
+    __syncthreads();  // s_minmax is reused by the next run
+    const int passes_d = (bit_length_u32(dh - dl) + kRadixBits - 1) / kRadixBits;
+    const int passes_r = (bit_length_u32(rh - rl) + kRadixBits - 1) / kRadixBits;
+    if (passes_r + passes_d == 0) {
+      for (int i = tid; i < count; i += kTileSortThreads) s_items[i] = src[i];
+      __syncthreads();
+      return;
+    }
+    for (int q = 0; q < passes_r + passes_d; ++q) {
+      const PassDigit dig = q < passes_r ? PassDigit{1, rl, q * kRadixBits}
+                                         : PassDigit{0, dl, (q - passes_r) * kRadixBits};
+      rank_chunk(it, dr, K, count, dig, s_u.rank);
+#pragma unroll
+      for (int k = 0; k < kTileSortItems; ++k) {
+        if (k >= K) break;
+        const uint32_t d = dr[k] >> 16;
+        if (d != kNoDigit) {
+          s_items[s_u.rank.digit_start[d] + s_u.rank.warp_hist[warp][d] + (dr[k] & 0xffffu)] = it[k];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kTileSortItems; ++k) {
+        if (k >= K) break;
+        const int idx = (warp * K + k) * 32 + lane;
+        if (idx < count) it[k] = s_items[idx];
+      }
+#pragma unroll
+      for (int w = 0; w < kTsWarps; ++w) s_u.rank.warp_hist[w][tid] = 0u;
+      __syncthreads();
+    }
+  };
 
   if (n <= kTileSortCap) {
     // ------------------------------------------------ split + insertion sort
@@ -405,44 +464,8 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
       __syncthreads();
     } else {
       // ------------------------------------------- stable LSD in shared memory
-      // Items are re-read warp-blocked (element (w * K + k) * 32 + l) for the
-      // stable ranking.
       __syncthreads();  // the split counters share storage with the rank state
-      for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
-        (&s_u.rank.warp_hist[0][0])[i] = 0u;
-      }
-#pragma unroll
-      for (int k = 0; k < kTileSortItems; ++k) {
-        if (k >= K) break;
-        const int idx = (warp * K + k) * 32 + lane;
-        if (idx < n) it[k] = bucket[idx];
-      }
-      __syncthreads();
-      const int passes_d = (range_bits + kRadixBits - 1) / kRadixBits;
-      const int passes_r = (bit_length_u32(rmax - rmin) + kRadixBits - 1) / kRadixBits;
-      for (int q = 0; q < passes_r + passes_d; ++q) {
-        const PassDigit dig = q < passes_r ? PassDigit{1, rmin, q * kRadixBits}
-                                           : PassDigit{0, dmin, (q - passes_r) * kRadixBits};
-        rank_chunk(it, dr, K, n, dig, s_u.rank);
-#pragma unroll
-        for (int k = 0; k < kTileSortItems; ++k) {
-          if (k >= K) break;
-          const uint32_t d = dr[k] >> 16;
-          if (d != kNoDigit) {
-            s_items[s_u.rank.digit_start[d] + s_u.rank.warp_hist[warp][d] + (dr[k] & 0xffffu)] = it[k];
-          }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kTileSortItems; ++k) {
-          if (k >= K) break;
-          const int idx = (warp * K + k) * 32 + lane;
-          if (idx < n) it[k] = s_items[idx];
-        }
-#pragma unroll
-        for (int w = 0; w < kTsWarps; ++w) s_u.rank.warp_hist[w][tid] = 0u;
-        __syncthreads();
-      }
+      lsd_run(bucket, n);
     }
     for (int i = tid; i < n; i += kTileSortThreads) {
       const uint64_t v = s_items[i];
@@ -453,7 +476,124 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
   }
 
   // ------------------------------------------------------------ large buckets
-  // Stable chunked LSD over the full entry through global memory,
+  // Split by the top kSplitBits bits of the tile's depth range through global
+  // memory (count, then scatter into the same range of the temp buffer with
+  // shared-memory cursors), then sort runs of whole splits in shared memory:
+  // one insertion sort per split when every split is short, else stable LSD
+  // passes over each run.  Two passes over the bucket.
+  {
+    uint32_t dlo = 0xffffffffu, dhi = 0u, rlo = 0xffffffffu, rhi = 0u;
+    for (int b = tid; b < kSplits; b += kTileSortThreads) s_u.split[b] = 0u;
+    for (int i = tid; i < n; i += kTileSortThreads) {
+      const uint32_t dw = static_cast<uint32_t>(bucket[i] >> 32);
+      dlo = min(dlo, dw);
+      dhi = max(dhi, dw);
+    }
+    block_minmax(dlo, dhi, rlo, rhi, s_minmax);
+    const int range_bits = bit_length_u32(dhi - dlo);
+    const int shift = range_bits > kSplitBits ? range_bits - kSplitBits : 0;
+    for (int i = tid; i < n; i += kTileSortThreads) {
+      atomicAdd(&s_u.split[(static_cast<uint32_t>(bucket[i] >> 32) - dlo) >> shift], 1u);
+    }
+    __syncthreads();
+    uint32_t c[kSplitsPerThread];
+    {
+      const uint4 lo4 = reinterpret_cast<const uint4*>(s_u.split)[tid * 2];
+      const uint4 hi4 = reinterpret_cast<const uint4*>(s_u.split)[tid * 2 + 1];
+      c[0] = lo4.x; c[1] = lo4.y; c[2] = lo4.z; c[3] = lo4.w;
+      c[4] = hi4.x; c[5] = hi4.y; c[6] = hi4.z; c[7] = hi4.w;
+    }
+    uint32_t sum = 0, big = 0;
+#pragma unroll
+    for (int j = 0; j < kSplitsPerThread; ++j) {
+      sum += c[j];
+      big = max(big, c[j]);
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    big = __reduce_max_sync(0xffffffffu, big);
+    if (lane == 31) s_scan[warp] = incl;
+    if (lane == 0) s_big[warp] = big;
+    __syncthreads();
+    uint32_t prefix = incl - sum;
+#pragma unroll
+    for (int w = 0; w < kTsWarps; ++w) {
+      prefix += w < warp ? s_scan[w] : 0u;
+      big = max(big, s_big[w]);
+    }
+    if (big <= static_cast<uint32_t>(kTileSortCap)) {
+      uint32_t off[kSplitsPerThread];
+#pragma unroll
+      for (int j = 0; j < kSplitsPerThread; ++j) {
+        off[j] = prefix;
+        prefix += c[j];
+      }
+      __syncthreads();  // every thread has read its counters
+      reinterpret_cast<uint4*>(s_off)[tid * 2] = make_uint4(off[0], off[1], off[2], off[3]);
+      reinterpret_cast<uint4*>(s_off)[tid * 2 + 1] = make_uint4(off[4], off[5], off[6], off[7]);
+      reinterpret_cast<uint4*>(s_u.split)[tid * 2] = make_uint4(off[0], off[1], off[2], off[3]);
+      reinterpret_cast<uint4*>(s_u.split)[tid * 2 + 1] = make_uint4(off[4], off[5], off[6], off[7]);
+      __syncthreads();
+      uint64_t* split_buf = p.temp + start;
+      for (int i = tid; i < n; i += kTileSortThreads) {
+        const uint64_t v = bucket[i];
+        split_buf[atomicAdd(&s_u.split[(static_cast<uint32_t>(v >> 32) - dlo) >> shift], 1u)] = v;
+      }
+      __syncthreads();
+      // Runs of whole splits that fit in shared memory, in split order.
+      int first = 0;
+      while (first < kSplits) {
+        const int base = static_cast<int>(s_off[first]);
+        int lo = first + 1, hi = kSplits;  // the run is [first, last): largest last in [lo, hi]
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          const int end_mid = mid < kSplits ? static_cast<int>(s_off[mid]) : n;
+          if (end_mid - base <= kTileSortCap) lo = mid; else hi = mid - 1;
+        }
+        const int last = lo;
+        const int count = (last < kSplits ? static_cast<int>(s_off[last]) : n) - base;
+        if (big > kMaxSplit) {
+          // Some split is too long for an insertion sort: order the run by
+          // stable LSD passes instead (same result, the run is a whole number
+          // of splits).
+          lsd_run(split_buf + base, count);
+        } else {
+        for (int i = tid; i < count; i += kTileSortThreads) s_items[i] = split_buf[base + i];
+        __syncthreads();
+        for (int sp = first + tid; sp < last; sp += kTileSortThreads) {
+          const int a0 = static_cast<int>(s_off[sp]) - base;
+          const int a1 = (sp + 1 < kSplits ? static_cast<int>(s_off[sp + 1]) : n) - base;
+          for (int a = a0 + 1; a < a1; ++a) {
+            const uint64_t v = s_items[a];
+            int b = a - 1;
+            while (b >= a0 && s_items[b] > v) {
+              s_items[b + 1] = s_items[b];
+              --b;
+            }
+            s_items[b + 1] = v;
+          }
+        }
+        __syncthreads();
+        }
+        for (int i = tid; i < count; i += kTileSortThreads) {
+          const uint64_t v = s_items[i];
+          p.keys_out[start + base + i] = key_tile | (v >> 32);
+          p.values_out[start + base + i] = static_cast<int32_t>(static_cast<uint32_t>(v));
+        }
+        __syncthreads();
+        first = last;
+      }
+      return;
+    }
+    __syncthreads();  // the split counters share storage with the rank state below
+  }
+
+  // A single split above kTileSortCap (many equal or nearly equal depths):
+  // stable chunked LSD over the full entry through global memory,
   // ping-ponging between the bucket and the same range of the temp buffer.
   constexpr int kChunkItems = 8;
   constexpr int kChunk = kTileSortThreads * kChunkItems;

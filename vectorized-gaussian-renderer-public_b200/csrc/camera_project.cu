@@ -27,8 +27,10 @@ struct __align__(16) CamConst {
   float fx, fy, cx, cy;
   float lim_xp, lim_xn, lim_yp, lim_yn;
   float width, height;
+  float r_scale2;   // upper bound of the largest eigenvalue of R^T R (1 for a rotation)
+  float pad[3];
 };
-static_assert(sizeof(CamConst) == 96, "CamConst is twelve 8-byte words");
+static_assert(sizeof(CamConst) == 112, "CamConst is fourteen 8-byte words");
 
 __device__ __forceinline__ void make_cam_const(const float* view, const float* env,
                                                const float* intr, int width, int height,
@@ -59,6 +61,21 @@ __device__ __forceinline__ void make_cam_const(const float* view, const float* e
   c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
   c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
   c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
+  // Gershgorin bound of R^T R (R includes any scale of the object->world
+  // transform); used only by the conservative early cull.
+  float bound = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float row = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float m = c->r[i] * c->r[j] + c->r[3 + i] * c->r[3 + j] + c->r[6 + i] * c->r[6 + j];
+      row += fabsf(m);
+    }
+    bound = fmaxf(bound, row);
+  }
+  c->r_scale2 = bound * 1.001f;
+  c->pad[0] = c->pad[1] = c->pad[2] = 0.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -204,6 +221,27 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
 
   const float* s = covariances + g * 6;
   const float s00 = s[0], s01 = s[1], s02 = s[2], s11 = s[3], s12 = s[4], s22 = s[5];
+  {
+    // Early off-screen cull, conservative so that it never drops a record
+    // the full test below keeps.  The x-row of the Jacobian has squared norm
+    // (fx/z)^2 (1 + clamp(x/z)^2) <= (fx/z)^2 (1 + L^2), the camera-space
+    // covariance R S R^T has largest eigenvalue at most trace(S) times the
+    // bound of R^T R's largest eigenvalue (r_scale2), and the extent
+    // factor is at most support_sigma, so the pixel radius is below
+    // R = support_sigma * sqrt((fx/z)^2 (1 + L^2) trace + eps) (+ margins
+    // for rounding and the ceiling).  Rounding is monotone, so
+    // u + R <= 0 implies u + radius <= 0 as computed below, and likewise
+    // for the other three sides.
+    const float trace = (s00 + s11 + s22) * c.r_scale2;
+    const float lx = fmaxf(c.lim_xp, c.lim_xn), ly = fmaxf(c.lim_yp, c.lim_yn);
+    const float gx = c.fx * iz, gy = c.fy * iz;
+    const float bx = support_sigma * sqrtf(gx * gx * (1.0f + lx * lx) * trace + cov_eps) * 1.01f + 2.0f;
+    const float by = support_sigma * sqrtf(gy * gy * (1.0f + ly * ly) * trace + cov_eps) * 1.01f + 2.0f;
+    if (fadd(u, bx) <= 0.0f || fadd(v, by) <= 0.0f || fsub(u, bx) >= c.width ||
+        fsub(v, by) >= c.height) {
+      return false;
+    }
+  }
   float tm[9];
 #pragma unroll
   for (int row = 0; row < 3; ++row) {
@@ -444,7 +482,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   const int64_t total_vblocks = p.total_vblocks;
   while (true) {
     // Warp 0 takes the ticket and stages the slot's plan (7 words) and
-    // projection constants (12 words) with one load per lane.
+    // projection constants (14 words) with one load per lane.
     if (warp == 0) {
       int64_t ticket = 0;
       if (lane == 0) ticket = atomicAdd(&header->project_queue, 1u);
@@ -454,7 +492,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         if (lane < 7) {
           reinterpret_cast<uint64_t*>(&s_plan)[lane] =
               reinterpret_cast<const uint64_t*>(plans + slot)[lane];
-        } else if (lane < 19) {
+        } else if (lane < 21) {
           reinterpret_cast<uint64_t*>(&s_cam)[lane - 7] =
               reinterpret_cast<const uint64_t*>(cam_consts + slot)[lane - 7];
         }

@@ -79,7 +79,7 @@ __host__ __device__ inline int64_t align_up(int64_t v, int64_t a) {
 struct ScratchLayout {
   int64_t header;         // ScratchHeader
   int64_t plans;          // CamPlan[A]
-  int64_t cam_consts;     // CamConst[A] (96 bytes each)
+  int64_t cam_consts;     // CamConst[A] (112 bytes each)
   int64_t tile_prefix;    // int64[A+1] exclusive prefix of tiles over active slots
   int64_t project_desc;   // uint64[vblocks]
   int64_t sort_hist;      // uint32[passes][256]
@@ -102,7 +102,7 @@ __host__ __device__ inline ScratchLayout make_scratch_layout(
   l.plans = off;
   off = align_up(off + max_active_cameras * static_cast<int64_t>(sizeof(CamPlan)), 256);
   l.cam_consts = off;
-  off = align_up(off + max_active_cameras * 96, 256);
+  off = align_up(off + max_active_cameras * 112, 256);
   l.tile_prefix = off;
   off = align_up(off + (max_active_cameras + 1) * 8, 256);
   l.project_desc = off;

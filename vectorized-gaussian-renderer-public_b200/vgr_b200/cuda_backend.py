@@ -686,7 +686,7 @@ class CustomCudaBackend:
 
     def set_stage_events(self, events: list[torch.cuda.Event] | None) -> None:
         """Record ``events[i]`` at stage boundary i of every native render
-        (start, setup, projection, sort histogram, radix passes, ranges,
+        (start, setup, projection, tile scan, bucket scatter, tile sort,
         compositor); None disables.  Used for live per-kernel timing."""
         if events is None:
             self._stage_event_handles = None

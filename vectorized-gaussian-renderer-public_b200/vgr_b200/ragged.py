@@ -65,6 +65,8 @@ class RaggedBatch:
         self.tile_size = int(tile_size or backend.tile_size)
         self._visible_capacity = 0
         self._intersection_capacity = 0
+        self._stage_events = None
+        self.autotune_ms: dict[int, float] = {}
         self.workspace: dict[str, torch.Tensor] = {}
         pixel_offsets = [0]
         for h, w in zip(self.heights, self.widths):
@@ -237,9 +239,27 @@ class RaggedBatch:
             sh_degree=-1 if b.sh_degree is None else b.sh_degree,
             sorted_buffer_hint=1,
         )
+        if self._stage_events is not None:
+            options.stage_events = self._stage_events
+            options.stage_event_count = _native.STAGE_EVENTS
         selector = _native._c_i64(1)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _native.check(lib.vgr_render(scene, cams, outs, native_ws, options, stream, selector), "ragged render")
+
+    def set_stage_events(self, events: list[torch.cuda.Event] | None) -> None:
+        """Record ``events[i]`` at the native stage boundaries of every render
+        (as ``CustomCudaBackend.set_stage_events``); None disables."""
+        if events is None:
+            self._stage_events = None
+            return
+        if len(events) != _native.STAGE_EVENTS:
+            raise ValueError(f"need {_native.STAGE_EVENTS} events")
+        stream = torch.cuda.current_stream(self.device)
+        for event in events:
+            event.record(stream)  # materialise the handle
+        handles = (_native._c_p * len(events))(*[event.cuda_event for event in events])
+        self._events_keepalive = list(events)
+        self._stage_events = handles
 
     def read_counters(self) -> dict[str, int]:
         values = self.workspace["counters"].detach().cpu().tolist()
@@ -341,6 +361,7 @@ def autotune_tile_size(
         stop.record(stream)
         stop.synchronize()
         ms = start.elapsed_time(stop) / repeats
+        ragged.autotune_ms[tile] = ms
         if ms < best_ms:
             best, best_ms = tile, ms
     assert best is not None
