@@ -329,6 +329,10 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
   }
 
   const int64_t vblocks = render_vblocks(active, scene->max_scene_gaussians);
+  if (vblocks >= static_cast<int64_t>(UINT32_MAX)) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "active cameras x max_scene_gaussians exceeds 2^41 projection tasks");
+  }
   const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, vblocks, false);
   if (ws->scratch_bytes < layout.total) {
     return fail(VGR_ERR_SCRATCH_TOO_SMALL,
