@@ -159,8 +159,10 @@ const char* vgr_last_error(void);
 
 /* Scratch bytes vgr_render needs for a given intersection capacity, projection
  * task bound (active cameras * max scene Gaussians), global tile count and
- * active-camera bound.  No counterpart in the reference: the reference sizes
- * CUB temporary storage through the two functions below. */
+ * active-camera bound.  The size depends on the active-camera bound (per-camera
+ * plans and projection constants) and a constant part; the other bounds are
+ * accepted for interface stability.  No counterpart in the reference: the
+ * reference sizes CUB temporary storage through the two functions below. */
 int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
                                  int64_t max_projection_tasks,
                                  int64_t global_tiles,
@@ -223,10 +225,9 @@ int vgr_render(const vgr_scene* scene, const vgr_cameras* cameras,
  * workspace exactly as for vgr_render; workspace->scratch and scratch_bytes
  * are ignored and a VGR_STATIC_SCRATCH_BYTES array inside the library is used
  * instead (every GPU that loads the library keeps it until exit).  The
- * scratch grows with the projection work (8 bytes per 512 (camera, Gaussian)
- * tasks, 64 bytes per active camera), not with the intersections: renders of
- * more than about 2^31 tasks (e.g. 64 cameras x 16M Gaussians) fail with
- * VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
+ * scratch grows with the active cameras (160 bytes each, plus about 9 KB),
+ * not with the scene or the intersections: a render of more than about
+ * 104,000 active cameras fails with VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
  * the array: calls ordered on one stream are fine, calls that overlap on the
  * GPU race.  The first call on a device looks the array's address up while
  * that device is current; make it before any stream capture. */

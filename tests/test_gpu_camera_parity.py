@@ -221,6 +221,30 @@ def test_partial_depth_ties_in_shared_memory_buckets():
     assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
 
 
+@pytest.mark.parametrize("count", [2_400, 16_000])
+def test_paired_depth_ties_in_radix_sorted_buckets(count):
+    # Most Gaussians sit in a thin depth band (splits above the insertion-sort
+    # limit, so buckets take the radix passes) and come in pairs at the same
+    # position: short runs of equal depth inside radix-sorted buckets, below
+    # (2,400) and above (16,000) the shared-memory capacity.
+    scene = synthetic_scene(count, seed=64, mean_half_extent=0.05, log_scale_mean=-5.0)
+    gen = torch.Generator().manual_seed(5)
+    band = torch.arange(count // 2, dtype=torch.float32) * 1e-6
+    spread = (torch.rand((count // 2,), generator=gen) - 0.5) * 0.04
+    z = torch.where(torch.arange(count // 2) % 5 == 0, spread, band)
+    scene.means[0::2, 2] = z
+    scene.means[1::2] = scene.means[0::2]
+    rig = _dense_cluster_rig()
+    gpu = render_gpu([(0, scene)], rig, [0])
+    cpu = render_oracle([(0, scene)], rig, [0], with_tiles=True)
+    if count > 6_000:
+        assert cpu.tile_counts.max() > 4096
+    else:
+        assert 1 < cpu.tile_counts.max() <= 3072
+    _compare(gpu, cpu)
+    assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
+
+
 def test_large_tile_grid_bitwise():
     # 19,200 4x4-pixel tiles over four 320x240 cameras.
     scene = synthetic_scene(20_000, seed=71, mean_half_extent=1.5, log_scale_mean=-3.5)

@@ -21,7 +21,7 @@ import pytest
 import torch
 
 from vgr_b200 import CustomCudaBackend, RendererService, _native
-from vgr_b200.workloads import orbit_cameras, synthetic_scene
+from vgr_b200.workloads import CameraRig, orbit_cameras, pinhole, synthetic_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -40,7 +40,7 @@ def _setup():
     return device, rig, backend
 
 
-def _structs(device, rig, backend, intersection_capacity=None, max_scene_gaussians=None):
+def _structs(device, rig, backend, intersection_capacity=None, max_scene_gaussians=None, tiles=None):
     packed = backend._packed_scene
     ws = backend.workspace
     batch = rig.viewmats.shape[0]
@@ -50,7 +50,7 @@ def _structs(device, rig, backend, intersection_capacity=None, max_scene_gaussia
     scene_ids = torch.full((batch,), 4, dtype=torch.int64, device=device)
     icap = intersection_capacity or backend.current_intersection_capacity
     vcap = backend.current_visible_capacity
-    tiles = ws["tile_starts"].numel()
+    tiles = max(tiles or 0, ws["tile_starts"].numel())
     buffers = {
         "records": torch.empty((vcap, 12), dtype=torch.float32, device=device),
         "keys_in": torch.empty((icap,), dtype=torch.uint64, device=device),
@@ -165,9 +165,13 @@ def test_static_scratch_matches_vgr_render_twice_in_a_row():
 def test_static_scratch_refuses_oversized_render():
     device, rig, backend = _setup()
     lib = _native.load_library()
-    # A scene bound of 2^31 - 1 Gaussians needs 4.2M projection look-back
-    # descriptors per camera, far past the 16 MiB array.
-    structs = _structs(device, rig, backend, max_scene_gaussians=2**31 - 1)
+    # The array holds the plans and projection constants of about 104,000
+    # active cameras (160 bytes each); 120,000 one-pixel cameras need more.
+    count = 120_000
+    view = torch.eye(4).repeat(count, 1, 1)
+    view[:, 2, 3] = 5.0
+    big_rig = CameraRig(view.contiguous(), pinhole(count, 1.0, 1.0, 0.5, 0.5), 1, 1)
+    structs = _structs(device, big_rig, backend, tiles=count)
     structs[5]["counters"].fill_(-1)
     code, _ = _call(lib.vgr_render_static_scratch, device, structs)
     assert code == _native.VGR_ERR_SCRATCH_TOO_SMALL

@@ -30,6 +30,8 @@
 // Traffic per key: 12 bytes read and 8 written by the scatter, 8 read and 12
 // written by the tile sort, against 24 bytes per radix pass (6 passes for a
 // 44-bit key at 64 cameras of 640x480) of the global sort.
+#include <type_traits>
+
 #include "../../include/vgr_b200.h"
 #include "vgr_kernels.h"
 
@@ -205,6 +207,15 @@ __global__ void __launch_bounds__(kTileScanThreads) tile_scan_kernel(BucketParam
   if (tid == 0) {
     header->bucket_total = s_carry;
     p.counters[VGR_COUNTER_ACTIVE_TILES] = static_cast<int64_t>(s_active);
+    // Frame counters from the projection's reservations.
+    const uint64_t tv = header->visible_total;
+    const uint64_t ti = header->isect_total;
+    const uint64_t vcap = static_cast<uint64_t>(p.visible_capacity);
+    const uint64_t icap = static_cast<uint64_t>(p.capacity);
+    p.counters[0] = static_cast<int64_t>(tv);
+    p.counters[1] = static_cast<int64_t>(ti);
+    p.counters[2] = tv > vcap ? static_cast<int64_t>(tv - vcap) : 0;
+    p.counters[3] = ti > icap ? static_cast<int64_t>(ti - icap) : 0;
   }
 }
 
@@ -257,7 +268,7 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(BucketParams p) {
   }
 }
 
-// One CTA per tile: order the bucket by (depth bits, record index).
+// One CTA per tile: order the bucket by (depth bits, Gaussian id).
 //
 // Buckets of at most kTileSortCap entries stay in shared memory.  The common
 // path splits them by the top kSplitBits bits of the tile's depth range with
@@ -265,7 +276,8 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(BucketParams p) {
 // then insertion-sorted by the full 64-bit entry by the thread that owns it),
 // which costs one pass and a handful of barriers.  A bucket whose largest
 // split exceeds kMaxSplit (many equal or nearly equal depths) is sorted by
-// stable LSD passes over the record word and then the depth word instead.
+// stable LSD passes over the depth bits instead, after which runs of equal
+// depth bits are ordered by Gaussian id.
 // Buckets above kTileSortCap are split the same way through global memory
 // into runs that fit in shared memory; only a single split above
 // kTileSortCap takes chunked LSD passes through global memory.
@@ -285,6 +297,7 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
   __shared__ uint32_t s_minmax[4][kTsWarps];
   __shared__ uint32_t s_scan[kTsWarps];
   __shared__ uint32_t s_big[kTsWarps];
+  __shared__ uint32_t s_run_count;
 
   const int64_t tile = blockIdx.x;
   const int64_t start = p.tile_starts[tile];
@@ -310,40 +323,54 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
   uint32_t dr[kTileSortItems];
   uint32_t dmin = 0xffffffffu, dmax = 0u, rmin = 0xffffffffu, rmax = 0u;
 
-  // Stable LSD over the full entry (record word, then depth word) of
-  // count <= kTileSortCap entries read from src, leaving them sorted in
-  // s_items.  Items are held warp-blocked (element (w * K + k) * 32 + l) for
-  // the stable ranking; s_u.rank must be free (not holding split counters).
-  auto lsd_run = [&](const uint64_t* src, int count) {
+  // Order of two entries of this tile: depth bits, then Gaussian id (the
+  // reference's tie-break; ids are unique within a camera, so the order is
+  // total).  The id is read from the record only when the depths are equal.
+  const Record* records = p.records;
+  auto gaussian_id = [&](uint64_t e) -> uint32_t {
+    return __float_as_uint(__ldg(&records[static_cast<uint32_t>(e)].b).w);
+  };
+  auto greater = [&](uint64_t a, uint64_t b) -> bool {
+    const uint32_t da = static_cast<uint32_t>(a >> 32);
+    const uint32_t db = static_cast<uint32_t>(b >> 32);
+    if (da != db) return da > db;
+    return gaussian_id(a) > gaussian_id(b);
+  };
+
+  // Stable LSD of count <= kTileSortCap entries read from src, leaving them
+  // sorted in s_items.  by_gid false: passes over the depth bits only (equal
+  // depths keep the order of src).  by_gid true: passes over the Gaussian id
+  // (placed in the high word for the passes), then over the depth bits.
+  // Items are held warp-blocked (element (w * K + k) * 32 + l) for the stable
+  // ranking; s_u.rank must be free (not holding split counters).
+  auto lsd_run = [&](const uint64_t* src, int count, auto by_gid_tag) {
+    constexpr bool by_gid = decltype(by_gid_tag)::value;
     const int K = (count + kTileSortThreads - 1) / kTileSortThreads;
     for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
       (&s_u.rank.warp_hist[0][0])[i] = 0u;
     }
-    uint32_t dl = 0xffffffffu, dh = 0u, rl = 0xffffffffu, rh = 0u;
+    uint32_t gl = 0xffffffffu, gh = 0u, dl = 0xffffffffu, dh = 0u;
 #pragma unroll
     for (int k = 0; k < kTileSortItems; ++k) {
       if (k >= K) break;
       const int idx = (warp * K + k) * 32 + lane;
       if (idx < count) {
-        it[k] = src[idx];
-        dl = min(dl, static_cast<uint32_t>(it[k] >> 32));
-        dh = max(dh, static_cast<uint32_t>(it[k] >> 32));
-        rl = min(rl, static_cast<uint32_t>(it[k]));
-        rh = max(rh, static_cast<uint32_t>(it[k]));
+        const uint64_t v = src[idx];
+        if constexpr (by_gid) {
+          const uint32_t g = gaussian_id(v);
+          it[k] = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(v);
+          gl = min(gl, g);
+          gh = max(gh, g);
+        } else {
+          it[k] = v;
+        }
+        dl = min(dl, static_cast<uint32_t>(v >> 32));
+        dh = max(dh, static_cast<uint32_t>(v >> 32));
       }
     }
-    block_minmax(dl, dh, rl, rh, s_minmax);
+    block_minmax(gl, gh, dl, dh, s_minmax);
     __syncthreads();  // s_minmax is reused by the next run
-    const int passes_d = (bit_length_u32(dh - dl) + kRadixBits - 1) / kRadixBits;
-    const int passes_r = (bit_length_u32(rh - rl) + kRadixBits - 1) / kRadixBits;
-    if (passes_r + passes_d == 0) {
-      for (int i = tid; i < count; i += kTileSortThreads) s_items[i] = src[i];
-      __syncthreads();
-      return;
-    }
-    for (int q = 0; q < passes_r + passes_d; ++q) {
-      const PassDigit dig = q < passes_r ? PassDigit{1, rl, q * kRadixBits}
-                                         : PassDigit{0, dl, (q - passes_r) * kRadixBits};
+    auto pass = [&](PassDigit dig) {
       rank_chunk(it, dr, K, count, dig, s_u.rank);
 #pragma unroll
       for (int k = 0; k < kTileSortItems; ++k) {
@@ -363,6 +390,112 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
 #pragma unroll
       for (int w = 0; w < kTsWarps; ++w) s_u.rank.warp_hist[w][tid] = 0u;
       __syncthreads();
+    };
+    const int passes_d = (bit_length_u32(dh - dl) + kRadixBits - 1) / kRadixBits;
+    if constexpr (by_gid) {
+      const int passes_g = (bit_length_u32(gh - gl) + kRadixBits - 1) / kRadixBits;
+      for (int q = 0; q < passes_g; ++q) pass(PassDigit{0, gl, q * kRadixBits});
+#pragma unroll
+      for (int k = 0; k < kTileSortItems; ++k) {
+        if (k >= K) break;
+        const int idx = (warp * K + k) * 32 + lane;
+        if (idx < count) {
+          const uint32_t r = static_cast<uint32_t>(it[k]);
+          const uint32_t depth = __float_as_uint(__ldg(&records[r].b).z);
+          it[k] = (static_cast<uint64_t>(depth) << 32) | r;
+        }
+      }
+    }
+    for (int q = 0; q < passes_d; ++q) pass(PassDigit{0, dl, q * kRadixBits});
+#pragma unroll
+    for (int k = 0; k < kTileSortItems; ++k) {
+      if (k >= K) break;
+      const int idx = (warp * K + k) * 32 + lane;
+      if (idx < count) s_items[idx] = it[k];
+    }
+    __syncthreads();
+  };
+
+  // Stable LSD by the depth bits, then runs of equal depth bits ordered by
+  // Gaussian id: each run is insertion-sorted by the thread that finds its
+  // first entry; a run longer than kMaxTieRun sends the whole range through
+  // the LSD passes again with the Gaussian id as the second key.
+  auto lsd_sort = [&](const uint64_t* src, int count) {
+    constexpr int kMaxTieRun = 32;
+    if (tid == 0) s_run_count = 0u;  // read after the barriers inside lsd_run
+    lsd_run(src, count, std::false_type{});
+    auto depth_at = [&](int i) { return static_cast<uint32_t>(s_items[i] >> 32); };
+    auto run_end = [&](int i) {
+      // End of the run of equal depth bits that starts at i, or -1 when i
+      // does not start a run of two or more.
+      const uint32_t d = depth_at(i);
+      if ((i > 0 && depth_at(i - 1) == d) || i + 1 >= count || depth_at(i + 1) != d) return -1;
+      int e = i + 2;
+      while (e < count && e - i <= kMaxTieRun && depth_at(e) == d) ++e;
+      return e;
+    };
+    // Runs of two or more are listed as (start, end) pairs in the split
+    // counters' storage, which is free once lsd_run returns.
+    uint32_t* s_runs = s_u.split;
+    constexpr int kMaxRuns = kSplits / 2;
+    bool long_run = false;
+    for (int i = tid; i < count; i += kTileSortThreads) {
+      const int e = run_end(i);
+      if (e < 0) continue;
+      const uint32_t slot = e - i > kMaxTieRun ? kMaxRuns : atomicAdd(&s_run_count, 1u);
+      if (slot < kMaxRuns) {
+        s_runs[2 * slot] = i;
+        s_runs[2 * slot + 1] = e;
+      } else {
+        long_run = true;
+      }
+    }
+    if (__syncthreads_or(long_run)) {
+      lsd_run(src, count, std::true_type{});
+      return;
+    }
+    const int nruns = static_cast<int>(s_run_count);
+    for (int r = tid; r < nruns; r += kTileSortThreads) {
+      const int lo = static_cast<int>(s_runs[2 * r]);
+      const int hi = static_cast<int>(s_runs[2 * r + 1]);
+      for (int a = lo + 1; a < hi; ++a) {
+        const uint64_t v = s_items[a];
+        int b = a - 1;
+        while (b >= lo && gaussian_id(s_items[b]) > gaussian_id(v)) {
+          s_items[b + 1] = s_items[b];
+          --b;
+        }
+        s_items[b + 1] = v;
+      }
+    }
+    __syncthreads();
+  };
+
+  // Insertion sort of s_items[lo, hi) by the full entry (depth bits, record
+  // index), then again with the Gaussian id as the second key only if two
+  // entries share their depth bits.
+  auto insertion_sort = [&](int lo, int hi) {
+    bool tie = false;
+    for (int a = lo + 1; a < hi; ++a) {
+      const uint64_t v = s_items[a];
+      int b = a - 1;
+      while (b >= lo && s_items[b] > v) {
+        s_items[b + 1] = s_items[b];
+        --b;
+      }
+      s_items[b + 1] = v;
+      tie |= b >= lo && (s_items[b] >> 32) == (v >> 32);
+      tie |= b + 2 <= a && (s_items[b + 2] >> 32) == (v >> 32);
+    }
+    if (!tie) return;
+    for (int a = lo + 1; a < hi; ++a) {
+      const uint64_t v = s_items[a];
+      int b = a - 1;
+      while (b >= lo && greater(s_items[b], v)) {
+        s_items[b + 1] = s_items[b];
+        --b;
+      }
+      s_items[b + 1] = v;
     }
   };
 
@@ -451,21 +584,13 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
         const int split = tid * kSplitsPerThread + j;
         const int lo = static_cast<int>(s_off[split]);
         const int hi = split + 1 < kSplits ? static_cast<int>(s_off[split + 1]) : n;
-        for (int a = lo + 1; a < hi; ++a) {
-          const uint64_t v = s_items[a];
-          int b = a - 1;
-          while (b >= lo && s_items[b] > v) {
-            s_items[b + 1] = s_items[b];
-            --b;
-          }
-          s_items[b + 1] = v;
-        }
+        insertion_sort(lo, hi);
       }
       __syncthreads();
     } else {
       // ------------------------------------------- stable LSD in shared memory
       __syncthreads();  // the split counters share storage with the rank state
-      lsd_run(bucket, n);
+      lsd_sort(bucket, n);
     }
     for (int i = tid; i < n; i += kTileSortThreads) {
       const uint64_t v = s_items[i];
@@ -560,22 +685,14 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
           // Some split is too long for an insertion sort: order the run by
           // stable LSD passes instead (same result, the run is a whole number
           // of splits).
-          lsd_run(split_buf + base, count);
+          lsd_sort(split_buf + base, count);
         } else {
         for (int i = tid; i < count; i += kTileSortThreads) s_items[i] = split_buf[base + i];
         __syncthreads();
         for (int sp = first + tid; sp < last; sp += kTileSortThreads) {
           const int a0 = static_cast<int>(s_off[sp]) - base;
           const int a1 = (sp + 1 < kSplits ? static_cast<int>(s_off[sp + 1]) : n) - base;
-          for (int a = a0 + 1; a < a1; ++a) {
-            const uint64_t v = s_items[a];
-            int b = a - 1;
-            while (b >= a0 && s_items[b] > v) {
-              s_items[b + 1] = s_items[b];
-              --b;
-            }
-            s_items[b + 1] = v;
-          }
+          insertion_sort(a0, a1);
         }
         __syncthreads();
         }
@@ -593,30 +710,41 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
   }
 
   // A single split above kTileSortCap (many equal or nearly equal depths):
-  // stable chunked LSD over the full entry through global memory,
-  // ping-ponging between the bucket and the same range of the temp buffer.
+  // stable chunked LSD through global memory, ping-ponging between the bucket
+  // and the same range of the temp buffer: passes over the Gaussian id
+  // (placed in the high word), then over the depth bits.
   constexpr int kChunkItems = 8;
   constexpr int kChunk = kTileSortThreads * kChunkItems;
   for (int i = tid; i < kTsWarps * kRadixBins; i += kTileSortThreads) {
     (&s_u.rank.warp_hist[0][0])[i] = 0u;
   }
+  uint32_t gmin = 0xffffffffu, gmax = 0u;
   for (int i = tid; i < n; i += kTileSortThreads) {
     const uint64_t v = bucket[i];
     const uint32_t dw = static_cast<uint32_t>(v >> 32);
-    const uint32_t rw = static_cast<uint32_t>(v);
+    const uint32_t g = gaussian_id(v);
     dmin = min(dmin, dw);
     dmax = max(dmax, dw);
-    rmin = min(rmin, rw);
-    rmax = max(rmax, rw);
+    gmin = min(gmin, g);
+    gmax = max(gmax, g);
+    bucket[i] = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(v);
   }
-  block_minmax(dmin, dmax, rmin, rmax, s_minmax);
+  block_minmax(gmin, gmax, dmin, dmax, s_minmax);
+  const int passes_g = (bit_length_u32(gmax - gmin) + kRadixBits - 1) / kRadixBits;
   const int passes_d = (bit_length_u32(dmax - dmin) + kRadixBits - 1) / kRadixBits;
-  const int passes_r = (bit_length_u32(rmax - rmin) + kRadixBits - 1) / kRadixBits;
   uint64_t* src = bucket;
   uint64_t* dst = p.temp + start;
-  for (int q = 0; q < passes_r + passes_d; ++q) {
-    const PassDigit dig = q < passes_r ? PassDigit{1, rmin, q * kRadixBits}
-                                       : PassDigit{0, dmin, (q - passes_r) * kRadixBits};
+  for (int q = 0; q < passes_g + passes_d; ++q) {
+    if (q == passes_g) {
+      // Switch the high word from the Gaussian id to the depth bits.
+      __syncthreads();
+      for (int i = tid; i < n; i += kTileSortThreads) {
+        const uint32_t r = static_cast<uint32_t>(src[i]);
+        src[i] = (static_cast<uint64_t>(__float_as_uint(__ldg(&records[r].b).z)) << 32) | r;
+      }
+    }
+    const PassDigit dig = q < passes_g ? PassDigit{0, gmin, q * kRadixBits}
+                                       : PassDigit{0, dmin, (q - passes_g) * kRadixBits};
     s_base[tid] = 0u;
     __syncthreads();
     for (int i = tid; i < n; i += kTileSortThreads) atomicAdd(&s_base[dig(src[i])], 1u);
@@ -662,6 +790,15 @@ __global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketPa
     src = dst;
     dst = t;
   }
+  if (passes_d == 0) {
+    // No depth pass ran: the high word still holds the Gaussian id.
+    __syncthreads();
+    for (int i = tid; i < n; i += kTileSortThreads) {
+      const uint32_t r = static_cast<uint32_t>(src[i]);
+      src[i] = (static_cast<uint64_t>(__float_as_uint(__ldg(&records[r].b).z)) << 32) | r;
+    }
+  }
+  __syncthreads();
   for (int i = tid; i < n; i += kTileSortThreads) {
     const uint64_t v = src[i];
     p.keys_out[start + i] = key_tile | (v >> 32);

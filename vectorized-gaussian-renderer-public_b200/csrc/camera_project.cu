@@ -5,12 +5,12 @@
 // cull, radius, conic) and :1691-1829 (tile cover and key), restructured for
 // B200: one persistent launch walks virtual blocks of kProjectChunk
 // (camera, Gaussian) tasks handed out by an atomic ticket, compacts visible
-// records and their tile intersections in task order through a decoupled
-// look-back prefix (so the visible list and the key list are deterministic,
-// ascending Gaussian id within each camera), and emits the keys cooperatively
+// records and their tile intersections in task order within the block,
+// reserves the block's output ranges with one atomic per kind (blocks never
+// wait on each other, whatever their cost), and emits the keys cooperatively
 // from shared memory so every store is coalesced, counting each tile's keys
-// for the bucket sort.  There is no host round trip: the emitted count stays
-// on the device for the sort.
+// for the bucket sort.  There is no host round trip: the totals stay on the
+// device for the sort.
 #include "vgr_camera.cuh"
 #include "vgr_kernels.h"
 
@@ -406,54 +406,6 @@ __device__ __forceinline__ uint32_t footprint_box(float opacity, float a, float 
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-__device__ __forceinline__ uint64_t sat_pack(uint64_t vis, uint64_t isect) {
-  if (vis > kDescCountMask) vis = kDescCountMask;
-  if (isect > kDescCountMask) isect = kDescCountMask;
-  return (vis << 31) | isect;
-}
-
-// Warp-cooperative decoupled look-back over virtual blocks [0, b): returns
-// the (visible, intersection) exclusive prefix.  Lane l inspects b-1-l-32k.
-__device__ __forceinline__ void project_lookback(uint64_t* desc, int64_t b, uint64_t* out_vis,
-                                                 uint64_t* out_isect, int32_t* status) {
-  const int lane = threadIdx.x & 31;
-  uint64_t vis = 0, isect = 0;
-  int64_t window_end = b;  // inspect [window_end-32, window_end)
-  uint32_t spins = 0;
-  while (window_end > 0) {
-    const int64_t j = window_end - 1 - lane;
-    uint64_t d = kDescInclusive;  // out-of-range lanes act as a zero inclusive
-    if (j >= 0) d = ld_acquire_u64(desc + j);
-    const uint32_t not_ready = __ballot_sync(0xffffffffu, (d >> 62) == 0);
-    if (not_ready) {
-      if (++spins > kSpinLimit) {
-        if (lane == 0) atomicOr(status, kDeviceErrorLookback);
-        break;
-      }
-      continue;
-    }
-    const uint32_t inclusive = __ballot_sync(0xffffffffu, (d >> 62) == 2);
-    // Lanes up to and including the first inclusive descriptor contribute.
-    const int stop = inclusive ? (__ffs(inclusive) - 1) : 31;
-    uint64_t dv = 0, di = 0;
-    if (lane <= stop && j >= 0) {
-      dv = (d >> 31) & kDescCountMask;
-      di = d & kDescCountMask;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      dv += __shfl_xor_sync(0xffffffffu, dv, o);
-      di += __shfl_xor_sync(0xffffffffu, di, o);
-    }
-    vis += dv;
-    isect += di;
-    if (inclusive) break;
-    window_end -= 32;
-  }
-  *out_vis = vis;
-  *out_isect = isect;
-}
-
 template <int kShDegree>
 __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
@@ -474,7 +426,6 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
   const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
   const CamConst* cam_consts = reinterpret_cast<const CamConst*>(p.scratch + p.layout.cam_consts);
-  uint64_t* desc = reinterpret_cast<uint64_t*>(p.scratch + p.layout.project_desc);
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -506,11 +457,9 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
     const CamPlan plan = s_plan;
     const int64_t local_begin = chunk * kProjectChunk;
     const bool live = plan.camera >= 0 && plan.scene_slot >= 0 && local_begin < plan.g_count;
-    if (!live && b != total_vblocks - 1) {
+    if (!live) {
       // A virtual block past its camera's scene (ragged scene sizes) or of an
-      // invalid camera adds nothing: publish its zero aggregate and move on
-      // (the last block still runs the look-back, as it owns the totals).
-      if (tid == 0) st_release_u64(desc + b, (b == 0 ? kDescInclusive : kDescAggregate));
+      // invalid camera adds nothing.
       __syncthreads();
       continue;
     }
@@ -631,36 +580,14 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       s_nisect = s_prefix[block_vis];
     }
 
-    // Decoupled look-back for the global (visible, intersection) offsets.
-    if (warp == 0) {
-      const uint64_t agg = sat_pack(block_vis, block_isect);
-      if (b == 0) {
-        if (lane == 0) st_release_u64(desc + b, kDescInclusive | agg);
-        if (lane == 0) {
-          s_base_vis = 0;
-          s_base_isect = 0;
-        }
-      } else {
-        if (lane == 0) st_release_u64(desc + b, kDescAggregate | agg);
-        uint64_t pv = 0, pi = 0;
-        project_lookback(desc, b, &pv, &pi, &header->status);
-        if (lane == 0) {
-          st_release_u64(desc + b, kDescInclusive | sat_pack(pv + block_vis, pi + block_isect));
-          s_base_vis = pv;
-          s_base_isect = pi;
-        }
-      }
-      if (lane == 0 && b == total_vblocks - 1) {
-        // The last virtual block owns the frame totals.
-        const uint64_t tv = s_base_vis + block_vis;
-        const uint64_t ti = s_base_isect + block_isect;
-        p.counters[0] = static_cast<int64_t>(tv);
-        p.counters[1] = static_cast<int64_t>(ti);
-        const uint64_t vcap = static_cast<uint64_t>(p.visible_capacity);
-        const uint64_t icap = static_cast<uint64_t>(p.intersection_capacity);
-        p.counters[2] = tv > vcap ? static_cast<int64_t>(tv - vcap) : 0;
-        p.counters[3] = ti > icap ? static_cast<int64_t>(ti - icap) : 0;
-      }
+    // The block's output ranges: one reservation of (visible, intersection)
+    // slots per block, no waiting on other blocks.  The order of the blocks'
+    // ranges is therefore not fixed, but within a block records and keys stay
+    // in task order, and the tile sort orders every tile by (depth bits,
+    // Gaussian id), which does not depend on where the records landed.
+    if (tid == 0) {
+      s_base_vis = atomicAdd(&header->visible_total, static_cast<unsigned long long>(block_vis));
+      s_base_isect = atomicAdd(&header->isect_total, static_cast<unsigned long long>(block_isect));
     }
     __syncthreads();
 

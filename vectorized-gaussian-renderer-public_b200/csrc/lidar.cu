@@ -107,7 +107,7 @@ AccelLayout make_accel_layout(int64_t count, int packet) {
   l.keys_b = take(count * 8);
   l.vals_a = take(count * 4);
   l.vals_b = take(count * 4);
-  l.sort_layout = make_scratch_layout(count > 0 ? count : 1, 0, 0, true);
+  l.sort_layout = make_scratch_layout(count > 0 ? count : 1, 0, true);
   l.sort = take(l.sort_layout.total);
   l.total = off;
   return l;

@@ -97,7 +97,8 @@ extern "C" int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
   }
   const int64_t vblocks = (max_projection_tasks + kProjectChunk - 1) / kProjectChunk +
                           max_active_cameras;
-  return make_scratch_layout(intersection_capacity, max_active_cameras, vblocks, false).total;
+  (void)vblocks;
+  return make_scratch_layout(intersection_capacity, max_active_cameras, false).total;
 }
 
 // Scratch for a drop-in caller that only knows (items, segments): active
@@ -333,7 +334,7 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     return fail(VGR_ERR_INVALID_ARGUMENT,
                 "active cameras x max_scene_gaussians exceeds 2^41 projection tasks");
   }
-  const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, vblocks, false);
+  const ScratchLayout layout = make_scratch_layout(ws->intersection_capacity, active, false);
   if (ws->scratch_bytes < layout.total) {
     return fail(VGR_ERR_SCRATCH_TOO_SMALL,
                 "render scratch holds %lld bytes but this batch needs %lld",
@@ -359,10 +360,6 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
   int64_t selector = 1;
 
   if (!opt->reuse_projection) {
-    if (cudaMemsetAsync(scratch + layout.project_desc, 0, static_cast<size_t>(vblocks) * 8, stream) !=
-        cudaSuccess) {
-      return check_launch("render: clear projection descriptors", 0);
-    }
     if (global_tiles > 0 &&
         cudaMemsetAsync(ws->tile_ends, 0, static_cast<size_t>(global_tiles) * 4, stream) != cudaSuccess) {
       return check_launch("render: clear tile counts", 0);
@@ -459,6 +456,8 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     bp.temp = ws->keys_in;
     bp.tile_starts = ws->tile_starts;
     bp.tile_ends = ws->tile_ends;
+    bp.records = static_cast<const Record*>(ws->records);
+    bp.visible_capacity = ws->visible_capacity;
     tile_scan_kernel<<<1, kTileScanThreads, 0, stream>>>(bp);
     if ((rc = check_launch("render: tile scan")) != VGR_OK) return rc;
     mark(3);

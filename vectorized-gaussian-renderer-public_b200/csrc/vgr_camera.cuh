@@ -36,11 +36,14 @@ struct ScratchHeader {
   int32_t pad0;
   uint32_t project_queue;      // virtual-block ticket of the projection kernel
   uint32_t composite_queue;    // work-item ticket of the persistent compositor
-  uint32_t sort_queue[8];      // partition ticket per radix pass
+  uint32_t sort_queue[8];      // partition ticket per radix pass (LBVH sort)
   uint32_t ranges_done;
   uint32_t bucket_total;       // keys placed in tile buckets (tile_scan_kernel)
   uint32_t tail_cursor;        // overflow-sentinel keys placed after the buckets
-  uint32_t pad1[17];
+  uint32_t pad1;
+  unsigned long long visible_total;  // records reserved by the projection blocks
+  unsigned long long isect_total;    // keys reserved by the projection blocks
+  uint32_t pad2[12];
 };
 static_assert(sizeof(ScratchHeader) == 128, "ScratchHeader layout");
 
@@ -66,10 +69,6 @@ constexpr int kTileSortCap = kTileSortThreads * kTileSortItems;
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanItems = 16;
 
-// Projection look-back descriptor: flag (2 bits) | visible (31) | isects (31).
-constexpr uint64_t kDescAggregate = 1ull << 62;
-constexpr uint64_t kDescInclusive = 2ull << 62;
-constexpr uint64_t kDescCountMask = (1ull << 31) - 1;
 
 __host__ __device__ inline int64_t align_up(int64_t v, int64_t a) {
   return (v + a - 1) / a * a;
@@ -81,11 +80,9 @@ struct ScratchLayout {
   int64_t plans;          // CamPlan[A]
   int64_t cam_consts;     // CamConst[A] (112 bytes each)
   int64_t tile_prefix;    // int64[A+1] exclusive prefix of tiles over active slots
-  int64_t project_desc;   // uint64[vblocks]
   int64_t sort_hist;      // uint32[passes][256]
   int64_t sort_desc;      // uint64[passes][partitions][256]
   int64_t total;
-  int64_t max_vblocks;
   int64_t max_partitions;
 };
 
@@ -93,8 +90,7 @@ struct ScratchLayout {
 // the global onesweep sort (the LBVH Morton sort); the camera path sorts in
 // tile buckets and needs none.
 __host__ __device__ inline ScratchLayout make_scratch_layout(
-    int64_t intersection_capacity, int64_t max_active_cameras,
-    int64_t max_vblocks, bool onesweep_descriptors) {
+    int64_t intersection_capacity, int64_t max_active_cameras, bool onesweep_descriptors) {
   ScratchLayout l{};
   int64_t off = 0;
   l.header = off;
@@ -105,9 +101,6 @@ __host__ __device__ inline ScratchLayout make_scratch_layout(
   off = align_up(off + max_active_cameras * 112, 256);
   l.tile_prefix = off;
   off = align_up(off + (max_active_cameras + 1) * 8, 256);
-  l.project_desc = off;
-  l.max_vblocks = max_vblocks;
-  off = align_up(off + max_vblocks * 8, 256);
   l.sort_hist = off;
   off = align_up(off + kMaxSortPasses * kRadixBins * 4, 256);
   l.sort_desc = off;

@@ -98,6 +98,8 @@ struct BucketParams {
   uint64_t* temp;              // ping-pong space for tiles above kTileSortCap
   int32_t* tile_starts;
   int32_t* tile_ends;
+  const Record* records;       // projected records (Gaussian ids break depth ties)
+  int64_t visible_capacity;
 };
 
 struct CompositeParams {

@@ -8,17 +8,17 @@
 // being captured into a CUDA graph, where a fresh cudaMalloc is not an
 // operation the capture can record.  Such a caller can still hand over the
 // buffers it already owns (inputs, outputs and the record/key/value/range
-// workspace), but has nowhere to get the projection look-back descriptors,
-// queue tickets and per-camera plans from.  Those fit in a fixed array that
+// workspace), but has nowhere to get the queue tickets, per-camera plans and
+// projection constants from.  Those fit in a fixed array that
 // the library carries itself.
 //
 // Limits and rules:
 //  * The array is VGR_STATIC_SCRATCH_BYTES (16 MiB).  Every GPU on which the
 //    library is loaded holds it until the process exits.  The scratch grows
-//    with the projection tasks (8 bytes per 512 (camera, Gaussian) pairs) and
-//    the active cameras, not with the intersections; a render past about 2^31
-//    tasks is rejected with VGR_ERR_SCRATCH_TOO_SMALL before anything is
-//    launched.
+//    with the active cameras (160 bytes each: plan, projection constants and
+//    tile prefix) plus about 9 KB, not with the scene or the intersections; a
+//    render of more than about 104,000 active cameras is rejected with
+//    VGR_ERR_SCRATCH_TOO_SMALL before anything is launched.
 //  * Every call on a device shares the one array, and it keeps the previous
 //    call's contents.  vgr_render clears everything that must start at zero
 //    (counters, queue tickets, tile counts, look-back descriptors) on the
