@@ -21,7 +21,7 @@
 //    VGR_ERR_SCRATCH_TOO_SMALL before anything is launched.
 //  * Every call on a device shares the one array, and it keeps the previous
 //    call's contents.  vgr_render clears everything that must start at zero
-//    (counters, queue tickets, tile counts, look-back descriptors) on the
+//    (counters, queue tickets, reserved totals, tile counts) on the
 //    stream, so back-to-back calls on one stream are correct; calls whose
 //    work overlaps on the GPU (different streams, or different host threads
 //    without ordering) race on the array and produce wrong results.

@@ -717,7 +717,7 @@ class CustomCudaBackend:
         return dict(zip(COUNTER_NAMES, (int(v) for v in values)))
 
     def read_device_status(self, *, synchronize: bool = True) -> int:
-        """Device error bits of the last frame (1 = a look-back wait gave up)."""
+        """Device error bits of the last frame (nonzero: a bounded device wait gave up)."""
         if synchronize:
             self.synchronize()
         return int(self.workspace["scratch"][:4].view(torch.int32).cpu().item())

@@ -14,7 +14,7 @@ of libvgr_b200.so on the current PyTorch CUDA stream.
 ``render`` keeps the reference's 24-tensor workspace: keys/values double
 buffers, tile ranges and counters are used in place; the visible-record
 structure-of-arrays tensors are filled as mirrors; the 48-byte projected
-records and the look-back/sort scratch live in ``sort_temp``, whose size this
+records and the frame scratch live in ``sort_temp``, whose size this
 module reports through the two temp-bytes queries.
 """
 
