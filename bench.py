@@ -75,6 +75,8 @@ def parse_args() -> argparse.Namespace:
                         help="override the LiDAR sensor count (small profiling captures)")
     parser.add_argument("--ragged-frames", type=int, default=20,
                         help="frames of the ragged-batch workload (0: skip)")
+    parser.add_argument("--diff-steps", type=int, default=10,
+                        help="timed steps of the differentiable-form workload (0: skip)")
     parser.add_argument("--ragged-scale", type=float, default=1.0,
                         help="scale scene sizes and camera counts of the ragged workload")
     return parser.parse_args()
@@ -577,6 +579,96 @@ def run_ragged(args, device, world: int) -> dict:
     return result
 
 
+# --------------------------------------------------------------------------- differentiable form
+DIFF_METRIC = "fwd+bwd ms/iter, loss L2(RGB) + 0.1 L1(depth) vs a perturbed-scene target"
+
+
+def run_differentiable(args, device, world: int) -> dict:
+    """Differentiable form: 500k Gaussians (SH3) as raw parameters, 16 cameras
+    of 512x512, loss L2(RGB) + 0.1 L1(depth) against images of a perturbed
+    copy of the scene.  One step = training forward (activation, projection,
+    tile sort, compositor with training outputs, capacity check) + loss +
+    backward (compositor backward, per-Gaussian projection backward)."""
+    from vgr_b200 import workloads
+    from vgr_b200.differentiable import DifferentiableRenderer
+
+    rank = int(os.environ.get("RANK", "0"))
+    work = workloads.training_workload(seed=13 + rank)
+    rig = work.rig
+    names = ("means", "log_scales", "rotations", "opacity_logits", "features")
+    params = {k: v.to(device).requires_grad_(True) for k, v in work.params.items()}
+    view = rig.viewmats.to(device)
+    intr = rig.intrinsics.to(device)
+    renderer = DifferentiableRenderer(height=rig.height, width=rig.width, sh_degree=3, device=device)
+    target = [t.clone() for t in renderer.forward_native(*(work.targets[k].to(device) for k in names), view, intr)]
+    t_rgb, t_depth = target[0], target[1]
+
+    def step() -> None:
+        rgb, depth, _ = renderer.render(*(params[k] for k in names), view, intr)
+        finite = torch.isfinite(depth) & torch.isfinite(t_depth)
+        diff = torch.where(finite, depth - t_depth, torch.zeros_like(depth))
+        loss = ((rgb - t_rgb) ** 2).mean() + 0.1 * diff.abs().mean()
+        loss.backward()
+        for p in params.values():
+            p.grad = None
+
+    stream = torch.cuda.current_stream(device)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(device)
+    steps = max(args.diff_steps, 1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    start.record(stream)
+    for _ in range(steps):
+        step()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    step_ms = max_over_ranks(start.elapsed_time(stop), world, device) / steps
+    # Forward alone (the same training forward, no autograd).
+    with torch.no_grad():
+        detached = [params[k].detach() for k in names]
+        for _ in range(3):
+            renderer.forward_native(*detached, view, intr)
+        torch.cuda.synchronize(device)
+        start.record(stream)
+        for _ in range(steps):
+            renderer.forward_native(*detached, view, intr)
+        stop.record(stream)
+        torch.cuda.synchronize(device)
+    fwd_ms = max_over_ranks(start.elapsed_time(stop), world, device) / steps
+    # Backward kernels alone, from one forward (record clear + compositor
+    # backward + projection backward), for the stage split.
+    rgb, depth, alpha = renderer.forward_native(*detached, view, intr)
+    g_rgb = torch.randn_like(rgb)
+    g_depth = torch.randn_like(depth) * 0.1
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    for _ in range(steps):
+        renderer.backward_native(renderer.frame, g_rgb, g_depth, None)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    bwd_ms = start.elapsed_time(stop) / steps
+    pixels = rig.viewmats.shape[0] * rig.height * rig.width
+    return {
+        "metric": DIFF_METRIC,
+        "value": round(step_ms, 3),
+        "unit": "ms/iter",
+        "higher_is_better": False,
+        "steps": steps,
+        "forward_ms": round(fwd_ms, 3),
+        "backward_kernels_ms": round(bwd_ms, 3),
+        "fwd_bwd_over_fwd": round(step_ms / fwd_ms, 3),
+        "target_fwd_bwd_over_fwd": 2.5,
+        "gradients": "hand-written CUDA backward; float64 autograd + central-difference checks in tests",
+        "config": {"workload": "train-500k-sh3-16x512", "gaussians": work.params["means"].shape[0],
+                   "cameras": rig.viewmats.shape[0], "height": rig.height, "width": rig.width,
+                   "pixels": pixels, "sh_degree": 3, "tile_size": renderer.tile_size,
+                   "visible_records": renderer.last_counters.get("visible_gaussians"),
+                   "tile_intersections": renderer.last_counters.get("tile_intersections")},
+    }
+
+
 def run_b200(args) -> None:
     world, rank, local = dist_setup()
     if not torch.cuda.is_available():
@@ -724,6 +816,10 @@ def run_b200(args) -> None:
     if args.ragged_frames > 0:
         ragged = run_ragged(args, device, world)
 
+    differentiable = None
+    if args.diff_steps > 0:
+        differentiable = run_differentiable(args, device, world)
+
     lidar = None
     if args.lidar_steps > 0:
         lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
@@ -753,6 +849,7 @@ def run_b200(args) -> None:
             "clocks": clocks,
             "capacity_check": {k: check[k] for k in ("visible_overflow", "intersection_overflow")},
             "ragged": ragged,
+            "differentiable": differentiable,
             "lidar": lidar,
         }
         print(json.dumps(line), flush=True)

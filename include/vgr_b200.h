@@ -237,6 +237,63 @@ int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras
                               const vgr_render_options* options, void* stream,
                               int64_t* sorted_buffer_selector);
 
+/* ----------------------------------------------------- differentiable form */
+/* Training form of the camera path: the forward above plus hand-written
+ * backward kernels for the compositor and the projection.  No counterpart in
+ * the reference, which renders forward only and measures gradients through
+ * gsplat's rasterization (benchmarks/compare_custom_gsplat.py:1163-1203).
+ * Parameters are the raw optimisation variables; the forward applies
+ * scale = exp(log_scale), q / |q| and opacity = sigmoid(logit). */
+typedef struct vgr_train_params {
+  const float* log_scales;     /* [G,3] */
+  const float* rotations;      /* [G,4] WXYZ, any norm */
+  const float* opacity_logits; /* [G] */
+} vgr_train_params;
+/* Per-frame state the forward leaves for the backward.  P = output pixels,
+ * A = active cameras. */
+typedef struct vgr_train_state {
+  float* final_transmittance;  /* [P] */
+  int32_t* last_position;      /* [P] sorted position one past the last blended record */
+  int32_t* record_map;         /* [A, max_scene_gaussians] record of (camera, Gaussian) or -1 */
+  int64_t record_map_capacity; /* elements */
+  void* record_grads;          /* visible_capacity * VGR_RECORD_BYTES, 16-byte aligned */
+} vgr_train_state;
+/* Gradients of the loss with respect to the forward outputs (pixel-major,
+ * same layout as vgr_outputs). */
+typedef struct vgr_output_grads {
+  const float* rgb;   /* [P,3] */
+  const float* depth; /* [P] or NULL */
+  const float* alpha; /* [P] or NULL */
+} vgr_output_grads;
+/* Gradients with respect to the parameters; every element is written. */
+typedef struct vgr_param_grads {
+  float* means;          /* [G,3] */
+  float* log_scales;     /* [G,3] */
+  float* rotations;      /* [G,4] */
+  float* opacity_logits; /* [G] */
+  float* features;       /* [G,F] */
+} vgr_param_grads;
+/* Activation: covariances [G,6] (as vgr_precompute_covariances with
+ * exp(log_scales)) and opacities [G] = sigmoid(opacity_logits), for the
+ * scene passed to vgr_render_train. */
+int vgr_train_activate(const vgr_train_params* params, int64_t gaussian_count,
+                       float* covariances, float* opacities, void* stream);
+/* vgr_render that also fills the training state.  Requires
+ * full_sensor_output = 1, output_srgb = 0, antialiased = 0 and
+ * reuse_projection = 0. */
+int vgr_render_train(const vgr_scene* scene, const vgr_cameras* cameras,
+                     const vgr_outputs* outputs, const vgr_workspace* workspace,
+                     const vgr_render_options* options, const vgr_train_state* state,
+                     void* stream, int64_t* sorted_buffer_selector);
+/* Backward of the last vgr_render_train with the same arguments (workspace,
+ * scratch and state untouched since): compositor backward into per-record
+ * gradients, then one pass per Gaussian over the cameras that saw it through
+ * the projection, the colour model and the activations. */
+int vgr_render_backward(const vgr_scene* scene, const vgr_train_params* params,
+                        const vgr_cameras* cameras, const vgr_outputs* outputs,
+                        const vgr_workspace* workspace, const vgr_render_options* options,
+                        const vgr_train_state* state, const vgr_output_grads* grads,
+                        const vgr_param_grads* param_grads, void* stream);
 /* ------------------------------------------------------------------ LiDAR */
 
 /* Caller-owned Gaussian LiDAR scene (lidar_scene.py:13-96): WXYZ rotations,

@@ -22,20 +22,6 @@
 
 namespace vgr {
 
-template <int kTile>
-struct CompositeGeometry {
-  static constexpr int kBlockW = kTile < 8 ? kTile : 8;  // warp block width (px)
-  static constexpr int kLaneRows =
-      (32 / kBlockW) < (kTile / 2) ? (32 / kBlockW) : (kTile / 2);  // lane rows
-  static constexpr int kBlockH = 2 * kLaneRows;  // warp block height (px)
-  static constexpr int kWarpsX = kTile / kBlockW;
-  static constexpr int kWarpsY = kTile / kBlockH;
-  static constexpr int kWarps = kWarpsX * kWarpsY;
-  static constexpr int kThreads = kWarps * 32;
-};
-
-constexpr int kCompositeBatch = 256;
-
 // Per-pixel accumulation.  A pixel that terminates gets a NaN row coordinate,
 // so every later power evaluates to NaN and fails the range test: the hot
 // path never tests `done`, which only drives the warp and CTA exits.
@@ -44,6 +30,7 @@ struct PixelState {
   float r, g, b, depth;
   float best_weight;
   int32_t best_pos;  // sorted position of the largest single weight
+  int32_t last;      // training: sorted position one past the last blended record
   bool done;
 };
 
@@ -52,7 +39,7 @@ struct PixelState {
 // max(-qmax/2, -20) merges the conservative q bound with the reference's
 // power >= -20 cut, so the test below is the reference's
 // `power <= 0 && power >= -20` restricted to records that can reach 1/255.
-template <bool kFull>
+template <bool kFull, bool kTrain>
 __device__ __forceinline__ void blend(PixelState& s, float& cy, float power, float lo, float o,
                                       int32_t pos, const float4& col) {
   if (!(power >= lo && power <= 0.0f)) return;
@@ -75,10 +62,11 @@ __device__ __forceinline__ void blend(PixelState& s, float& cy, float power, flo
       s.best_pos = pos;
     }
   }
+  if (kTrain) s.last = pos + 1;
   s.transmittance = next_t;
 }
 
-template <bool kFull>
+template <bool kFull, bool kTrain>
 __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamPlan& plan, int x,
                                             int y, PixelState& s) {
   const int64_t pixel = plan.pixel_base + static_cast<int64_t>(y) * plan.width + x;
@@ -101,9 +89,13 @@ __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamP
     }
     p.semantic[pixel] = semantic;
   }
+  if (kTrain) {
+    p.final_transmittance[pixel] = s.transmittance;
+    p.last_position[pixel] = s.last;
+  }
 }
 
-template <int kTile, bool kFull>
+template <int kTile, bool kFull, bool kTrain>
 __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
                                   2048 / CompositeGeometry<kTile>::kThreads / 2)
     composite_kernel(CompositeParams p) {
@@ -113,31 +105,12 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
   __shared__ uint32_t s_mask[kCompositeBatch];
 
-  const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
-  const int64_t* tile_prefix = reinterpret_cast<const int64_t*>(p.scratch + p.layout.tile_prefix);
-
-  // Work item -> active slot.  Slots are dense in [0, A) and every slot's
-  // tiles are contiguous; tile_prefix is monotone, so search it.
-  const int64_t item = blockIdx.x;
-  const int64_t total = tile_prefix[p.active_count];
-  if (item >= total) return;
-  int64_t lo = 0, hi = p.active_count;  // tile_prefix[lo] <= item < tile_prefix[hi]
-  {
-    const int64_t tpi = p.tiles_per_camera_hint;
-    if (tpi > 0) {
-      const int64_t guess = item / tpi;
-      if (guess < p.active_count && tile_prefix[guess] <= item && item < tile_prefix[guess + 1]) {
-        lo = guess;
-        hi = guess + 1;
-      }
-    }
-    while (hi - lo > 1) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (tile_prefix[mid] <= item) lo = mid; else hi = mid;
-    }
+  CamPlan plan;
+  int64_t local_tile;
+  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, blockIdx.x, plan,
+                   local_tile)) {
+    return;
   }
-  const CamPlan plan = plans[lo];
-  const int64_t local_tile = item - tile_prefix[lo];
   const int tile_y = static_cast<int>(local_tile / plan.tiles_x);
   const int tile_x = static_cast<int>(local_tile - static_cast<int64_t>(tile_y) * plan.tiles_x);
   const int64_t global_tile = plan.tile_base + local_tile;
@@ -160,8 +133,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   float cy0 = valid0 ? fadd(static_cast<float>(pixel_y0), 0.5f) : kNaN;
   float cy1 = valid1 ? fadd(static_cast<float>(pixel_y1), 0.5f) : kNaN;
 
-  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, !valid0};
-  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, !valid1};
+  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid0};
+  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid1};
   bool warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
 
   const int64_t range_start = p.tile_starts[global_tile];
@@ -173,28 +146,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
     for (int64_t chunk = range_start; chunk < range_end; chunk += kCompositeBatch) {
       const int n = static_cast<int>(min(static_cast<int64_t>(kCompositeBatch), range_end - chunk));
       for (int j = tid; j < n; j += Geo::kThreads) {
-        const int32_t v = p.values[chunk + j];
-        const Record rec = p.records[v];
-        s_geo[j] = make_float4(rec.a.x, rec.a.y, fmul(-0.5f, rec.a.z), -rec.a.w);
-        const float o = rec.b.y;
-        const float qmax = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
-        s_cpo[j] = make_float4(fmul(-0.5f, rec.b.x), fmaxf(fmul(-0.5f, qmax), -20.0f), o, 0.0f);
-        s_col[j] = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
-        const __half2 box = *reinterpret_cast<const __half2*>(&rec.c.w);
-        const float hx = __low2float(box);
-        const float hy = __high2float(box);
-        uint32_t mask = 0;
-#pragma unroll
-        for (int w = 0; w < Geo::kWarps; ++w) {
-          const float bx0 = tile_x0 + static_cast<float>((w % Geo::kWarpsX) * Geo::kBlockW) + 0.5f;
-          const float by0 = tile_y0 + static_cast<float>((w / Geo::kWarpsX) * Geo::kBlockH) + 0.5f;
-          const float bx1 = bx0 + static_cast<float>(Geo::kBlockW - 1);
-          const float by1 = by0 + static_cast<float>(Geo::kBlockH - 1);
-          const bool hit = rec.a.x + hx >= bx0 && rec.a.x - hx <= bx1 && rec.a.y + hy >= by0 &&
-                           rec.a.y - hy <= by1;
-          mask |= hit ? (1u << w) : 0u;
-        }
-        s_mask[j] = mask;
+        stage_composite_record<kTile>(p.records[p.values[chunk + j]], tile_x0, tile_y0, s_geo[j],
+                                      s_cpo[j], s_col[j], s_mask[j]);
       }
       __syncthreads();
       if (!warp_done) {
@@ -218,8 +171,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
             const bool in1 = p1 >= cpo.y && p1 <= 0.0f;
             if (in0 || in1) {
               const float4 col = s_col[j];
-              blend<kFull>(s0, cy0, p0, cpo.y, cpo.z, chunk_pos + j, col);
-              blend<kFull>(s1, cy1, p1, cpo.y, cpo.z, chunk_pos + j, col);
+              blend<kFull, kTrain>(s0, cy0, p0, cpo.y, cpo.z, chunk_pos + j, col);
+              blend<kFull, kTrain>(s1, cy1, p1, cpo.y, cpo.z, chunk_pos + j, col);
             }
           }
           warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
@@ -229,15 +182,18 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
     }
   }
 
-  if (valid0) write_pixel<kFull>(p, plan, pixel_x, pixel_y0, s0);
-  if (valid1) write_pixel<kFull>(p, plan, pixel_x, pixel_y1, s1);
+  if (valid0) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y0, s0);
+  if (valid1) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y1, s1);
 }
 
-template __global__ void composite_kernel<4, false>(CompositeParams);
-template __global__ void composite_kernel<4, true>(CompositeParams);
-template __global__ void composite_kernel<8, false>(CompositeParams);
-template __global__ void composite_kernel<8, true>(CompositeParams);
-template __global__ void composite_kernel<16, false>(CompositeParams);
-template __global__ void composite_kernel<16, true>(CompositeParams);
+template __global__ void composite_kernel<4, false, false>(CompositeParams);
+template __global__ void composite_kernel<4, true, false>(CompositeParams);
+template __global__ void composite_kernel<8, false, false>(CompositeParams);
+template __global__ void composite_kernel<8, true, false>(CompositeParams);
+template __global__ void composite_kernel<16, false, false>(CompositeParams);
+template __global__ void composite_kernel<16, true, false>(CompositeParams);
+template __global__ void composite_kernel<4, true, true>(CompositeParams);
+template __global__ void composite_kernel<8, true, true>(CompositeParams);
+template __global__ void composite_kernel<16, true, true>(CompositeParams);
 
 }  // namespace vgr

@@ -12,39 +12,12 @@ __global__ void __launch_bounds__(256) precompute_covariances_kernel(
     float* __restrict__ covariances) {
   const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (g >= count) return;
-  float w = rotations[g * 4 + 0];
-  float x = rotations[g * 4 + 1];
-  float y = rotations[g * 4 + 2];
-  float z = rotations[g * 4 + 3];
-  const float norm2 = ffma(z, z, ffma(y, y, ffma(x, x, fmul(w, w))));
-  const float inv = fdiv(1.0f, fsqrt(fmaxf(norm2, 1.0e-20f)));
-  w = fmul(w, inv);
-  x = fmul(x, inv);
-  y = fmul(y, inv);
-  z = fmul(z, inv);
-  const float xx = fmul(x, x), yy = fmul(y, y), zz = fmul(z, z);
-  const float xy = fmul(x, y), xz = fmul(x, z), yz = fmul(y, z);
-  const float wx = fmul(w, x), wy = fmul(w, y), wz = fmul(w, z);
-  float r[9];
-  r[0] = fsub(1.0f, fmul(2.0f, fadd(yy, zz)));
-  r[1] = fmul(2.0f, fsub(xy, wz));
-  r[2] = fmul(2.0f, fadd(xz, wy));
-  r[3] = fmul(2.0f, fadd(xy, wz));
-  r[4] = fsub(1.0f, fmul(2.0f, fadd(xx, zz)));
-  r[5] = fmul(2.0f, fsub(yz, wx));
-  r[6] = fmul(2.0f, fsub(xz, wy));
-  r[7] = fmul(2.0f, fadd(yz, wx));
-  r[8] = fsub(1.0f, fmul(2.0f, fadd(xx, yy)));
-  const float sx = scales[g * 3 + 0], sy = scales[g * 3 + 1], sz = scales[g * 3 + 2];
-  const float s2[3] = {fmul(sx, sx), fmul(sy, sy), fmul(sz, sz)};
-  const int rows[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  float cov[6];
+  covariance_from_quaternion(rotations[g * 4 + 0], rotations[g * 4 + 1], rotations[g * 4 + 2],
+                             rotations[g * 4 + 3], scales[g * 3 + 0], scales[g * 3 + 1],
+                             scales[g * 3 + 2], cov);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const float* a = r + rows[k][0] * 3;
-    const float* b = r + rows[k][1] * 3;
-    covariances[g * 6 + k] =
-        ffma(fmul(a[2], b[2]), s2[2], ffma(fmul(a[1], b[1]), s2[1], fmul(fmul(a[0], b[0]), s2[0])));
-  }
+  for (int k = 0; k < 6; ++k) covariances[g * 6 + k] = cov[k];
 }
 
 // Logical -> physical chunk bookkeeping (renderer_cuda.cu:2307-2360).

@@ -17,68 +17,6 @@
 namespace vgr {
 
 // ---------------------------------------------------------------------------
-// Per-camera constants of the projection, computed once per active slot by
-// the setup kernel.  R = view_rotation * env_rotation and
-// t = view_rotation * env_t + view_t, so camera-space p = R m + t.
-// ---------------------------------------------------------------------------
-struct __align__(16) CamConst {
-  float r[9];
-  float t[3];
-  float fx, fy, cx, cy;
-  float lim_xp, lim_xn, lim_yp, lim_yn;
-  float width, height;
-  float r_scale2;   // upper bound of the largest eigenvalue of R^T R (1 for a rotation)
-  float pad[3];
-};
-static_assert(sizeof(CamConst) == 112, "CamConst is fourteen 8-byte words");
-
-__device__ __forceinline__ void make_cam_const(const float* view, const float* env,
-                                               const float* intr, int width, int height,
-                                               CamConst* c) {
-#pragma unroll
-  for (int row = 0; row < 3; ++row) {
-#pragma unroll
-    for (int col = 0; col < 3; ++col) {
-      c->r[row * 3 + col] =
-          ffma(view[row * 4 + 2], env[8 + col],
-               ffma(view[row * 4 + 1], env[4 + col], fmul(view[row * 4 + 0], env[col])));
-    }
-    c->t[row] = ffma(view[row * 4 + 2], env[11],
-                     ffma(view[row * 4 + 1], env[7],
-                          ffma(view[row * 4 + 0], env[3], view[row * 4 + 3])));
-  }
-  c->fx = intr[0];
-  c->fy = intr[4];
-  c->cx = intr[2];
-  c->cy = intr[5];
-  const float w = static_cast<float>(width);
-  const float h = static_cast<float>(height);
-  c->width = w;
-  c->height = h;
-  const float tan_x = fdiv(fmul(0.5f, w), c->fx);
-  const float tan_y = fdiv(fmul(0.5f, h), c->fy);
-  c->lim_xp = ffma(0.3f, tan_x, fdiv(fsub(w, c->cx), c->fx));
-  c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
-  c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
-  c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
-  // Gershgorin bound of R^T R (R includes any scale of the object->world
-  // transform); used only by the conservative early cull.
-  float bound = 0.0f;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    float row = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const float m = c->r[i] * c->r[j] + c->r[3 + i] * c->r[3 + j] + c->r[6 + i] * c->r[6 + j];
-      row += fabsf(m);
-    }
-    bound = fmaxf(bound, row);
-  }
-  c->r_scale2 = bound * 1.001f;
-  c->pad[0] = c->pad[1] = c->pad[2] = 0.0f;
-}
-
-// ---------------------------------------------------------------------------
 // Camera setup: one CTA builds the per-active-camera plans and projection
 // constants, the exclusive prefix of tiles over active cameras (the
 // compositor's work list), and zeroes counters and queue tickets so the frame
@@ -604,6 +542,16 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         const uint32_t rank = i / 3;
         const uint64_t r = base_vis + rank;
         if (r < vcap) dst[r * 3 + (i - rank * 3)] = src[s_slot[rank] * 3 + (i - rank * 3)];
+      }
+      if (p.record_map) {
+        // Training: record index of each visible (slot, Gaussian), for the
+        // per-Gaussian backward pass.
+        int32_t* map_row = p.record_map + (b % p.active_count) * p.record_map_stride;
+        for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
+          const uint64_t r = base_vis + i;
+          const int64_t local = __float_as_int(s_rec[s_slot[i]].b.w) - plan.g_begin;
+          if (r < vcap) map_row[local] = static_cast<int32_t>(r);
+        }
       }
       if (p.mirror_means2d) {
         for (uint32_t i = tid; i < nvis; i += kProjectThreads) {

@@ -193,10 +193,11 @@ extern "C" int vgr_aggregate_chunk_counters(const int64_t* chunk_counters, int64
   return check_launch("aggregate_chunk_counters");
 }
 
-extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
-                          const vgr_outputs* out, const vgr_workspace* ws,
-                          const vgr_render_options* opt, void* stream_ptr,
-                          int64_t* sorted_buffer_selector) {
+namespace vgr {
+
+int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_outputs* out,
+                  const vgr_workspace* ws, const vgr_render_options* opt, void* stream_ptr,
+                  int64_t* sorted_buffer_selector, const TrainHooks* train) {
   if (!scene || !cams || !out || !ws || !opt || !sorted_buffer_selector) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "render arguments must be non-null");
   }
@@ -390,6 +391,14 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     if ((rc = check_launch("render: camera setup")) != VGR_OK) return rc;
     mark(1);
 
+    if (train) {
+      const int64_t map_elems = active * scene->max_scene_gaussians;
+      if (map_elems > 0 &&
+          cudaMemsetAsync(train->record_map, 0xff, static_cast<size_t>(map_elems) * 4, stream) !=
+              cudaSuccess) {
+        return check_launch("render: clear record map", 0);
+      }
+    }
     ProjectParams pp{};
     pp.scratch = scratch;
     pp.layout = layout;
@@ -426,6 +435,8 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     pp.mirror_camera_ids = ws->visible_camera_ids;
     pp.mirror_gaussian_ids = ws->visible_gaussian_ids;
     pp.mirror_radii = ws->visible_radii;
+    pp.record_map = train ? train->record_map : nullptr;
+    pp.record_map_stride = scene->max_scene_gaussians;
     if (pp.mirror_means2d && !(pp.mirror_conics && pp.mirror_depths && pp.mirror_opacities &&
                                pp.mirror_camera_ids && pp.mirror_gaussian_ids && pp.mirror_radii)) {
       return fail(VGR_ERR_INVALID_ARGUMENT, "the visible-record mirrors must be all set or all null");
@@ -498,21 +509,36 @@ extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
     cp.depth = out->depth;
     cp.alpha = out->alpha;
     cp.semantic = out->semantic;
+    cp.final_transmittance = train ? train->final_transmittance : nullptr;
+    cp.last_position = train ? train->last_position : nullptr;
     const unsigned grid = static_cast<unsigned>(max_items);
     const bool full = opt->full_sensor_output != 0;
-    if (ts == 16) {
-      if (full) composite_kernel<16, true><<<grid, composite_threads(16), 0, stream>>>(cp);
-      else composite_kernel<16, false><<<grid, composite_threads(16), 0, stream>>>(cp);
+    if (train) {
+      if (ts == 16) composite_kernel<16, true, true><<<grid, composite_threads(16), 0, stream>>>(cp);
+      else if (ts == 8) composite_kernel<8, true, true><<<grid, composite_threads(8), 0, stream>>>(cp);
+      else composite_kernel<4, true, true><<<grid, composite_threads(4), 0, stream>>>(cp);
+    } else if (ts == 16) {
+      if (full) composite_kernel<16, true, false><<<grid, composite_threads(16), 0, stream>>>(cp);
+      else composite_kernel<16, false, false><<<grid, composite_threads(16), 0, stream>>>(cp);
     } else if (ts == 8) {
-      if (full) composite_kernel<8, true><<<grid, composite_threads(8), 0, stream>>>(cp);
-      else composite_kernel<8, false><<<grid, composite_threads(8), 0, stream>>>(cp);
+      if (full) composite_kernel<8, true, false><<<grid, composite_threads(8), 0, stream>>>(cp);
+      else composite_kernel<8, false, false><<<grid, composite_threads(8), 0, stream>>>(cp);
     } else {
-      if (full) composite_kernel<4, true><<<grid, composite_threads(4), 0, stream>>>(cp);
-      else composite_kernel<4, false><<<grid, composite_threads(4), 0, stream>>>(cp);
+      if (full) composite_kernel<4, true, false><<<grid, composite_threads(4), 0, stream>>>(cp);
+      else composite_kernel<4, false, false><<<grid, composite_threads(4), 0, stream>>>(cp);
     }
     if ((rc = check_launch("render: compositor")) != VGR_OK) return rc;
   }
   mark(6);
   *sorted_buffer_selector = selector;
   return VGR_OK;
+}
+
+}  // namespace vgr
+
+extern "C" int vgr_render(const vgr_scene* scene, const vgr_cameras* cams,
+                          const vgr_outputs* out, const vgr_workspace* ws,
+                          const vgr_render_options* opt, void* stream_ptr,
+                          int64_t* sorted_buffer_selector) {
+  return vgr::render_camera(scene, cams, out, ws, opt, stream_ptr, sorted_buffer_selector, nullptr);
 }

@@ -30,6 +30,113 @@ struct __align__(16) Record {
   float4 c;  // red, green, blue, bits(half2(hx, hy))
 };
 
+// ---------------------------------------------------------------------------
+// Per-camera constants of the projection, computed once per active slot by
+// the setup kernel.  R = view_rotation * env_rotation and
+// t = view_rotation * env_t + view_t, so camera-space p = R m + t.
+// ---------------------------------------------------------------------------
+struct __align__(16) CamConst {
+  float r[9];
+  float t[3];
+  float fx, fy, cx, cy;
+  float lim_xp, lim_xn, lim_yp, lim_yn;
+  float width, height;
+  float r_scale2;   // upper bound of the largest eigenvalue of R^T R (1 for a rotation)
+  float pad[3];
+};
+static_assert(sizeof(CamConst) == 112, "CamConst is fourteen 8-byte words");
+
+__device__ __forceinline__ void make_cam_const(const float* view, const float* env,
+                                               const float* intr, int width, int height,
+                                               CamConst* c) {
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col) {
+      c->r[row * 3 + col] =
+          ffma(view[row * 4 + 2], env[8 + col],
+               ffma(view[row * 4 + 1], env[4 + col], fmul(view[row * 4 + 0], env[col])));
+    }
+    c->t[row] = ffma(view[row * 4 + 2], env[11],
+                     ffma(view[row * 4 + 1], env[7],
+                          ffma(view[row * 4 + 0], env[3], view[row * 4 + 3])));
+  }
+  c->fx = intr[0];
+  c->fy = intr[4];
+  c->cx = intr[2];
+  c->cy = intr[5];
+  const float w = static_cast<float>(width);
+  const float h = static_cast<float>(height);
+  c->width = w;
+  c->height = h;
+  const float tan_x = fdiv(fmul(0.5f, w), c->fx);
+  const float tan_y = fdiv(fmul(0.5f, h), c->fy);
+  c->lim_xp = ffma(0.3f, tan_x, fdiv(fsub(w, c->cx), c->fx));
+  c->lim_xn = ffma(0.3f, tan_x, fdiv(c->cx, c->fx));
+  c->lim_yp = ffma(0.3f, tan_y, fdiv(fsub(h, c->cy), c->fy));
+  c->lim_yn = ffma(0.3f, tan_y, fdiv(c->cy, c->fy));
+  // Gershgorin bound of R^T R (R includes any scale of the object->world
+  // transform); used only by the conservative early cull.
+  float bound = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float row = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float m = c->r[i] * c->r[j] + c->r[3 + i] * c->r[3 + j] + c->r[6 + i] * c->r[6 + j];
+      row += fabsf(m);
+    }
+    bound = fmaxf(bound, row);
+  }
+  c->r_scale2 = bound * 1.001f;
+  c->pad[0] = c->pad[1] = c->pad[2] = 0.0f;
+}
+
+// Rotation matrix (row-major) of a WXYZ quaternion normalised by
+// 1/sqrt(max(|q|^2, 1e-20)) with IEEE division and square root
+// (renderer_cuda.cu:112-143); inv_norm receives that factor.
+__device__ __forceinline__ void quaternion_rotation(float w, float x, float y, float z, float* r,
+                                                    float* inv_norm) {
+  const float norm2 = ffma(z, z, ffma(y, y, ffma(x, x, fmul(w, w))));
+  const float inv = fdiv(1.0f, fsqrt(fmaxf(norm2, 1.0e-20f)));
+  *inv_norm = inv;
+  w = fmul(w, inv);
+  x = fmul(x, inv);
+  y = fmul(y, inv);
+  z = fmul(z, inv);
+  const float xx = fmul(x, x), yy = fmul(y, y), zz = fmul(z, z);
+  const float xy = fmul(x, y), xz = fmul(x, z), yz = fmul(y, z);
+  const float wx = fmul(w, x), wy = fmul(w, y), wz = fmul(w, z);
+  r[0] = fsub(1.0f, fmul(2.0f, fadd(yy, zz)));
+  r[1] = fmul(2.0f, fsub(xy, wz));
+  r[2] = fmul(2.0f, fadd(xz, wy));
+  r[3] = fmul(2.0f, fadd(xy, wz));
+  r[4] = fsub(1.0f, fmul(2.0f, fadd(xx, zz)));
+  r[5] = fmul(2.0f, fsub(yz, wx));
+  r[6] = fmul(2.0f, fsub(xz, wy));
+  r[7] = fmul(2.0f, fadd(yz, wx));
+  r[8] = fsub(1.0f, fmul(2.0f, fadd(xx, yy)));
+}
+
+// Object-space covariance Sigma = R diag(s^2) R^T, upper triangle
+// (00, 01, 02, 11, 12, 22) (renderer_cuda.cu:492-540).
+__device__ __forceinline__ void covariance_from_quaternion(float w, float x, float y, float z,
+                                                           float sx, float sy, float sz,
+                                                           float* cov) {
+  float r[9];
+  float inv;
+  quaternion_rotation(w, x, y, z, r, &inv);
+  const float s2[3] = {fmul(sx, sx), fmul(sy, sy), fmul(sz, sz)};
+  const int rows[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float* a = r + rows[k][0] * 3;
+    const float* b = r + rows[k][1] * 3;
+    cov[k] =
+        ffma(fmul(a[2], b[2]), s2[2], ffma(fmul(a[1], b[1]), s2[1], fmul(fmul(a[0], b[0]), s2[0])));
+  }
+}
+
 // Scratch header at offset 0 of the scratch buffer.
 struct ScratchHeader {
   int32_t status;              // device error bits (kDeviceError*)

@@ -66,6 +66,8 @@ struct ProjectParams {
   int32_t* mirror_camera_ids;
   int32_t* mirror_gaussian_ids;
   int32_t* mirror_radii;
+  int32_t* record_map;         // training: [A, record_map_stride] record of (slot, local Gaussian)
+  int64_t record_map_stride;
 };
 
 struct SortParams {
@@ -118,6 +120,136 @@ struct CompositeParams {
   float* depth;
   float* alpha;
   int64_t* semantic;
+  float* final_transmittance;  // training: [P] transmittance after the last blended record
+  int32_t* last_position;      // training: [P] sorted position one past the last blended record
+};
+
+template <int kTile>
+struct CompositeGeometry {
+  static constexpr int kBlockW = kTile < 8 ? kTile : 8;  // warp block width (px)
+  static constexpr int kLaneRows =
+      (32 / kBlockW) < (kTile / 2) ? (32 / kBlockW) : (kTile / 2);  // lane rows
+  static constexpr int kBlockH = 2 * kLaneRows;  // warp block height (px)
+  static constexpr int kWarpsX = kTile / kBlockW;
+  static constexpr int kWarpsY = kTile / kBlockH;
+  static constexpr int kWarps = kWarpsX * kWarpsY;
+  static constexpr int kThreads = kWarps * 32;
+};
+
+constexpr int kCompositeBatch = 256;
+
+// Shared-memory form of one record for the compositor loops (forward and
+// backward use the same values, so both see the same alpha decisions):
+// geo = (mean_x, mean_y, -conic_xx/2, -conic_xy), cpo = (-conic_yy/2, lo,
+// opacity, -), col = (r, g, b, depth), and the mask of the warp blocks the
+// record's conservative alpha footprint touches.  lo = max(-qmax/2, -20)
+// merges the footprint bound with the reference's power >= -20 cut.
+template <int kTile>
+__device__ __forceinline__ void stage_composite_record(const Record& rec, float tile_x0,
+                                                       float tile_y0, float4& geo, float4& cpo,
+                                                       float4& col, uint32_t& mask_out) {
+  using Geo = CompositeGeometry<kTile>;
+  geo = make_float4(rec.a.x, rec.a.y, fmul(-0.5f, rec.a.z), -rec.a.w);
+  const float o = rec.b.y;
+  const float qmax = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
+  cpo = make_float4(fmul(-0.5f, rec.b.x), fmaxf(fmul(-0.5f, qmax), -20.0f), o, 0.0f);
+  col = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
+  const __half2 box = *reinterpret_cast<const __half2*>(&rec.c.w);
+  const float hx = __low2float(box);
+  const float hy = __high2float(box);
+  uint32_t mask = 0;
+#pragma unroll
+  for (int w = 0; w < Geo::kWarps; ++w) {
+    const float bx0 = tile_x0 + static_cast<float>((w % Geo::kWarpsX) * Geo::kBlockW) + 0.5f;
+    const float by0 = tile_y0 + static_cast<float>((w / Geo::kWarpsX) * Geo::kBlockH) + 0.5f;
+    const float bx1 = bx0 + static_cast<float>(Geo::kBlockW - 1);
+    const float by1 = by0 + static_cast<float>(Geo::kBlockH - 1);
+    const bool hit = rec.a.x + hx >= bx0 && rec.a.x - hx <= bx1 && rec.a.y + hy >= by0 &&
+                     rec.a.y - hy <= by1;
+    mask |= hit ? (1u << w) : 0u;
+  }
+  mask_out = mask;
+}
+
+// Work item (one (camera, tile) of the compositor grid) -> active slot plan
+// and tile index within the camera.  Slots are dense in [0, A) and every
+// slot's tiles are contiguous; tile_prefix is monotone, so it is searched
+// (starting from item / hint when every camera has `hint` tiles).
+__device__ __forceinline__ bool locate_tile(const unsigned char* scratch, const ScratchLayout& layout,
+                                            int64_t active_count, int64_t hint, int64_t item,
+                                            CamPlan& plan, int64_t& local_tile) {
+  const CamPlan* plans = reinterpret_cast<const CamPlan*>(scratch + layout.plans);
+  const int64_t* tile_prefix = reinterpret_cast<const int64_t*>(scratch + layout.tile_prefix);
+  const int64_t total = tile_prefix[active_count];
+  if (item >= total) return false;
+  int64_t lo = 0, hi = active_count;  // tile_prefix[lo] <= item < tile_prefix[hi]
+  if (hint > 0) {
+    const int64_t guess = item / hint;
+    if (guess < active_count && tile_prefix[guess] <= item && item < tile_prefix[guess + 1]) {
+      lo = guess;
+      hi = guess + 1;
+    }
+  }
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (tile_prefix[mid] <= item) lo = mid; else hi = mid;
+  }
+  plan = plans[lo];
+  local_tile = item - tile_prefix[lo];
+  return true;
+}
+
+// Differentiable form.
+struct TrainActivateParams {
+  const float* log_scales;      // [G,3]
+  const float* rotations;       // [G,4] WXYZ, any norm
+  const float* opacity_logits;  // [G]
+  int64_t count;
+  float* covariances;           // [G,6] out
+  float* opacities;             // [G] out
+};
+
+struct CompositeBackwardParams {
+  const unsigned char* scratch;
+  ScratchLayout layout;
+  int64_t active_count;
+  int64_t tiles_per_camera_hint;
+  const Record* records;
+  const int32_t* values;              // sorted record indices
+  const int32_t* tile_starts;
+  const int32_t* tile_ends;
+  const float* final_transmittance;   // [P]
+  const int32_t* last_position;       // [P]
+  const float* depth;                 // [P] forward depth output
+  const float* grad_rgb;              // [P,3]
+  const float* grad_depth;            // [P] or null
+  const float* grad_alpha;            // [P] or null
+  float4* record_grads;               // [V,3]
+};
+
+struct ProjectBackwardParams {
+  const unsigned char* scratch;
+  ScratchLayout layout;
+  int64_t active_count;
+  const int64_t* scene_offsets;
+  int scene_count;
+  int64_t gaussian_count;
+  const float* means;
+  const float* covariances;     // forward activation output
+  const float* opacities;       // forward activation output
+  const float* features;
+  int64_t feature_width;
+  const float* log_scales;
+  const float* rotations;
+  float cov_eps;
+  const int32_t* record_map;
+  int64_t record_map_stride;
+  const float4* record_grads;
+  float* d_means;
+  float* d_log_scales;
+  float* d_rotations;
+  float* d_opacity_logits;
+  float* d_features;
 };
 
 __global__ void camera_setup_kernel(SetupParams p);
@@ -128,8 +260,15 @@ __global__ void sort_onesweep_kernel(SortParams p);
 __global__ void tile_scan_kernel(BucketParams p);
 __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
-template <int kTile, bool kFull>
+template <int kTile, bool kFull, bool kTrain>
 __global__ void composite_kernel(CompositeParams p);
+
+__global__ void train_activate_kernel(TrainActivateParams p);
+__global__ void zero_record_grads_kernel(float4* grads, const int64_t* counters, int64_t capacity);
+template <int kTile>
+__global__ void composite_backward_kernel(CompositeBackwardParams p);
+template <int kShDegree>
+__global__ void project_backward_kernel(ProjectBackwardParams p);
 
 // Threads per compositor CTA (two pixels per thread, 8x8-pixel warp blocks).
 constexpr int composite_threads(int tile) { return tile >= 16 ? 128 : 32; }

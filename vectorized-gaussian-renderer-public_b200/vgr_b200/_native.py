@@ -115,6 +115,34 @@ class VgrRenderOptions(ctypes.Structure):
     ]
 
 
+class VgrTrainParams(ctypes.Structure):
+    _fields_ = [("log_scales", _c_p), ("rotations", _c_p), ("opacity_logits", _c_p)]
+
+
+class VgrTrainState(ctypes.Structure):
+    _fields_ = [
+        ("final_transmittance", _c_p),
+        ("last_position", _c_p),
+        ("record_map", _c_p),
+        ("record_map_capacity", _c_i64),
+        ("record_grads", _c_p),
+    ]
+
+
+class VgrOutputGrads(ctypes.Structure):
+    _fields_ = [("rgb", _c_p), ("depth", _c_p), ("alpha", _c_p)]
+
+
+class VgrParamGrads(ctypes.Structure):
+    _fields_ = [
+        ("means", _c_p),
+        ("log_scales", _c_p),
+        ("rotations", _c_p),
+        ("opacity_logits", _c_p),
+        ("features", _c_p),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
     ("vgr_version", ctypes.c_char_p, []),
@@ -158,6 +186,41 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
             ctypes.POINTER(VgrRenderOptions),
             _c_p,
             ctypes.POINTER(_c_i64),
+        ],
+    ),
+    (
+        "vgr_train_activate",
+        ctypes.c_int,
+        [ctypes.POINTER(VgrTrainParams), _c_i64, _c_p, _c_p, _c_p],
+    ),
+    (
+        "vgr_render_train",
+        ctypes.c_int,
+        [
+            ctypes.POINTER(VgrScene),
+            ctypes.POINTER(VgrCameras),
+            ctypes.POINTER(VgrOutputs),
+            ctypes.POINTER(VgrWorkspace),
+            ctypes.POINTER(VgrRenderOptions),
+            ctypes.POINTER(VgrTrainState),
+            _c_p,
+            ctypes.POINTER(_c_i64),
+        ],
+    ),
+    (
+        "vgr_render_backward",
+        ctypes.c_int,
+        [
+            ctypes.POINTER(VgrScene),
+            ctypes.POINTER(VgrTrainParams),
+            ctypes.POINTER(VgrCameras),
+            ctypes.POINTER(VgrOutputs),
+            ctypes.POINTER(VgrWorkspace),
+            ctypes.POINTER(VgrRenderOptions),
+            ctypes.POINTER(VgrTrainState),
+            ctypes.POINTER(VgrOutputGrads),
+            ctypes.POINTER(VgrParamGrads),
+            _c_p,
         ],
     ),
 ]

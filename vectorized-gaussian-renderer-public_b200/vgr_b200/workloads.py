@@ -295,3 +295,32 @@ def ragged_workload(frames: int = 100, *, seed: int = 7, scale: float = 1.0) -> 
         w, h = widths[c], heights[c]
         intr[c] = pinhole(1, 0.75 * w, 0.75 * w, w / 2.0, h / 2.0)[0]
     return RaggedWorkload(scenes, scene_ids, heights, widths, torch.stack(views).contiguous(), intr)
+
+
+# --------------------------------------------------------------------------- differentiable form
+@dataclass
+class TrainingWorkload:
+    params: dict[str, torch.Tensor]   # means, log_scales, rotations, opacity_logits, features
+    targets: dict[str, torch.Tensor]  # the target scene's parameters (perturbed copy)
+    rig: CameraRig
+
+
+def training_workload(gaussians: int = 500_000, cameras: int = 16, size: int = 512, *,
+                      seed: int = 13) -> TrainingWorkload:
+    """Differentiable-form workload: a 500k-Gaussian SH3 scene (the batched
+    scene's laws) as raw parameters, 16 orbit cameras of 512x512 (focal 420),
+    and a target scene = means + N(0, 0.01), SH coefficients + N(0, 0.05)."""
+    scene = synthetic_scene(gaussians, seed=seed, mean_half_extent=5.0, sh_degree=3)
+    params = {
+        "means": scene.means,
+        "log_scales": torch.log(scene.scales),
+        "rotations": scene.rotations,
+        "opacity_logits": torch.logit(scene.opacities.double(), eps=1e-6).float(),
+        "features": scene.features,
+    }
+    gen = torch.Generator().manual_seed(seed + 1)
+    targets = dict(params)
+    targets["means"] = (params["means"] + torch.randn(params["means"].shape, generator=gen) * 0.01).contiguous()
+    targets["features"] = (params["features"] + torch.randn(params["features"].shape, generator=gen) * 0.05).contiguous()
+    rig = orbit_cameras(cameras, seed=seed + 2, width=size, height=size, focal=420.0)
+    return TrainingWorkload(params=params, targets=targets, rig=rig)
