@@ -294,6 +294,13 @@ int vgr_render_backward(const vgr_scene* scene, const vgr_train_params* params,
                         const vgr_workspace* workspace, const vgr_render_options* options,
                         const vgr_train_state* state, const vgr_output_grads* grads,
                         const vgr_param_grads* param_grads, void* stream);
+/* Training loss of the differentiable form's benchmark and trainers:
+ * L = mean((rgb - target_rgb)^2) + depth_weight * sum(|depth - target_depth|)
+ * / pixels, the depth term over pixels where both depths are finite.  Writes
+ * loss[0] and the gradients dL/drgb [P,3] and dL/ddepth [P] in one pass. */
+int vgr_photometric_loss(const float* rgb, const float* target_rgb, const float* depth,
+                         const float* target_depth, int64_t pixels, double depth_weight,
+                         float* loss, float* grad_rgb, float* grad_depth, void* stream);
 /* ------------------------------------------------------------------ LiDAR */
 
 /* Caller-owned Gaussian LiDAR scene (lidar_scene.py:13-96): WXYZ rotations,

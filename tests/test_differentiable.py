@@ -177,3 +177,56 @@ def test_gpu_backward_needs_the_last_frame():
         first[0].sum().backward()
     second[0].sum().backward()
     assert params["means"].grad is not None and torch.isfinite(params["means"].grad).all()
+
+
+@pytest.mark.gpu
+def test_gpu_photometric_loss_matches_torch():
+    from vgr_b200.differentiable import photometric_loss
+
+    gen = torch.Generator().manual_seed(2)
+    rgb = torch.rand((2, 8, 8, 3), generator=gen).cuda().requires_grad_(True)
+    depth = (torch.rand((2, 8, 8, 1), generator=gen) * 5).cuda()
+    depth[0, 0, 0, 0] = float("inf")
+    depth = depth.requires_grad_(True)
+    t_rgb = torch.rand((2, 8, 8, 3), generator=gen).cuda()
+    t_depth = (torch.rand((2, 8, 8, 1), generator=gen) * 5).cuda()
+    t_depth[1, 2, 3, 0] = float("inf")
+    loss = photometric_loss(rgb, depth, t_rgb, t_depth, 0.1)
+    loss.backward()
+    r = rgb.detach().clone().requires_grad_(True)
+    d = depth.detach().clone().requires_grad_(True)
+    finite = torch.isfinite(d) & torch.isfinite(t_depth)
+    diff = torch.where(finite, d - torch.where(finite, t_depth, torch.zeros_like(t_depth)), torch.zeros_like(d))
+    want = ((r - t_rgb) ** 2).mean() + 0.1 * diff.abs().mean()
+    want.backward()
+    assert abs(float(loss.detach()) - float(want.detach())) < 1e-6
+    assert torch.allclose(rgb.grad, r.grad, rtol=1e-5, atol=1e-8)
+    assert torch.allclose(depth.grad, d.grad, rtol=1e-5, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_gpu_deferred_capacity_check_raises_and_regrows():
+    from vgr_b200.differentiable import DifferentiableRenderer
+
+    scene = _scene(8)
+    view, intr = _cameras(2)
+    sync = DifferentiableRenderer(height=SIZE, width=SIZE, sh_degree=3, tile_size=4)
+    deferred = DifferentiableRenderer(height=SIZE, width=SIZE, sh_degree=3, tile_size=4, capacity_check="deferred")
+    grads = []
+    for renderer in (sync, deferred):
+        params = {k: v.cuda().requires_grad_(True) for k, v in scene.items()}
+        for _ in range(2):  # the first frame calibrates, the second is checked late
+            rgb, depth, alpha = renderer.render(*(params[k] for k in NAMES), view.cuda(), intr.cuda())
+            (rgb.sum() + alpha.sum()).backward()
+        grads.append(params["means"].grad.clone())
+    assert torch.allclose(grads[0], grads[1], rtol=1e-5, atol=1e-6)
+    # Much larger Gaussians overflow the calibrated intersection capacity.
+    big = dict(scene)
+    big["log_scales"] = scene["log_scales"] + 2.5
+    params = {k: v.cuda().requires_grad_(True) for k, v in big.items()}
+    rgb, depth, alpha = deferred.render(*(params[k] for k in NAMES), view.cuda(), intr.cuda())
+    with pytest.raises(RuntimeError, match="overflowed"):
+        rgb.sum().backward()
+    rgb, depth, alpha = deferred.render(*(params[k] for k in NAMES), view.cuda(), intr.cuda())
+    rgb.sum().backward()
+    assert torch.isfinite(params["means"].grad).all()

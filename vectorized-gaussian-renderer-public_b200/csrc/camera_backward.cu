@@ -67,11 +67,58 @@ __global__ void __launch_bounds__(256) zero_record_grads_kernel(float4* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Photometric loss L = mean((rgb - t)^2) + w mean(|depth - t_depth|) over the
+// pixels where both depths are finite, with its gradient, in one pass.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) photometric_loss_kernel(PhotometricLossParams p) {
+  __shared__ float s_warp[8];
+  const float rgb_scale = 1.0f / static_cast<float>(3 * p.pixels);
+  const float depth_scale = p.depth_weight / static_cast<float>(p.pixels);
+  float sum = 0.0f;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.pixels;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float d = p.rgb[i * 3 + c] - p.target_rgb[i * 3 + c];
+      sum = fmaf(d * d, rgb_scale, sum);
+      p.grad_rgb[i * 3 + c] = 2.0f * rgb_scale * d;
+    }
+    const float z = p.depth[i];
+    const float tz = p.target_depth[i];
+    float gz = 0.0f;
+    if (isfinite(z) && isfinite(tz)) {
+      const float d = z - tz;
+      sum = fmaf(fabsf(d), depth_scale, sum);
+      gz = d > 0.0f ? depth_scale : (d < 0.0f ? -depth_scale : 0.0f);
+    }
+    p.grad_depth[i] = gz;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float block = 0.0f;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) block += s_warp[w];
+    atomicAdd(p.loss, block);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Compositor backward.
 // ---------------------------------------------------------------------------
-// Partial derivatives of one record, in this order.
-enum RecordGrad { kGMeanX, kGMeanY, kGConic0, kGConic1, kGConic2, kGOpacity, kGRed, kGGreen, kGBlue,
-                  kGDepth, kRecordGradCount };
+// Per-record sums gathered over a record's pixels, in this order: the
+// moments of dp = dL/dpower against the pixel offset (dx, dy) from the mean
+// (dp dx, dp dy, dp dx^2, dp dx dy, dp dy^2), from which the flush forms the
+// mean and conic derivatives with the record's conic; dL/dopacity; the
+// colour and depth derivatives.
+enum RecordGrad { kMDx, kMDy, kMDxx, kMDxy, kMDyy, kGOpacity, kGRed, kGGreen, kGBlue, kGDepth,
+                  kRecordGradCount };
+// Shared-memory stride of one record's terms: odd, so that both the lanes
+// of a transposed sum (one term each) and the flush (one record each) hit
+// distinct banks.
+constexpr int kGradStride = kRecordGradCount + 1;
 
 struct PixelGrad {
   float t;       // transmittance after the records not yet visited
@@ -106,40 +153,50 @@ __device__ __forceinline__ PixelGrad load_pixel_grad(const CompositeBackwardPara
   return q;
 }
 
-// One record on one pixel, back to front.  The alpha decision repeats the
-// forward's arithmetic on the same staged values.
-__device__ __forceinline__ bool backward_pixel(PixelGrad& q, float power, int32_t pos,
-                                               const float4& geo, const float4& cpo,
+__device__ __forceinline__ float fast_exp(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.4426950408889634f));
+  return y;
+}
+
+__device__ __forceinline__ float fast_rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One record on one pixel, back to front, without branches: c says whether
+// the record was blended into the pixel (power in range, before the pixel's
+// last blended record, alpha >= 1/255 on the forward's exact arithmetic).
+// A record that was not blended enters with alpha = 0, which leaves the
+// pixel state unchanged and adds nothing.  Derivative values use the
+// special-function unit's exp and reciprocal (relative error ~1e-7).
+__device__ __forceinline__ void backward_pixel(PixelGrad& q, bool c, float oe, float e,
                                                const float4& col, float dx, float dy, float* g) {
-  if (pos >= q.last) return false;
-  if (!(power >= cpo.y && power <= 0.0f)) return false;
-  const float e = vexp(power);
-  const float oe = fmul(cpo.z, e);
-  const float alpha = fminf(kMaxAlpha, oe);
-  if (!(alpha >= kAlphaThreshold)) return false;
-  const float one_minus = 1.0f - alpha;
-  const float t_before = q.t / one_minus;
+  const bool unclamped = c && oe < kMaxAlpha;
+  const float alpha = c ? fminf(kMaxAlpha, oe) : 0.0f;
+  const float de = unclamped ? e : 0.0f;          // d alpha / d opacity
+  const float dpow = unclamped ? alpha : 0.0f;    // d alpha / d power
+  const float inv = c ? fast_rcp(1.0f - alpha) : 1.0f;
+  const float t_before = q.t * inv;
   const float w = alpha * t_before;
   const float f = q.gr * col.x + q.gg * col.y + q.gb * col.z + q.gz * col.w;
-  const float d_alpha = f * t_before + (q.k - q.s) / one_minus;
+  const float d_alpha = f * t_before + (q.k - q.s) * inv;
   q.s = fmaf(f, w, q.s);
   q.t = t_before;
-  g[kGRed] += q.gr * w;
-  g[kGGreen] += q.gg * w;
-  g[kGBlue] += q.gb * w;
-  g[kGDepth] += q.gz * w;
-  if (oe < kMaxAlpha) {
-    g[kGOpacity] += d_alpha * e;
-    const float dp = d_alpha * alpha;
-    // power = geo.z dx^2 + geo.w dx dy + cpo.x dy^2 with geo.z = -c0/2,
-    // geo.w = -c1, cpo.x = -c2/2 and dx = px - mean_x.
-    g[kGMeanX] -= dp * (2.0f * geo.z * dx + geo.w * dy);
-    g[kGMeanY] -= dp * (geo.w * dx + 2.0f * cpo.x * dy);
-    g[kGConic0] -= 0.5f * dp * dx * dx;
-    g[kGConic1] -= dp * dx * dy;
-    g[kGConic2] -= 0.5f * dp * dy * dy;
-  }
-  return true;
+  g[kGRed] = fmaf(q.gr, w, g[kGRed]);
+  g[kGGreen] = fmaf(q.gg, w, g[kGGreen]);
+  g[kGBlue] = fmaf(q.gb, w, g[kGBlue]);
+  g[kGDepth] = fmaf(q.gz, w, g[kGDepth]);
+  g[kGOpacity] = fmaf(d_alpha, de, g[kGOpacity]);
+  const float dp = d_alpha * dpow;
+  const float dpx = dp * dx;
+  const float dpy = dp * dy;
+  g[kMDx] += dpx;
+  g[kMDy] += dpy;
+  g[kMDxx] = fmaf(dpx, dx, g[kMDxx]);
+  g[kMDxy] = fmaf(dpx, dy, g[kMDxy]);
+  g[kMDyy] = fmaf(dpy, dy, g[kMDyy]);
 }
 
 template <int kTile>
@@ -150,7 +207,7 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
   __shared__ float4 s_cpo[kCompositeBatch];
   __shared__ float4 s_col[kCompositeBatch];
   __shared__ uint32_t s_mask[kCompositeBatch];
-  __shared__ float s_grad[kRecordGradCount][kCompositeBatch];
+  __shared__ float s_grad[kCompositeBatch * kGradStride];
   __shared__ int32_t s_last[Geo::kWarps];
 
   CamPlan plan;
@@ -200,7 +257,7 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
       stage_composite_record<kTile>(p.records[p.values[lo + j]], tile_x0, tile_y0, s_geo[j],
                                     s_cpo[j], s_col[j], s_mask[j]);
 #pragma unroll
-      for (int f = 0; f < kRecordGradCount; ++f) s_grad[f][j] = 0.0f;
+      for (int f = 0; f < kRecordGradCount; ++f) s_grad[j * kGradStride + f] = 0.0f;
     }
     __syncthreads();
     if (lo < warp_last) {
@@ -222,25 +279,63 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
           const float dy1 = fsub(cy1, geo.y);
           const float p0 = ffma(fmul(cpo.x, dy0), dy0, ffma(bdx, dy0, adx));
           const float p1 = ffma(fmul(cpo.x, dy1), dy1, ffma(bdx, dy1, adx));
+          const bool in0 = p0 >= cpo.y && p0 <= 0.0f && pos < q0.last;
+          const bool in1 = p1 >= cpo.y && p1 <= 0.0f && pos < q1.last;
+          if (!__any_sync(0xffffffffu, in0 || in1)) continue;
+          const float o = cpo.z;
+          float e0 = fast_exp(p0);
+          float e1 = fast_exp(p1);
+          float oe0 = o * e0;
+          float oe1 = o * e1;
+          // The 1/255 decision must be the forward's: near it, take it on
+          // the forward's exact exp (rare, so warp-uniform).
+          const bool near = (in0 && fabsf(oe0 - kAlphaThreshold) <= 1.0e-5f * kAlphaThreshold) ||
+                            (in1 && fabsf(oe1 - kAlphaThreshold) <= 1.0e-5f * kAlphaThreshold);
+          if (__any_sync(0xffffffffu, near)) {
+            e0 = vexp(p0);
+            e1 = vexp(p1);
+            oe0 = fmul(o, e0);
+            oe1 = fmul(o, e1);
+          }
+          const bool c0 = in0 && oe0 >= kAlphaThreshold;
+          const bool c1 = in1 && oe1 >= kAlphaThreshold;
+          const uint32_t hits = __ballot_sync(0xffffffffu, c0 || c1);
+          if (hits == 0u) continue;
+          const float4 col = s_col[j];
           float g[kRecordGradCount];
 #pragma unroll
           for (int f = 0; f < kRecordGradCount; ++f) g[f] = 0.0f;
-          bool hit = false;
-          if ((p0 >= cpo.y && p0 <= 0.0f) || (p1 >= cpo.y && p1 <= 0.0f)) {
-            const float4 col = s_col[j];
-            hit |= backward_pixel(q0, p0, pos, geo, cpo, col, dx, dy0, g);
-            hit |= backward_pixel(q1, p1, pos, geo, cpo, col, dx, dy1, g);
-          }
-          if (__any_sync(0xffffffffu, hit)) {
+          backward_pixel(q0, c0, oe0, e0, col, dx, dy0, g);
+          backward_pixel(q1, c1, oe1, e1, col, dx, dy1, g);
+          const bool hit = c0 || c1;
+          float* dst = s_grad + j * kGradStride;
+          if (__popc(hits) <= 4) {
+            // At most four pixel pairs touched the record: add their terms
+            // directly.
+            if (hit) {
 #pragma unroll
-            for (int f = 0; f < kRecordGradCount; ++f) {
-#pragma unroll
-              for (int o = 16; o > 0; o >>= 1) g[f] += __shfl_xor_sync(0xffffffffu, g[f], o);
+              for (int f = 0; f < kRecordGradCount; ++f) atomicAdd(dst + f, g[f]);
             }
-            if (lane == 0) {
+          } else {
+            // Transposed warp sum: four halving exchanges leave lane l with
+            // a partial sum of term (l >> 1) over 16 lanes, the last one
+            // adds the other half; 16 shuffles instead of 5 per term.
+            float v[16];
 #pragma unroll
-              for (int f = 0; f < kRecordGradCount; ++f) atomicAdd(&s_grad[f][j], g[f]);
+            for (int f = 0; f < 16; ++f) v[f] = f < kRecordGradCount ? g[f] : 0.0f;
+#pragma unroll
+            for (int half = 8; half >= 1; half >>= 1) {
+              const bool upper = (lane & (half * 2)) != 0;
+#pragma unroll
+              for (int i = 0; i < half; ++i) {
+                const float send = upper ? v[i] : v[i + half];
+                const float keep = upper ? v[i + half] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half * 2);
+              }
             }
+            v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+            const int term = lane >> 1;
+            if ((lane & 1) == 0 && term < kRecordGradCount) atomicAdd(dst + term, v[0]);
           }
         }
       }
@@ -251,13 +346,19 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
       bool any = false;
 #pragma unroll
       for (int f = 0; f < kRecordGradCount; ++f) {
-        g[f] = s_grad[f][j];
+        g[f] = s_grad[j * kGradStride + f];
         any |= g[f] != 0.0f;
       }
       if (!any) continue;
+      // power = geo.z dx^2 + geo.w dx dy + cpo.x dy^2 with geo.z = -c0/2,
+      // geo.w = -c1, cpo.x = -c2/2 and (dx, dy) = pixel - mean.
+      const float4 geo = s_geo[j];
+      const float cyy = s_cpo[j].x;
+      const float d_mean_x = -(2.0f * geo.z * g[kMDx] + geo.w * g[kMDy]);
+      const float d_mean_y = -(geo.w * g[kMDx] + 2.0f * cyy * g[kMDy]);
       float4* dst = p.record_grads + static_cast<int64_t>(p.values[lo + j]) * 3;
-      atomicAdd(dst + 0, make_float4(g[kGMeanX], g[kGMeanY], g[kGConic0], g[kGConic1]));
-      atomicAdd(dst + 1, make_float4(g[kGConic2], g[kGOpacity], g[kGDepth], 0.0f));
+      atomicAdd(dst + 0, make_float4(d_mean_x, d_mean_y, -0.5f * g[kMDxx], -g[kMDxy]));
+      atomicAdd(dst + 1, make_float4(-0.5f * g[kMDyy], g[kGOpacity], g[kGDepth], 0.0f));
       atomicAdd(dst + 2, make_float4(g[kGRed], g[kGGreen], g[kGBlue], 0.0f));
     }
     __syncthreads();
@@ -271,6 +372,7 @@ template __global__ void composite_backward_kernel<16>(CompositeBackwardParams);
 // ---------------------------------------------------------------------------
 // Projection backward, one thread per Gaussian.
 // ---------------------------------------------------------------------------
+constexpr int kProjectBackwardThreads = 128;
 // Real SH basis (the forward's constants) and its derivative with respect to
 // the unit view direction (x, y, z), contracted with per-coefficient weights
 // d_basis: returns sum_k d_basis[k] * d basis_k / d(x, y, z).
@@ -357,7 +459,7 @@ __device__ __forceinline__ void sh_direction_grad(float x, float y, float z, con
 }
 
 template <int kShDegree>
-__global__ void __launch_bounds__(128) project_backward_kernel(ProjectBackwardParams p) {
+__global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kernel(ProjectBackwardParams p) {
   constexpr int kCount = kShDegree < 0 ? 1 : (kShDegree + 1) * (kShDegree + 1);
   constexpr int kFloats = kShDegree < 0 ? 3 : kCount * 3;
   const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -384,9 +486,13 @@ __global__ void __launch_bounds__(128) project_backward_kernel(ProjectBackwardPa
   float dm[3] = {0.0f, 0.0f, 0.0f};
   float dcov[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
   float dop = 0.0f;
-  float dsh[kFloats];
+  // Colour-coefficient sums live in shared memory (thread-major, so each
+  // access is conflict-free): 48 accumulators in registers would cap the
+  // kernel at two CTAs per SM.
+  __shared__ float s_dsh[kFloats * kProjectBackwardThreads];
+  float* dsh = s_dsh + threadIdx.x;
 #pragma unroll
-  for (int k = 0; k < kFloats; ++k) dsh[k] = 0.0f;
+  for (int k = 0; k < kFloats; ++k) dsh[k * kProjectBackwardThreads] = 0.0f;
 
   const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
   const CamConst* consts = reinterpret_cast<const CamConst*>(p.scratch + p.layout.cam_consts);
@@ -491,8 +597,8 @@ __global__ void __launch_bounds__(128) project_backward_kernel(ProjectBackwardPa
     // Colour.
     if (kShDegree < 0) {
       dsh[0] += g2.x;
-      dsh[1] += g2.y;
-      dsh[2] += g2.z;
+      dsh[kProjectBackwardThreads] += g2.y;
+      dsh[2 * kProjectBackwardThreads] += g2.z;
     } else {
       const float dvx = ffma(R[6], pz, ffma(R[3], py, fmul(R[0], px)));
       const float dvy = ffma(R[7], pz, ffma(R[4], py, fmul(R[1], px)));
@@ -519,7 +625,7 @@ __global__ void __launch_bounds__(128) project_backward_kernel(ProjectBackwardPa
         db[k] = 0.0f;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
-          dsh[k * 3 + ch] += basis[k] * drgb[ch];
+          dsh[(k * 3 + ch) * kProjectBackwardThreads] += basis[k] * drgb[ch];
           db[k] += __ldg(coeffs + k * 3 + ch) * drgb[ch];
         }
       }
@@ -615,7 +721,7 @@ __global__ void __launch_bounds__(128) project_backward_kernel(ProjectBackwardPa
   for (int k = 0; k < 3; ++k) p.d_means[g * 3 + k] = dm[k];
   float* dfeat = p.d_features + g * p.feature_width;
 #pragma unroll
-  for (int k = 0; k < kFloats; ++k) dfeat[k] = dsh[k];
+  for (int k = 0; k < kFloats; ++k) dfeat[k] = dsh[k * kProjectBackwardThreads];
   for (int64_t k = kFloats; k < p.feature_width; ++k) dfeat[k] = 0.0f;
 }
 

@@ -227,6 +227,18 @@ struct CompositeBackwardParams {
   float4* record_grads;               // [V,3]
 };
 
+struct PhotometricLossParams {
+  const float* rgb;            // [P,3]
+  const float* target_rgb;     // [P,3]
+  const float* depth;          // [P]
+  const float* target_depth;   // [P]
+  int64_t pixels;
+  float depth_weight;
+  float* loss;                 // [1], zeroed before the launch
+  float* grad_rgb;             // [P,3] dL/drgb
+  float* grad_depth;           // [P] dL/ddepth
+};
+
 struct ProjectBackwardParams {
   const unsigned char* scratch;
   ScratchLayout layout;
@@ -265,6 +277,7 @@ __global__ void composite_kernel(CompositeParams p);
 
 __global__ void train_activate_kernel(TrainActivateParams p);
 __global__ void zero_record_grads_kernel(float4* grads, const int64_t* counters, int64_t capacity);
+__global__ void photometric_loss_kernel(PhotometricLossParams p);
 template <int kTile>
 __global__ void composite_backward_kernel(CompositeBackwardParams p);
 template <int kShDegree>

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cmath>
 
 #include "../../include/vgr_b200.h"
 #include "vgr_api_internal.h"
@@ -207,15 +208,48 @@ extern "C" int vgr_render_backward(const vgr_scene* scene, const vgr_train_param
     pb.d_rotations = pg->rotations;
     pb.d_opacity_logits = pg->opacity_logits;
     pb.d_features = pg->features;
-    const unsigned grid = static_cast<unsigned>((count + 127) / 128);
+    constexpr int kThreads = 128;  // kProjectBackwardThreads
+    const unsigned grid = static_cast<unsigned>((count + kThreads - 1) / kThreads);
     switch (opt->sh_degree) {
-      case -1: vgr::project_backward_kernel<-1><<<grid, 128, 0, stream>>>(pb); break;
-      case 0: vgr::project_backward_kernel<0><<<grid, 128, 0, stream>>>(pb); break;
-      case 1: vgr::project_backward_kernel<1><<<grid, 128, 0, stream>>>(pb); break;
-      case 2: vgr::project_backward_kernel<2><<<grid, 128, 0, stream>>>(pb); break;
-      default: vgr::project_backward_kernel<3><<<grid, 128, 0, stream>>>(pb); break;
+      case -1: vgr::project_backward_kernel<-1><<<grid, kThreads, 0, stream>>>(pb); break;
+      case 0: vgr::project_backward_kernel<0><<<grid, kThreads, 0, stream>>>(pb); break;
+      case 1: vgr::project_backward_kernel<1><<<grid, kThreads, 0, stream>>>(pb); break;
+      case 2: vgr::project_backward_kernel<2><<<grid, kThreads, 0, stream>>>(pb); break;
+      default: vgr::project_backward_kernel<3><<<grid, kThreads, 0, stream>>>(pb); break;
     }
     if ((rc = vgr::check_launch("backward: projection")) != VGR_OK) return rc;
   }
   return VGR_OK;
+}
+
+extern "C" int vgr_photometric_loss(const float* rgb, const float* target_rgb, const float* depth,
+                                    const float* target_depth, int64_t pixels, double depth_weight,
+                                    float* loss, float* grad_rgb, float* grad_depth,
+                                    void* stream_ptr) {
+  if (!rgb || !target_rgb || !depth || !target_depth || !loss || !grad_rgb || !grad_depth) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "loss arguments must be non-null");
+  }
+  if (pixels <= 0) return fail(VGR_ERR_INVALID_ARGUMENT, "pixels must be positive");
+  if (!std::isfinite(depth_weight)) return fail(VGR_ERR_INVALID_ARGUMENT, "depth_weight must be finite");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  if (cudaMemsetAsync(loss, 0, sizeof(float), stream) != cudaSuccess) {
+    return vgr::check_launch("photometric loss: clear", 0);
+  }
+  int sms = 0;
+  int rc = vgr::device_sms(&sms);
+  if (rc != VGR_OK) return rc;
+  vgr::PhotometricLossParams p{};
+  p.rgb = rgb;
+  p.target_rgb = target_rgb;
+  p.depth = depth;
+  p.target_depth = target_depth;
+  p.pixels = pixels;
+  p.depth_weight = static_cast<float>(depth_weight);
+  p.loss = loss;
+  p.grad_rgb = grad_rgb;
+  p.grad_depth = grad_depth;
+  int64_t blocks = (pixels + 255) / 256;
+  if (blocks > static_cast<int64_t>(sms) * 8) blocks = static_cast<int64_t>(sms) * 8;
+  vgr::photometric_loss_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p);
+  return vgr::check_launch("photometric loss");
 }

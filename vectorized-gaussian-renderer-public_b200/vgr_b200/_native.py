@@ -208,6 +208,11 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
         ],
     ),
     (
+        "vgr_photometric_loss",
+        ctypes.c_int,
+        [_c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_double, _c_p, _c_p, _c_p, _c_p],
+    ),
+    (
         "vgr_render_backward",
         ctypes.c_int,
         [

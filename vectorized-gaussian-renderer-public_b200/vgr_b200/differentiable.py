@@ -49,6 +49,7 @@ class DifferentiableRenderer:
         gaussian_support_sigma: float = 3.33,
         covariance_epsilon: float = 0.3,
         headroom: float = 1.25,
+        capacity_check: str = "sync",
         device: torch.device | str | None = None,
     ) -> None:
         if height <= 0 or width <= 0:
@@ -57,6 +58,9 @@ class DifferentiableRenderer:
             raise ValueError("sh_degree must be -1 (linear RGB features) or in [0, 3]")
         if tile_size not in (4, 8, 16):
             raise ValueError("tile_size must be 4, 8 or 16")
+        if capacity_check not in ("sync", "deferred"):
+            raise ValueError("capacity_check must be 'sync' or 'deferred'")
+        self.capacity_check = capacity_check
         self.height = int(height)
         self.width = int(width)
         self.sh_degree = int(sh_degree)
@@ -74,6 +78,8 @@ class DifferentiableRenderer:
         self._frame = 0
         self._pending: dict[str, Any] | None = None
         self._key: tuple[Any, ...] | None = None
+        self._calibrated = False
+        self._host_counters: torch.Tensor | None = None
         self.last_counters: dict[str, int] = {}
 
     # ------------------------------------------------------------------ API
@@ -264,6 +270,7 @@ class DifferentiableRenderer:
         rgb = torch.empty((b, self.height, self.width, 3), dtype=torch.float32, device=device)
         depth = torch.empty((b, self.height, self.width, 1), dtype=torch.float32, device=device)
         alpha = torch.empty((b, self.height, self.width, 1), dtype=torch.float32, device=device)
+        counter_event = None
         for _attempt in range(8):
             scene, cams, outs, native_ws, options, state = self._structs(
                 means, features, viewmats, intrinsics, rgb, depth, alpha
@@ -273,9 +280,19 @@ class DifferentiableRenderer:
                 self._lib.vgr_render_train(scene, cams, outs, native_ws, options, state, stream, selector),
                 "render_train",
             )
+            if self.capacity_check == "deferred" and self._calibrated:
+                # Checked by the backward (or the next forward), which waits
+                # only for this forward, not for the work queued after it.
+                if self._host_counters is None:
+                    self._host_counters = torch.empty(5, dtype=torch.int64, pin_memory=True)
+                self._host_counters.copy_(self._ws["counters"], non_blocking=True)
+                counter_event = torch.cuda.Event()
+                counter_event.record(torch.cuda.current_stream(device))
+                break
             counters = self._ws["counters"].tolist()
             self.last_counters = {"visible_gaussians": counters[0], "tile_intersections": counters[1]}
             if counters[0] <= self._visible_capacity and counters[1] <= self._intersection_capacity:
+                self._calibrated = True
                 break
             self._visible_capacity = min(max(self._visible_capacity, int(counters[0] * self.headroom) + 1), _INT32_MAX)
             self._intersection_capacity = min(
@@ -291,8 +308,35 @@ class DifferentiableRenderer:
             "frame": self._frame,
             "tensors": (means, log_scales, rotations, opacity_logits, features, viewmats, intrinsics),
             "outputs": (rgb, depth, alpha),
+            "counter_event": counter_event,
         }
         return rgb, depth, alpha
+
+    def check_capacity(self) -> None:
+        """Deferred capacity check of the last forward: raises when it
+        overflowed (its outputs and gradients are invalid), after growing the
+        capacity so that rendering the frame again succeeds."""
+        pending = self._pending
+        event = pending.get("counter_event") if pending else None
+        if event is None:
+            return
+        event.synchronize()
+        pending["counter_event"] = None
+        counters = self._host_counters.tolist()
+        self.last_counters = {"visible_gaussians": counters[0], "tile_intersections": counters[1]}
+        if counters[0] <= self._visible_capacity and counters[1] <= self._intersection_capacity:
+            return
+        self._visible_capacity = min(max(self._visible_capacity, int(counters[0] * self.headroom) + 1), _INT32_MAX)
+        self._intersection_capacity = min(
+            max(self._intersection_capacity, int(counters[1] * self.headroom) + 1), _INT32_MAX
+        )
+        self._grow(self._pending["outputs"][0].device)
+        self._calibrated = False
+        raise RuntimeError(
+            f"frame {pending['frame']} overflowed the record or intersection capacity "
+            f"({counters[0]} records, {counters[1]} intersections); its outputs are invalid. "
+            "Capacity has been grown: render the frame again."
+        )
 
     # -------------------------------------------------------------- backward
     def backward_native(self, frame: int, grad_rgb, grad_depth, grad_alpha):
@@ -303,6 +347,7 @@ class DifferentiableRenderer:
                 "DifferentiableRenderer keeps one frame in flight: run the backward of a frame "
                 "before rendering the next one"
             )
+        self.check_capacity()
         means, log_scales, rotations, opacity_logits, features, viewmats, intrinsics = pending["tensors"]
         rgb, depth, alpha = pending["outputs"]
         device = means.device
@@ -360,3 +405,42 @@ class _RenderFunction(torch.autograd.Function):
     def backward(ctx, grad_rgb, grad_depth, grad_alpha):
         grads = ctx.renderer.backward_native(ctx.frame, grad_rgb, grad_depth, grad_alpha)
         return (None, *grads, None, None)
+
+
+class _PhotometricLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, rgb, depth, target_rgb, target_depth, depth_weight):
+        lib = _native.load_library()
+        rgb_c, depth_c = rgb.contiguous(), depth.contiguous()
+        t_rgb, t_depth = target_rgb.contiguous(), target_depth.contiguous()
+        pixels = depth_c.numel()
+        if rgb_c.numel() != 3 * pixels or t_rgb.shape != rgb_c.shape or t_depth.shape != depth_c.shape:
+            raise ValueError("rgb [...,3], depth [...,1] and their targets must match")
+        for t in (rgb_c, depth_c, t_rgb, t_depth):
+            if t.dtype != torch.float32 or t.device.type != "cuda":
+                raise ValueError("photometric_loss takes float32 CUDA tensors")
+        loss = torch.empty((), dtype=torch.float32, device=rgb.device)
+        grad_rgb = torch.empty_like(rgb_c)
+        grad_depth = torch.empty_like(depth_c)
+        stream = torch.cuda.current_stream(rgb.device).cuda_stream
+        _native.check(
+            lib.vgr_photometric_loss(rgb_c.data_ptr(), t_rgb.data_ptr(), depth_c.data_ptr(), t_depth.data_ptr(),
+                                     pixels, float(depth_weight), loss.data_ptr(), grad_rgb.data_ptr(),
+                                     grad_depth.data_ptr(), stream),
+            "photometric_loss",
+        )
+        ctx.save_for_backward(grad_rgb, grad_depth)
+        return loss
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        grad_rgb, grad_depth = ctx.saved_tensors
+        return grad_rgb * grad_loss, grad_depth * grad_loss, None, None, None
+
+
+def photometric_loss(rgb: torch.Tensor, depth: torch.Tensor, target_rgb: torch.Tensor,
+                     target_depth: torch.Tensor, depth_weight: float = 0.1) -> torch.Tensor:
+    """``mean((rgb - target_rgb)^2) + depth_weight * mean(|depth - target_depth|)``
+    (the depth term over pixels where both depths are finite, divided by the
+    pixel count), forward and gradient in one CUDA pass."""
+    return _PhotometricLoss.apply(rgb, depth, target_rgb, target_depth, depth_weight)
