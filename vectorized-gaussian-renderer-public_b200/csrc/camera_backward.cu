@@ -462,6 +462,12 @@ template <int kShDegree>
 __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kernel(ProjectBackwardParams p) {
   constexpr int kCount = kShDegree < 0 ? 1 : (kShDegree + 1) * (kShDegree + 1);
   constexpr int kFloats = kShDegree < 0 ? 3 : kCount * 3;
+  constexpr int kVec = (kFloats + 3) / 4;
+  constexpr int kPrefetch = 8;
+  // Colour-coefficient sums live in shared memory as float4s, thread-major
+  // (conflict-free): 48 accumulators in registers next to the coefficients
+  // would cap the kernel at two CTAs per SM.
+  __shared__ float4 s_dsh[kVec * kProjectBackwardThreads];
   const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (g >= p.gaussian_count) return;
 
@@ -481,28 +487,55 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
   const float s00 = p.covariances[g * 6 + 0], s01 = p.covariances[g * 6 + 1];
   const float s02 = p.covariances[g * 6 + 2], s11 = p.covariances[g * 6 + 3];
   const float s12 = p.covariances[g * 6 + 4], s22 = p.covariances[g * 6 + 5];
-  const float* coeffs = p.features + g * p.feature_width;
+  // The Gaussian's colour coefficients, loaded once.
+  float coef[kVec * 4];
+  {
+    const float* row = p.features + g * p.feature_width;
+    if (p.vector_feature_loads) {
+#pragma unroll
+      for (int i = 0; i < kVec; ++i) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(row) + i);
+        coef[4 * i + 0] = v.x;
+        coef[4 * i + 1] = v.y;
+        coef[4 * i + 2] = v.z;
+        coef[4 * i + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < kVec * 4; ++f) coef[f] = f < kFloats ? __ldg(row + f) : 0.0f;
+    }
+  }
 
   float dm[3] = {0.0f, 0.0f, 0.0f};
   float dcov[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
   float dop = 0.0f;
-  // Colour-coefficient sums live in shared memory (thread-major, so each
-  // access is conflict-free): 48 accumulators in registers would cap the
-  // kernel at two CTAs per SM.
-  __shared__ float s_dsh[kFloats * kProjectBackwardThreads];
-  float* dsh = s_dsh + threadIdx.x;
+  float4* dsh = s_dsh + threadIdx.x;
 #pragma unroll
-  for (int k = 0; k < kFloats; ++k) dsh[k * kProjectBackwardThreads] = 0.0f;
+  for (int i = 0; i < kVec; ++i) dsh[i * kProjectBackwardThreads] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 
   const CamPlan* plans = reinterpret_cast<const CamPlan*>(p.scratch + p.layout.plans);
   const CamConst* consts = reinterpret_cast<const CamConst*>(p.scratch + p.layout.cam_consts);
-  for (int64_t a = 0; a < p.active_count && scene >= 0; ++a) {
-    const CamPlan plan = plans[a];
-    if (plan.camera < 0 || plan.scene_slot != scene) continue;
-    const int64_t local = g - plan.g_begin;
-    if (local < 0 || local >= plan.g_count || local >= p.record_map_stride) continue;
-    const int32_t r = p.record_map[a * p.record_map_stride + local];
+  for (int64_t a0 = 0; a0 < p.active_count && scene >= 0; a0 += kPrefetch) {
+    // Record indices of up to kPrefetch cameras, all loads in flight at once.
+    int32_t rr[kPrefetch];
+#pragma unroll
+    for (int u = 0; u < kPrefetch; ++u) {
+      const int64_t a = a0 + u;
+      rr[u] = -1;
+      if (a < p.active_count) {
+        const CamPlan& plan = plans[a];
+        const int64_t local = g - plan.g_begin;
+        if (plan.camera >= 0 && plan.scene_slot == scene && local >= 0 && local < plan.g_count &&
+            local < p.record_map_stride) {
+          rr[u] = p.record_map[a * p.record_map_stride + local];
+        }
+      }
+    }
+#pragma unroll 1
+  for (int u = 0; u < kPrefetch; ++u) {
+    const int32_t r = rr[u];
     if (r < 0) continue;
+    const int64_t a = a0 + u;
     const float4 g0 = p.record_grads[static_cast<int64_t>(r) * 3 + 0];
     const float4 g1 = p.record_grads[static_cast<int64_t>(r) * 3 + 1];
     const float4 g2 = p.record_grads[static_cast<int64_t>(r) * 3 + 2];
@@ -596,9 +629,11 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
 
     // Colour.
     if (kShDegree < 0) {
-      dsh[0] += g2.x;
-      dsh[kProjectBackwardThreads] += g2.y;
-      dsh[2 * kProjectBackwardThreads] += g2.z;
+      float4 d = dsh[0];
+      d.x += g2.x;
+      d.y += g2.y;
+      d.z += g2.z;
+      dsh[0] = d;
     } else {
       const float dvx = ffma(R[6], pz, ffma(R[3], py, fmul(R[0], px)));
       const float dvy = ffma(R[7], pz, ffma(R[4], py, fmul(R[1], px)));
@@ -612,24 +647,29 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
       for (int k = 0; k < kCount; ++k) {
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
-          const float v = __ldg(coeffs + k * 3 + ch);
-          acc[ch] = k == 0 ? fmul(basis[0], v) : ffma(basis[k], v, acc[ch]);
+          acc[ch] = k == 0 ? fmul(basis[0], coef[ch]) : ffma(basis[k], coef[k * 3 + ch], acc[ch]);
         }
       }
       const float drgb[3] = {fadd(acc[0], 0.5f) > 0.0f ? g2.x : 0.0f,
                              fadd(acc[1], 0.5f) > 0.0f ? g2.y : 0.0f,
                              fadd(acc[2], 0.5f) > 0.0f ? g2.z : 0.0f};
-      float db[16];
 #pragma unroll
-      for (int k = 0; k < kCount; ++k) {
-        db[k] = 0.0f;
+      for (int i = 0; i < kVec; ++i) {
+        float4 d = dsh[i * kProjectBackwardThreads];
+        float* dv = reinterpret_cast<float*>(&d);
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-          dsh[(k * 3 + ch) * kProjectBackwardThreads] += basis[k] * drgb[ch];
-          db[k] += __ldg(coeffs + k * 3 + ch) * drgb[ch];
+        for (int q = 0; q < 4; ++q) {
+          const int f = 4 * i + q;
+          if (f < kFloats) dv[q] = fmaf(basis[f / 3], drgb[f % 3], dv[q]);
         }
+        dsh[i * kProjectBackwardThreads] = d;
       }
       if (kShDegree >= 1) {
+        float db[16];
+#pragma unroll
+        for (int k = 0; k < kCount; ++k) {
+          db[k] = coef[k * 3 + 0] * drgb[0] + coef[k * 3 + 1] * drgb[1] + coef[k * 3 + 2] * drgb[2];
+        }
         float dn[3];
         sh_direction_grad<kShDegree < 0 ? 0 : kShDegree>(x, y, z, db, dn);
         const float ndot = x * dn[0] + y * dn[1] + z * dn[2];
@@ -670,6 +710,7 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
     dcov[3] += gs[1][1];
     dcov[4] += gs[1][2] + gs[2][1];
     dcov[5] += gs[2][2];
+  }
   }
 
   // Activations.  Opacity: o = sigmoid(logit).
@@ -721,7 +762,14 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
   for (int k = 0; k < 3; ++k) p.d_means[g * 3 + k] = dm[k];
   float* dfeat = p.d_features + g * p.feature_width;
 #pragma unroll
-  for (int k = 0; k < kFloats; ++k) dfeat[k] = dsh[k * kProjectBackwardThreads];
+  for (int i = 0; i < kVec; ++i) {
+    const float4 d = dsh[i * kProjectBackwardThreads];
+    const float dv[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (4 * i + q < kFloats) dfeat[4 * i + q] = dv[q];
+    }
+  }
   for (int64_t k = kFloats; k < p.feature_width; ++k) dfeat[k] = 0.0f;
 }
 

@@ -251,6 +251,7 @@ struct ProjectBackwardParams {
   const float* opacities;       // forward activation output
   const float* features;
   int64_t feature_width;
+  bool vector_feature_loads;    // rows 16-byte aligned and a multiple of 4 floats
   const float* log_scales;
   const float* rotations;
   float cov_eps;

@@ -197,6 +197,8 @@ extern "C" int vgr_render_backward(const vgr_scene* scene, const vgr_train_param
     pb.opacities = scene->opacities;
     pb.features = scene->features;
     pb.feature_width = scene->feature_width;
+    pb.vector_feature_loads = (reinterpret_cast<uintptr_t>(scene->features) & 15) == 0 &&
+                              (scene->feature_width & 3) == 0;
     pb.log_scales = params->log_scales;
     pb.rotations = params->rotations;
     pb.cov_eps = static_cast<float>(opt->covariance_epsilon);
