@@ -61,7 +61,20 @@ typedef struct vgr_scene {
   int64_t scene_count;                 /* S */
   int64_t gaussian_count;              /* G */
   int64_t max_scene_gaussians;         /* max_s (offsets[s+1]-offsets[s]) */
+  /* Optional spatial layout (no counterpart in the reference; NULL = none).
+   * gaussian_ids: packed Gaussian g is reported as gaussian_ids[g] (records,
+   * depth-tie order, semantic_ids index), so a scene stored in another order
+   * (vgr_scene_spatial_order) renders exactly as the original.  chunk_bounds:
+   * per chunk of VGR_PROJECT_CHUNK consecutive Gaussians of a registered
+   * scene, (min x, min y, min z, max covariance trace, max x, max y, max z,
+   * 0) from vgr_scene_chunk_bounds; chunk_offsets[s] is scene s's first
+   * chunk.  A chunk outside a camera's frustum is then not projected. */
+  const int32_t* gaussian_ids;         /* [G] or NULL */
+  const float* chunk_bounds;           /* [C,8] or NULL */
+  const int64_t* chunk_offsets;        /* [S+1], required with chunk_bounds */
 } vgr_scene;
+/* Gaussians per projection chunk (the unit of vgr_scene.chunk_bounds). */
+#define VGR_PROJECT_CHUNK 512
 
 /* Camera batch.  The plain form leaves the four per-camera resolution arrays
  * NULL and renders every camera at (height,width) of vgr_render_options.
@@ -237,6 +250,19 @@ int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras
                               const vgr_render_options* options, void* stream,
                               int64_t* sorted_buffer_selector);
 
+/* Spatial layout of a scene (no counterpart in the reference).  Temp bytes
+ * of vgr_scene_spatial_order for a scene of gaussian_count Gaussians. */
+int64_t vgr_scene_spatial_order_temp_bytes(int64_t gaussian_count);
+/* order[i] = index of the i-th Gaussian in Morton order of the means (30-bit
+ * keys over the means' bounding box, stable).  Storing a scene in this order
+ * makes projection chunks spatially compact. */
+int vgr_scene_spatial_order(const float* means, int64_t gaussian_count, int32_t* order,
+                            void* temp, int64_t temp_bytes, void* stream);
+/* Bounds of each chunk of VGR_PROJECT_CHUNK consecutive Gaussians of one
+ * scene: bounds[c*8 .. c*8+7] = (min x, min y, min z, max covariance trace,
+ * max x, max y, max z, 0), ceil(gaussian_count / VGR_PROJECT_CHUNK) chunks. */
+int vgr_scene_chunk_bounds(const float* means, const float* covariances,
+                           int64_t gaussian_count, float* bounds, void* stream);
 /* ----------------------------------------------------- differentiable form */
 /* Training form of the camera path: the forward above plus hand-written
  * backward kernels for the compositor and the projection.  No counterpart in

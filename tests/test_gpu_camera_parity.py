@@ -254,3 +254,26 @@ def test_large_tile_grid_bitwise():
     assert cpu.tile_counts.size >= 4096
     _compare(gpu, cpu)
     assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
+
+
+def test_spatial_layout_renders_identically():
+    # Scenes stored in Morton order with per-chunk frustum culling render
+    # exactly what the scene in id order renders: cameras inside a large
+    # scene (so most chunks are outside each frustum), two scenes, ties by id.
+    scenes = [
+        (4, synthetic_scene(40_000, seed=91, mean_half_extent=6.0, log_scale_mean=-3.0, sh_degree=1)),
+        (6, synthetic_scene(9_000, seed=92, mean_half_extent=2.0, log_scale_mean=-3.5, sh_degree=1)),
+    ]
+    eyes = torch.tensor([[0.0, 0.5, 0.0], [3.0, 0.0, -2.0], [0.0, 0.0, 4.0], [0.5, 1.0, 0.5]])
+    targets = torch.tensor([[5.0, 0.0, 0.0], [3.0, 0.0, 5.0], [0.0, 0.0, 0.0], [-4.0, 0.0, 0.0]])
+    rig = CameraRig(look_at_viewmats(eyes, targets), pinhole(4, 70.0, 70.0, 48.0, 32.0), 64, 96)
+    ids = [4, 4, 6, 4]
+    with_layout = render_gpu(scenes, rig, ids, sh_degree=1, spatial_layout=True)
+    without = render_gpu(scenes, rig, ids, sh_degree=1, spatial_layout=False)
+    assert "chunk_bounds" in with_layout.backend._packed_scene
+    for name in ("rgb", "depth", "alpha", "semantic_id"):
+        assert torch.equal(with_layout.outputs[name], without.outputs[name]), name
+    assert with_layout.counters == without.counters
+    assert_bitwise_equal(_sorted_gids(with_layout), _sorted_gids(without), "sorted gaussian ids")
+    cpu = render_oracle(scenes, rig, ids, sh_degree=1)
+    _compare(with_layout, cpu)

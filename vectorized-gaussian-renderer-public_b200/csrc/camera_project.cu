@@ -344,6 +344,63 @@ __device__ __forceinline__ uint32_t footprint_box(float opacity, float a, float 
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
+// True when no Gaussian of a chunk can pass the early off-screen cull of
+// project_gaussian for this camera, so the chunk need not be projected.
+// With p = R m + t (camera space), the early cull rejects a Gaussian when
+// pz is outside [near, far] or u + bx <= 0 (and likewise for the other three
+// image sides), bx = 1.01 sigma sqrt((fx/pz)^2 (1 + L^2) tr + eps) + 2 with
+// tr <= T (the chunk's largest trace times r_scale2).  Since
+// sqrt(a + b) <= sqrt(a) + sqrt(b), pz bx / fx <= K + pz m with
+// K = 1.01 sigma sqrt((1 + L^2) T) and m = (1.01 sigma sqrt(eps) + 2) / fx,
+// and u + bx = (fx / pz)(px + pz cx / fx + pz bx / fx), a Gaussian with
+// pz >= near is rejected on the left side whenever
+// px + pz (cx / fx + m) + K <= 0: a linear bound in p, whose maximum over
+// the chunk's box of means is the value at the centre plus sum |(R^T a)_i|
+// h_i.  Every comparison has a relative slack of 1e-4 for rounding, and a
+// non-finite bound culls nothing.
+__device__ __forceinline__ bool chunk_outside_frustum(const CamConst& c, float4 b0, float4 b1,
+                                                      float near_plane, float far_plane,
+                                                      float sigma, float eps) {
+  if (!(c.fx > 0.0f && c.fy > 0.0f)) return false;
+  const float hx = 0.5f * (b1.x - b0.x), hy = 0.5f * (b1.y - b0.y), hz = 0.5f * (b1.z - b0.z);
+  const float mx = 0.5f * (b0.x + b1.x), my = 0.5f * (b0.y + b1.y), mz = 0.5f * (b0.z + b1.z);
+  const float* R = c.r;
+  const float pcx = R[0] * mx + R[1] * my + R[2] * mz + c.t[0];
+  const float pcy = R[3] * mx + R[4] * my + R[5] * mz + c.t[1];
+  const float pcz = R[6] * mx + R[7] * my + R[8] * mz + c.t[2];
+  // sum_i |(R^T a)_i| h_i for the functional a . p.
+  auto extent = [&](float a0, float a1, float a2) {
+    return fabsf(a0 * R[0] + a1 * R[3] + a2 * R[6]) * hx + fabsf(a0 * R[1] + a1 * R[4] + a2 * R[7]) * hy +
+           fabsf(a0 * R[2] + a1 * R[5] + a2 * R[8]) * hz;
+  };
+  const float ez = extent(0.0f, 0.0f, 1.0f);
+  const float sz = 1.0e-4f * (fabsf(pcz) + ez) + 1.0e-6f;
+  if (pcz + ez < near_plane - sz) return true;
+  if (pcz - ez > far_plane + sz) return true;
+  const float t2 = b0.w * c.r_scale2;
+  const float lx = fmaxf(c.lim_xp, c.lim_xn), ly = fmaxf(c.lim_yp, c.lim_yn);
+  const float kx = 1.01f * sigma * sqrtf((1.0f + lx * lx) * t2) * 1.001f;
+  const float ky = 1.01f * sigma * sqrtf((1.0f + ly * ly) * t2) * 1.001f;
+  const float m_x = (1.01f * sigma * sqrtf(eps) + 2.0f) / c.fx * 1.001f;
+  const float m_y = (1.01f * sigma * sqrtf(eps) + 2.0f) / c.fy * 1.001f;
+  // Side planes: low side needs a.p + k > 0 somewhere, high side a.p - k < 0.
+  auto low_out = [&](float pc, float az, float ex, float k) {
+    const float v = pc + az * pcz + ex + k;
+    return v < -(1.0e-4f * (fabsf(pc) + fabsf(az * pcz) + ex + k) + 1.0e-6f);
+  };
+  auto high_out = [&](float pc, float az, float ex, float k) {
+    const float v = pc - az * pcz - ex - k;
+    return v > 1.0e-4f * (fabsf(pc) + fabsf(az * pcz) + ex + k) + 1.0e-6f;
+  };
+  const float ax_lo = c.cx / c.fx + m_x, ax_hi = (c.width - c.cx) / c.fx + m_x;
+  const float ay_lo = c.cy / c.fy + m_y, ay_hi = (c.height - c.cy) / c.fy + m_y;
+  if (low_out(pcx, ax_lo, extent(1.0f, 0.0f, ax_lo), kx)) return true;
+  if (high_out(pcx, ax_hi, extent(1.0f, 0.0f, -ax_hi), kx)) return true;
+  if (low_out(pcy, ay_lo, extent(0.0f, 1.0f, ay_lo), ky)) return true;
+  if (high_out(pcy, ay_hi, extent(0.0f, 1.0f, -ay_hi), ky)) return true;
+  return false;
+}
+
 template <int kShDegree>
 __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
@@ -354,9 +411,11 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   __shared__ int32_t s_radii[kProjectChunk * 2];
   __shared__ uint32_t s_warp_vis[kProjectRounds][kProjectThreads / 32];
   __shared__ uint64_t s_warp_isect[kProjectRounds][kProjectThreads / 32];
-  __shared__ CamConst s_cam;
-  __shared__ __align__(8) CamPlan s_plan;
-  __shared__ int64_t s_vblock;
+  __shared__ CamConst s_cams[kTicketBatch];
+  __shared__ __align__(8) CamPlan s_plans[kTicketBatch];
+  __shared__ int64_t s_vbs[kTicketBatch];
+  __shared__ int s_nlive;
+  __shared__ int s_exhausted;
   __shared__ uint64_t s_base_vis, s_base_isect;
   __shared__ uint32_t s_nvis;
   __shared__ uint32_t s_nisect;
@@ -369,38 +428,68 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   const int warp = tid >> 5;
 
   const int64_t total_vblocks = p.total_vblocks;
+  int cursor = 0;
+  int nlive = 0;
   while (true) {
-    // Warp 0 takes the ticket and stages the slot's plan (7 words) and
-    // projection constants (14 words) with one load per lane.
-    if (warp == 0) {
-      int64_t ticket = 0;
-      if (lane == 0) ticket = atomicAdd(&header->project_queue, 1u);
-      ticket = __shfl_sync(0xffffffffu, ticket, 0);
-      if (ticket < total_vblocks) {
-        const int64_t slot = ticket % p.active_count;
-        if (lane < 7) {
-          reinterpret_cast<uint64_t*>(&s_plan)[lane] =
-              reinterpret_cast<const uint64_t*>(plans + slot)[lane];
-        } else if (lane < 21) {
-          reinterpret_cast<uint64_t*>(&s_cam)[lane - 7] =
-              reinterpret_cast<const uint64_t*>(cam_consts + slot)[lane - 7];
+    if (cursor == nlive) {
+      // Warp 0 takes kTicketBatch consecutive virtual blocks; each lane
+      // stages one (plan, projection constants) and drops it when it adds
+      // nothing (an invalid camera, a chunk past its camera's scene, a chunk
+      // outside the frustum); the rest are compacted into shared memory.
+      // The previous vblock ended with a barrier, so the arrays are free.
+      if (warp == 0) {
+        int64_t base = 0;
+        if (lane == 0) base = atomicAdd(&header->project_queue, static_cast<uint32_t>(kTicketBatch));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const int64_t vb = base + lane;
+        bool live = vb < total_vblocks;
+        const int64_t slot = live ? vb % p.active_count : 0;
+        if (live) {
+          const int64_t chunk = vb / p.active_count;
+          const CamPlan& plan = plans[slot];
+          const int scene_slot = plan.scene_slot;
+          live = plan.camera >= 0 && scene_slot >= 0 && chunk * kProjectChunk < plan.g_count;
+          if (live && p.chunk_bounds) {
+            const int64_t ci = p.chunk_offsets[scene_slot] + chunk;
+            live = !chunk_outside_frustum(cam_consts[slot], p.chunk_bounds[ci * 2],
+                                          p.chunk_bounds[ci * 2 + 1], p.near_plane, p.far_plane,
+                                          p.support_sigma, p.cov_eps);
+          }
+        }
+        const uint32_t mask = __ballot_sync(0xffffffffu, live);
+        if (live) {
+          const int rank = __popc(mask & ((1u << lane) - 1u));
+#pragma unroll
+          for (int w = 0; w < 7; ++w) {
+            reinterpret_cast<uint64_t*>(&s_plans[rank])[w] =
+                reinterpret_cast<const uint64_t*>(plans + slot)[w];
+          }
+#pragma unroll
+          for (int w = 0; w < 7; ++w) {
+            reinterpret_cast<float4*>(&s_cams[rank])[w] = reinterpret_cast<const float4*>(cam_consts + slot)[w];
+          }
+          s_vbs[rank] = vb;
+        }
+        if (lane == 0) {
+          s_nlive = __popc(mask);
+          s_exhausted = base + kTicketBatch >= total_vblocks;
         }
       }
-      if (lane == 0) s_vblock = ticket;
-    }
-    __syncthreads();
-    const int64_t b = s_vblock;
-    if (b >= total_vblocks) break;
-    const int64_t chunk = b / p.active_count;
-    const CamPlan plan = s_plan;
-    const int64_t local_begin = chunk * kProjectChunk;
-    const bool live = plan.camera >= 0 && plan.scene_slot >= 0 && local_begin < plan.g_count;
-    if (!live) {
-      // A virtual block past its camera's scene (ragged scene sizes) or of an
-      // invalid camera adds nothing.
       __syncthreads();
-      continue;
+      nlive = s_nlive;
+      cursor = 0;
+      if (nlive == 0) {
+        if (s_exhausted) break;
+        continue;
+      }
     }
+    const int64_t b = s_vbs[cursor];
+    const CamPlan plan = s_plans[cursor];
+    const CamConst& s_cam = s_cams[cursor];
+    ++cursor;
+    const int64_t chunk = b / p.active_count;
+    const int64_t local_begin = chunk * kProjectChunk;
+    const bool live = true;
 
     // Project both rounds first (no barrier), then one block scan of
     // (visible, tiles) over the kProjectChunk tasks in task order.
@@ -452,8 +541,8 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           // Staged by task slot; the scan below maps ranks to slots.
           Record& staged = s_rec[round * kProjectThreads + tid];
           staged.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
-          staged.b =
-              make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(static_cast<int>(g)));
+          const int32_t id = p.gaussian_ids ? p.gaussian_ids[g] : static_cast<int32_t>(g);
+          staged.b = make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(id));
           staged.c = make_float4(
               rgb[0], rgb[1], rgb[2],
               __uint_as_float(footprint_box(pr.opacity, pr.cov_a, pr.cov_b, pr.cov_c)));
@@ -549,7 +638,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         int32_t* map_row = p.record_map + (b % p.active_count) * p.record_map_stride;
         for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
           const uint64_t r = base_vis + i;
-          const int64_t local = __float_as_int(s_rec[s_slot[i]].b.w) - plan.g_begin;
+          const int64_t local = local_begin + s_slot[i];
           if (r < vcap) map_row[local] = static_cast<int32_t>(r);
         }
       }

@@ -113,14 +113,6 @@ AccelLayout make_accel_layout(int64_t count, int packet) {
   return l;
 }
 
-__device__ __forceinline__ uint32_t float_order(float f) {
-  const uint32_t u = __float_as_uint(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float order_float(uint32_t u) {
-  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 __device__ __forceinline__ void quaternion_axes(const float* q, float3 axes[3]) {
   const float w = q[0], x = q[1], y = q[2], z = q[3];
   axes[0] = make_float3(1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y + z * w), 2.0f * (x * z - y * w));
@@ -144,15 +136,6 @@ __device__ __forceinline__ bool planar_axes(const float* scales, float planarity
   *t1 = b;
   const float tangent_min = fminf(scales[a], scales[b]);
   return scales[n] > 0.0f && !(scales[n] / tangent_min > planarity);
-}
-
-__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
-  v &= 0x000003ffu;
-  v = (v | (v << 16)) & 0x030000ffu;
-  v = (v | (v << 8)) & 0x0300f00fu;
-  v = (v | (v << 4)) & 0x030c30c3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
 }
 
 // ---------------------------------------------------------------- build

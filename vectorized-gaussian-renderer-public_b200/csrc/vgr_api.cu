@@ -32,6 +32,8 @@ thread_local OccupancyCache g_occ;
 
 }  // namespace
 
+static_assert(vgr::kProjectChunk == VGR_PROJECT_CHUNK, "projection chunk of the C ABI");
+
 namespace vgr {
 
 int fail(int code, const char* fmt, ...) {
@@ -331,7 +333,9 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   }
 
   const int64_t vblocks = render_vblocks(active, scene->max_scene_gaussians);
-  if (vblocks >= static_cast<int64_t>(UINT32_MAX)) {
+  // The 32-bit ticket queue runs past the last virtual block by at most one
+  // batch per resident CTA.
+  if (vblocks >= static_cast<int64_t>(UINT32_MAX) - (int64_t{1} << 24)) {
     return fail(VGR_ERR_INVALID_ARGUMENT,
                 "active cameras x max_scene_gaussians exceeds 2^41 projection tasks");
   }
@@ -437,6 +441,14 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     pp.mirror_radii = ws->visible_radii;
     pp.record_map = train ? train->record_map : nullptr;
     pp.record_map_stride = scene->max_scene_gaussians;
+    pp.gaussian_ids = scene->gaussian_ids;
+    pp.chunk_bounds = reinterpret_cast<const float4*>(scene->chunk_bounds);
+    pp.chunk_offsets = scene->chunk_offsets;
+    if (scene->chunk_bounds &&
+        (!scene->chunk_offsets || (reinterpret_cast<uintptr_t>(scene->chunk_bounds) & 15) != 0)) {
+      return fail(VGR_ERR_INVALID_ARGUMENT,
+                  "chunk_bounds must be 16-byte aligned and come with chunk_offsets");
+    }
     if (pp.mirror_means2d && !(pp.mirror_conics && pp.mirror_depths && pp.mirror_opacities &&
                                pp.mirror_camera_ids && pp.mirror_gaussian_ids && pp.mirror_radii)) {
       return fail(VGR_ERR_INVALID_ARGUMENT, "the visible-record mirrors must be all set or all null");

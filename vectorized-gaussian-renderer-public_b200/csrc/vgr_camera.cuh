@@ -157,6 +157,7 @@ static_assert(sizeof(ScratchHeader) == 128, "ScratchHeader layout");
 constexpr int kProjectThreads = 256;
 constexpr int kProjectRounds = 2;
 constexpr int kProjectChunk = kProjectThreads * kProjectRounds;  // tasks per virtual block
+constexpr int kTicketBatch = 32;  // virtual blocks taken per queue ticket (one per lane)
 
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;

@@ -129,4 +129,25 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr int kDeviceErrorLookback = 1;
 
+// Order-preserving map of a float to uint32 (unsigned comparison of the
+// codes orders the floats) and its inverse.
+__device__ __forceinline__ uint32_t float_order(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Spreads the low 10 bits of v to every third bit (one axis of a 30-bit
+// Morton code).
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+  v &= 0x000003ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
 }  // namespace vgr

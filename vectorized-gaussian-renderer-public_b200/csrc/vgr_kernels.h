@@ -68,6 +68,9 @@ struct ProjectParams {
   int32_t* mirror_radii;
   int32_t* record_map;         // training: [A, record_map_stride] record of (slot, local Gaussian)
   int64_t record_map_stride;
+  const int32_t* gaussian_ids; // reported id of packed Gaussian g, or null (g itself)
+  const float4* chunk_bounds;  // [C,2] per-chunk bounds, or null (no chunk culling)
+  const int64_t* chunk_offsets;// [S+1] first chunk of each registered scene
 };
 
 struct SortParams {

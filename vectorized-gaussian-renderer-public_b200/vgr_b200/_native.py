@@ -20,6 +20,7 @@ VGR_ERR_CUDA = -2
 VGR_ERR_SCRATCH_TOO_SMALL = -3
 VGR_ERR_UNSUPPORTED = -4
 RECORD_BYTES = 48
+PROJECT_CHUNK = 512
 STAGE_EVENTS = 7
 
 _c_i64 = ctypes.c_int64
@@ -40,6 +41,9 @@ class VgrScene(ctypes.Structure):
         ("scene_count", _c_i64),
         ("gaussian_count", _c_i64),
         ("max_scene_gaussians", _c_i64),
+        ("gaussian_ids", _c_p),
+        ("chunk_bounds", _c_p),
+        ("chunk_offsets", _c_p),
     ]
 
 
@@ -188,6 +192,9 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
             ctypes.POINTER(_c_i64),
         ],
     ),
+    ("vgr_scene_spatial_order_temp_bytes", _c_i64, [_c_i64]),
+    ("vgr_scene_spatial_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
+    ("vgr_scene_chunk_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
     (
         "vgr_train_activate",
         ctypes.c_int,

@@ -121,6 +121,7 @@ class CustomCudaBackend:
         allow_cpu_for_tests: bool = False,
         sh_degree: int | None = None,
         mirror_reference_workspace: bool = False,
+        spatial_layout: bool = True,
     ) -> None:
         if max_visible_records is not None and max_visible_records <= 0:
             raise ValueError("max_visible_records must be positive.")
@@ -223,6 +224,11 @@ class CustomCudaBackend:
         self.max_workspace_bytes = max_workspace_bytes
         self.sh_degree = sh_degree
         self.mirror_reference_workspace = mirror_reference_workspace
+        # Store registered scenes in Morton order of their means with
+        # per-chunk bounds, so that projection skips chunks outside a
+        # camera's frustum; every output is unchanged (Gaussians keep their
+        # ids).  No counterpart in the reference.
+        self.spatial_layout = spatial_layout
         self._native = native_module
         self._native_loader = native_loader
         self.allow_cpu_for_tests = allow_cpu_for_tests
@@ -593,19 +599,7 @@ class CustomCudaBackend:
         lib = _native.load_library()
         ws = self.workspace
         packed = self._packed_scene
-        scene = _native.VgrScene(
-            means=packed["means"].data_ptr(),
-            covariances=packed["covariances"].data_ptr(),
-            opacities=packed["opacities"].data_ptr(),
-            features=packed["features"].data_ptr(),
-            feature_width=packed["features"].shape[1],
-            semantic_ids=packed["semantic_ids"].data_ptr(),
-            registered_scene_ids=packed["registered_scene_ids"].data_ptr(),
-            scene_offsets=packed["scene_offsets"].data_ptr(),
-            scene_count=packed["registered_scene_ids"].numel(),
-            gaussian_count=packed["means"].shape[0],
-            max_scene_gaussians=self._max_scene_gaussians,
-        )
+        scene = self.native_scene()
         # An empty active-id tensor means "every camera", as at the reference's
         # native boundary (renderer_cuda.cu:2626-2628).
         use_active = active is not None and active.numel() > 0
@@ -683,6 +677,27 @@ class CustomCudaBackend:
             # the dictionary entries rather than copying.
             ws["keys_in"], ws["keys_out"] = ws["keys_out"], ws["keys_in"]
             ws["values_in"], ws["values_out"] = ws["values_out"], ws["values_in"]
+
+    def native_scene(self) -> _native.VgrScene:
+        """The packed scene as the C ABI's vgr_scene (with the spatial
+        layout when it is on)."""
+        packed = self._packed_scene
+        return _native.VgrScene(
+            means=packed["means"].data_ptr(),
+            covariances=packed["covariances"].data_ptr(),
+            opacities=packed["opacities"].data_ptr(),
+            features=packed["features"].data_ptr(),
+            feature_width=packed["features"].shape[1],
+            semantic_ids=packed["semantic_ids"].data_ptr(),
+            registered_scene_ids=packed["registered_scene_ids"].data_ptr(),
+            scene_offsets=packed["scene_offsets"].data_ptr(),
+            scene_count=packed["registered_scene_ids"].numel(),
+            gaussian_count=packed["means"].shape[0],
+            max_scene_gaussians=self._max_scene_gaussians,
+            gaussian_ids=packed["gaussian_ids"].data_ptr() if "gaussian_ids" in packed else None,
+            chunk_bounds=packed["chunk_bounds"].data_ptr() if "chunk_bounds" in packed else None,
+            chunk_offsets=packed["chunk_offsets"].data_ptr() if "chunk_offsets" in packed else None,
+        )
 
     def set_stage_events(self, events: list[torch.cuda.Event] | None) -> None:
         """Record ``events[i]`` at stage boundary i of every native render
@@ -1170,19 +1185,72 @@ class CustomCudaBackend:
             self._allocated_intersection_capacity,
         )
 
+    def _spatial_orders(self, scenes: list[GaussianScene]) -> list[torch.Tensor]:
+        """Morton order of each scene's means (vgr_scene_spatial_order)."""
+        lib = _native.load_library()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        orders = []
+        for scene in scenes:
+            count = scene.count
+            temp = torch.empty(
+                _native.check_size(lib.vgr_scene_spatial_order_temp_bytes(count), "spatial order"),
+                dtype=torch.uint8, device=self.device,
+            )
+            order = torch.empty(count, dtype=torch.int32, device=self.device)
+            means = scene.means.contiguous()
+            _native.check(
+                lib.vgr_scene_spatial_order(means.data_ptr(), count, order.data_ptr(), temp.data_ptr(),
+                                            temp.numel(), stream),
+                "spatial order",
+            )
+            orders.append(order.long())
+        return orders
+
     def _rebuild_packed_scene(self) -> None:
         assert self.device is not None
         scenes = list(self._scenes.values())
         packed: dict[str, torch.Tensor] = {}
+        layout = (
+            self.spatial_layout
+            and self.device.type == "cuda"
+            and all(scene.count > 0 for scene in scenes)
+        )
+        orders = self._spatial_orders(scenes) if layout else None
         for name in ("means", "scales", "rotations", "opacities", "features", "semantic_ids"):
             tensors = [getattr(scene, name) for scene in scenes]
+            if orders is not None and name != "semantic_ids":
+                # The semantic table stays in id order (it is indexed by id).
+                tensors = [t.index_select(0, order) for t, order in zip(tensors, orders)]
             packed[name] = tensors[0] if len(tensors) == 1 else torch.cat(tensors, dim=0).contiguous()
+            packed[name] = packed[name].contiguous()
         covariances = torch.empty((packed["scales"].shape[0], 6), device=self.device, dtype=torch.float32)
         self._native.precompute_covariances(packed["scales"], packed["rotations"], covariances)
         packed["covariances"] = covariances
         offsets = [0]
         for scene in scenes:
             offsets.append(offsets[-1] + scene.count)
+        if orders is not None:
+            lib = _native.load_library()
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            packed["gaussian_ids"] = torch.cat(
+                [order + off for order, off in zip(orders, offsets[:-1])]
+            ).to(torch.int32).contiguous()
+            chunk = _native.PROJECT_CHUNK
+            chunk_offsets = [0]
+            for scene in scenes:
+                chunk_offsets.append(chunk_offsets[-1] + (scene.count + chunk - 1) // chunk)
+            bounds = torch.empty((chunk_offsets[-1], 8), dtype=torch.float32, device=self.device)
+            for s, scene in enumerate(scenes):
+                off = offsets[s]
+                _native.check(
+                    lib.vgr_scene_chunk_bounds(
+                        packed["means"][off:].data_ptr(), covariances[off:].data_ptr(), scene.count,
+                        bounds[chunk_offsets[s]:].data_ptr(), stream,
+                    ),
+                    "chunk bounds",
+                )
+            packed["chunk_bounds"] = bounds
+            packed["chunk_offsets"] = torch.tensor(chunk_offsets, device=self.device, dtype=torch.int64)
         packed["registered_scene_ids"] = torch.tensor(list(self._scenes), device=self.device, dtype=torch.int64)
         packed["scene_offsets"] = torch.tensor(offsets, device=self.device, dtype=torch.int64)
         self._packed_scene = packed

@@ -173,20 +173,7 @@ class RaggedBatch:
         b = self.backend
         lib = _native.load_library()
         ws = self.workspace
-        packed = b._packed_scene
-        scene = _native.VgrScene(
-            means=packed["means"].data_ptr(),
-            covariances=packed["covariances"].data_ptr(),
-            opacities=packed["opacities"].data_ptr(),
-            features=packed["features"].data_ptr(),
-            feature_width=packed["features"].shape[1],
-            semantic_ids=packed["semantic_ids"].data_ptr(),
-            registered_scene_ids=packed["registered_scene_ids"].data_ptr(),
-            scene_offsets=packed["scene_offsets"].data_ptr(),
-            scene_count=packed["registered_scene_ids"].numel(),
-            gaussian_count=packed["means"].shape[0],
-            max_scene_gaussians=b._max_scene_gaussians,
-        )
+        scene = b.native_scene()
         cams = _native.VgrCameras(
             viewmats=viewmats.data_ptr(),
             intrinsics=intrinsics.data_ptr(),
