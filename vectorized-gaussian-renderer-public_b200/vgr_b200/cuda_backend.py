@@ -1186,11 +1186,21 @@ class CustomCudaBackend:
         )
 
     def _spatial_orders(self, scenes: list[GaussianScene]) -> list[torch.Tensor]:
-        """Morton order of each scene's means (vgr_scene_spatial_order)."""
+        """Morton order of each scene's means (vgr_scene_spatial_order),
+        computed once per registered scene tensor (a registration repacks
+        every scene, so the orders of the others are reused)."""
         lib = _native.load_library()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         orders = []
+        cache = getattr(self, "_order_cache", {})
+        fresh = {}
         for scene in scenes:
+            token = (scene.means.data_ptr(), scene.means._version, scene.count)
+            cached = cache.get(token)
+            if cached is not None:
+                orders.append(cached)
+                fresh[token] = cached
+                continue
             count = scene.count
             temp = torch.empty(
                 _native.check_size(lib.vgr_scene_spatial_order_temp_bytes(count), "spatial order"),
@@ -1204,6 +1214,8 @@ class CustomCudaBackend:
                 "spatial order",
             )
             orders.append(order.long())
+            fresh[token] = orders[-1]
+        self._order_cache = fresh
         return orders
 
     def _rebuild_packed_scene(self) -> None:

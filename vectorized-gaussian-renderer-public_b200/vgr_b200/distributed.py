@@ -1,0 +1,90 @@
+"""Multi-GPU plumbing of the camera, LiDAR and differentiable paths.
+
+One process per GPU (torchrun), ``torch.distributed`` over NCCL (gloo on CPU
+for tests).  Cameras and LiDAR sensors are independent units: a batch is
+split into contiguous per-rank shards and rendered against a replica of the
+scene with no exchange on the data path.  The differentiable form trains one
+scene data-parallel over cameras, so its only exchange is the sum of the
+scene-parameter gradients across ranks once per step (SURVEY's multi-GPU
+plan: one all-reduce of ~118 MB for 500k SH3 Gaussians), done here in a few
+large coalesced buckets.  Timings are taken on each rank with CUDA events and
+reduced with a MAX over ranks.
+"""
+
+from __future__ import annotations
+
+from typing import Sequence
+
+import torch
+
+
+def camera_shard(batch: int, world: int, rank: int) -> slice:
+    """Contiguous, balanced shard [start, stop) of ``batch`` units for ``rank``
+    (the first ``batch % world`` ranks take one extra unit)."""
+    if world <= 0 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    if batch < 0:
+        raise ValueError("batch must be non-negative")
+    base, extra = divmod(batch, world)
+    start = rank * base + min(rank, extra)
+    return slice(start, start + base + (1 if rank < extra else 0))
+
+
+def max_over_ranks(value: float, *, device: torch.device | str | None = None, group=None) -> float:
+    """MAX of a per-rank scalar (e.g. a CUDA-event time) over the group."""
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def allreduce_gradients(
+    tensors: Sequence[torch.Tensor],
+    *,
+    average: bool = True,
+    group=None,
+    bucket_bytes: int = 64 << 20,
+) -> None:
+    """Sum (or average) the given gradient tensors over the group in place.
+
+    Tensors of one dtype and device are packed into flat buckets of at most
+    ``bucket_bytes`` so that a few large collectives replace one per tensor;
+    each bucket is reduced with one all_reduce and copied back."""
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return
+    world = dist.get_world_size(group)
+    if world == 1:
+        return
+    pending: list[torch.Tensor] = []
+    size = 0
+
+    def flush() -> None:
+        nonlocal pending, size
+        if not pending:
+            return
+        flat = torch.cat([t.reshape(-1) for t in pending])
+        dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+        if average:
+            flat.div_(world)
+        offset = 0
+        for t in pending:
+            n = t.numel()
+            t.copy_(flat[offset: offset + n].view_as(t))
+            offset += n
+        pending = []
+        size = 0
+
+    for t in tensors:
+        if t is None:
+            continue
+        nbytes = t.numel() * t.element_size()
+        if pending and (size + nbytes > bucket_bytes or pending[0].dtype != t.dtype or pending[0].device != t.device):
+            flush()
+        pending.append(t)
+        size += nbytes
+    flush()

@@ -306,7 +306,7 @@ class TrainingWorkload:
 
 
 def training_workload(gaussians: int = 500_000, cameras: int = 16, size: int = 512, *,
-                      seed: int = 13) -> TrainingWorkload:
+                      seed: int = 13, camera_seed: int | None = None) -> TrainingWorkload:
     """Differentiable-form workload: a 500k-Gaussian SH3 scene (the batched
     scene's laws) as raw parameters, 16 orbit cameras of 512x512 (focal 420),
     and a target scene = means + N(0, 0.01), SH coefficients + N(0, 0.05)."""
@@ -322,5 +322,6 @@ def training_workload(gaussians: int = 500_000, cameras: int = 16, size: int = 5
     targets = dict(params)
     targets["means"] = (params["means"] + torch.randn(params["means"].shape, generator=gen) * 0.01).contiguous()
     targets["features"] = (params["features"] + torch.randn(params["features"].shape, generator=gen) * 0.05).contiguous()
-    rig = orbit_cameras(cameras, seed=seed + 2, width=size, height=size, focal=420.0)
+    rig = orbit_cameras(cameras, seed=seed + 2 if camera_seed is None else camera_seed,
+                        width=size, height=size, focal=420.0)
     return TrainingWorkload(params=params, targets=targets, rig=rig)
