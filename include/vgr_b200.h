@@ -263,6 +263,56 @@ int vgr_scene_spatial_order(const float* means, int64_t gaussian_count, int32_t*
  * max x, max y, max z, 0), ceil(gaussian_count / VGR_PROJECT_CHUNK) chunks. */
 int vgr_scene_chunk_bounds(const float* means, const float* covariances,
                            int64_t gaussian_count, float* bounds, void* stream);
+/* ---------------------------------------------------------------- ingestion */
+/* Scalar types of PLY properties (PLY names: char uchar short ushort int uint
+ * float double, and int64 for a semantic_id written by 64-bit tools). */
+#define VGR_PLY_INT8 0
+#define VGR_PLY_UINT8 1
+#define VGR_PLY_INT16 2
+#define VGR_PLY_UINT16 3
+#define VGR_PLY_INT32 4
+#define VGR_PLY_UINT32 5
+#define VGR_PLY_INT64 6
+#define VGR_PLY_FLOAT32 7
+#define VGR_PLY_FLOAT64 8
+/* Property roles (index into vgr_ply_layout.offsets/types). */
+#define VGR_PLY_X 0
+#define VGR_PLY_SCALE0 3
+#define VGR_PLY_ROT0 6
+#define VGR_PLY_OPACITY 10
+#define VGR_PLY_DC0 11
+#define VGR_PLY_SEMANTIC 14
+#define VGR_PLY_REST0 15
+#define VGR_PLY_MAX_PROPERTIES 64
+/* Byte layout of one packed vertex row of an INRIA 3DGS PLY body: x y z,
+ * scale_0..2, rot_0..3 (WXYZ), opacity, f_dc_0..2, semantic_id (optional),
+ * then f_rest_0..f_rest_{rest_count-1}. */
+typedef struct vgr_ply_layout {
+  int64_t row_bytes;
+  int32_t offsets[VGR_PLY_MAX_PROPERTIES];
+  int32_t types[VGR_PLY_MAX_PROPERTIES];
+  int32_t rest_count;  /* multiple of 3 */
+  int32_t has_semantic;
+} vgr_ply_layout;
+/* Replaces load_ply_to_gaussians + canonicalize_3dgs_scene
+ * (ply_loader.py:52-135) after the host has read the header and copied the
+ * vertex rows to the device: means [G,3], scales = exp [G,3], rotations =
+ * q / |q| (identity when |q| <= float32 eps) [G,4], opacities = sigmoid [G],
+ * features [G,F] = (clamp(0.5 + SH_C0 dc, 0, 1), f_rest coefficient-major,
+ * zero padding), semantic_ids [G] (0 without a semantic_id property). */
+int vgr_ply_canonicalize(const void* vertex_rows, int64_t count, const vgr_ply_layout* layout,
+                         float* means, float* scales, float* rotations, float* opacities,
+                         float* features, int64_t feature_width, int64_t* semantic_ids,
+                         void* stream);
+/* Replaces the Warp kernel fabric_world_to_opencv_viewmats
+ * (fabric_camera_kernels.py:8-49): USD row-vector world matrices [N,4,4]
+ * float64 -> OpenCV world->camera view matrices, camera i written to row
+ * camera_indices[i] (or i when NULL) of viewmats [viewmat_count,4,4];
+ * out-of-range indices are skipped and counted in *invalid_index_count
+ * (device int32, caller-zeroed). */
+int vgr_world_to_opencv_viewmats(const double* world_matrices, const int32_t* camera_indices,
+                                 int64_t count, float* viewmats, int64_t viewmat_count,
+                                 int32_t* invalid_index_count, void* stream);
 /* ----------------------------------------------------- differentiable form */
 /* Training form of the camera path: the forward above plus hand-written
  * backward kernels for the compositor and the projection.  No counterpart in

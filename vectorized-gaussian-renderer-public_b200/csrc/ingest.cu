@@ -1,0 +1,213 @@
+// Scene and camera ingestion on the device: INRIA 3DGS PLY vertex rows ->
+// renderer-ready canonical scene tensors, and USD (row-vector) camera world
+// matrices -> OpenCV view matrices.
+//
+// PLY canonicalisation follows src/isaacsim_gaussian_renderer/ply_loader.py:
+// load_ply_to_gaussians (:52-90: property selection, f_rest channel-major ->
+// coefficient-major reorder, semantic_id or 0) and canonicalize_3dgs_scene
+// (:93-135: scale = exp, opacity = sigmoid, quaternion / max(|q|, eps) with
+// |q| <= eps -> identity, features[0..2] = clamp(0.5 + SH_C0 dc, 0, 1)).
+// The reference parses with plyfile on the host and activates with torch
+// operations; here one thread per vertex reads its packed row (any of the
+// PLY scalar types, at the byte offsets of the header) and writes every
+// output, so a scene is ingested in one pass over the file's bytes.
+//
+// Camera ingestion follows src/isaacsim_gaussian_renderer/
+// fabric_camera_kernels.py:8-49 (world matrix rows -> R = rows with the y and
+// z axes negated, t = -R * position), one thread per camera.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstring>
+
+#include "../../include/vgr_b200.h"
+#include "vgr_api_internal.h"
+#include "vgr_common.cuh"
+
+namespace vgr {
+namespace {
+
+__device__ __forceinline__ double read_scalar(const unsigned char* p, int type) {
+  // Rows are packed (no alignment): assemble the value from bytes.
+  unsigned char b[8];
+  const int size = (type == VGR_PLY_FLOAT64 || type == VGR_PLY_INT64) ? 8
+                   : (type == VGR_PLY_INT16 || type == VGR_PLY_UINT16) ? 2
+                   : (type == VGR_PLY_INT8 || type == VGR_PLY_UINT8)   ? 1
+                                                                       : 4;
+  for (int i = 0; i < size; ++i) b[i] = p[i];
+  switch (type) {
+    case VGR_PLY_FLOAT32: { float v; memcpy(&v, b, 4); return v; }
+    case VGR_PLY_FLOAT64: { double v; memcpy(&v, b, 8); return v; }
+    case VGR_PLY_INT8: { int8_t v; memcpy(&v, b, 1); return v; }
+    case VGR_PLY_UINT8: { uint8_t v; memcpy(&v, b, 1); return v; }
+    case VGR_PLY_INT16: { int16_t v; memcpy(&v, b, 2); return v; }
+    case VGR_PLY_UINT16: { uint16_t v; memcpy(&v, b, 2); return v; }
+    case VGR_PLY_INT32: { int32_t v; memcpy(&v, b, 4); return v; }
+    case VGR_PLY_UINT32: { uint32_t v; memcpy(&v, b, 4); return v; }
+    default: { int64_t v; memcpy(&v, b, 8); return static_cast<double>(v); }
+  }
+}
+
+__device__ __forceinline__ int64_t read_integer(const unsigned char* p, int type) {
+  if (type == VGR_PLY_INT64) {
+    int64_t v;
+    memcpy(&v, p, 8);  // byte copy: rows are unaligned
+    return v;
+  }
+  return static_cast<int64_t>(read_scalar(p, type));
+}
+
+struct PlyParams {
+  const unsigned char* rows;
+  int64_t count;
+  vgr_ply_layout layout;
+  float* means;
+  float* scales;
+  float* rotations;
+  float* opacities;
+  float* features;
+  int64_t feature_width;
+  int64_t* semantic_ids;
+};
+
+__global__ void __launch_bounds__(256) ply_canonicalize_kernel(PlyParams p) {
+  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= p.count) return;
+  const unsigned char* row = p.rows + g * p.layout.row_bytes;
+  const vgr_ply_layout& l = p.layout;
+  auto f = [&](int role) {
+    return static_cast<float>(read_scalar(row + l.offsets[role], l.types[role]));
+  };
+  for (int a = 0; a < 3; ++a) p.means[g * 3 + a] = f(VGR_PLY_X + a);
+  for (int a = 0; a < 3; ++a) p.scales[g * 3 + a] = expf(f(VGR_PLY_SCALE0 + a));
+  const float opacity = f(VGR_PLY_OPACITY);
+  p.opacities[g] = 1.0f / (1.0f + expf(-opacity));
+  float q[4];
+  for (int a = 0; a < 4; ++a) q[a] = f(VGR_PLY_ROT0 + a);
+  const float norm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  const float eps = 1.1920928955078125e-07f;  // float32 machine epsilon
+  if (norm <= eps) {
+    p.rotations[g * 4 + 0] = 1.0f;
+    p.rotations[g * 4 + 1] = 0.0f;
+    p.rotations[g * 4 + 2] = 0.0f;
+    p.rotations[g * 4 + 3] = 0.0f;
+  } else {
+    for (int a = 0; a < 4; ++a) p.rotations[g * 4 + a] = q[a] / norm;
+  }
+  float* feat = p.features + g * p.feature_width;
+  const float sh_c0 = 0.28209479177387814f;
+  for (int c = 0; c < 3; ++c) feat[c] = fminf(fmaxf(0.5f + sh_c0 * f(VGR_PLY_DC0 + c), 0.0f), 1.0f);
+  // f_rest is stored channel-major ([3, K-1]); features are coefficient-major.
+  const int rest = l.rest_count;
+  const int per_channel = rest / 3;
+  for (int k = 0; k < per_channel; ++k) {
+    for (int c = 0; c < 3; ++c) {
+      feat[3 + k * 3 + c] = f(VGR_PLY_REST0 + c * per_channel + k);
+    }
+  }
+  for (int64_t i = 3 + rest; i < p.feature_width; ++i) feat[i] = 0.0f;
+  p.semantic_ids[g] = l.has_semantic ? read_integer(row + l.offsets[VGR_PLY_SEMANTIC], l.types[VGR_PLY_SEMANTIC]) : 0;
+}
+
+__global__ void __launch_bounds__(256) world_to_opencv_kernel(const double* __restrict__ world,
+                                                              const int32_t* __restrict__ indices,
+                                                              int64_t count, int64_t out_count,
+                                                              float* __restrict__ viewmats,
+                                                              int* __restrict__ bad) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int32_t out = indices ? indices[i] : static_cast<int32_t>(i);
+  if (out < 0 || out >= out_count) {
+    atomicAdd(bad, 1);
+    return;
+  }
+  const double* w = world + i * 16;  // row-vector convention: rows 0..2 axes, row 3 position
+  const float px = static_cast<float>(w[12]), py = static_cast<float>(w[13]), pz = static_cast<float>(w[14]);
+  float r[9];
+  for (int c = 0; c < 3; ++c) {
+    r[0 + c] = static_cast<float>(w[0 * 4 + c]);
+    r[3 + c] = -static_cast<float>(w[1 * 4 + c]);
+    r[6 + c] = -static_cast<float>(w[2 * 4 + c]);
+  }
+  float* v = viewmats + static_cast<int64_t>(out) * 16;
+  for (int row = 0; row < 3; ++row) {
+    v[row * 4 + 0] = r[row * 3 + 0];
+    v[row * 4 + 1] = r[row * 3 + 1];
+    v[row * 4 + 2] = r[row * 3 + 2];
+    v[row * 4 + 3] = -(r[row * 3 + 0] * px + r[row * 3 + 1] * py + r[row * 3 + 2] * pz);
+  }
+  v[12] = 0.0f;
+  v[13] = 0.0f;
+  v[14] = 0.0f;
+  v[15] = 1.0f;
+}
+
+}  // namespace
+}  // namespace vgr
+
+using vgr::fail;
+
+extern "C" int vgr_ply_canonicalize(const void* vertex_rows, int64_t count,
+                                    const vgr_ply_layout* layout, float* means, float* scales,
+                                    float* rotations, float* opacities, float* features,
+                                    int64_t feature_width, int64_t* semantic_ids, void* stream) {
+  if (!vertex_rows || !layout || !means || !scales || !rotations || !opacities || !features ||
+      !semantic_ids) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "PLY ingestion arguments must be non-null");
+  }
+  if (count <= 0 || count > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "vertex count must be in [1, INT_MAX]");
+  if (layout->row_bytes <= 0) return fail(VGR_ERR_INVALID_ARGUMENT, "row_bytes must be positive");
+  if (layout->rest_count < 0 || layout->rest_count % 3 != 0 ||
+      layout->rest_count > VGR_PLY_MAX_PROPERTIES - VGR_PLY_REST0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "Expected an RGB-multiple number of f_rest fields, got %d.", layout->rest_count);
+  }
+  if (feature_width < 3 + layout->rest_count) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "features are narrower than 3 + f_rest fields");
+  }
+  const int roles = VGR_PLY_REST0 + layout->rest_count;
+  for (int r = 0; r < roles; ++r) {
+    if (r == VGR_PLY_SEMANTIC && !layout->has_semantic) continue;
+    const int t = layout->types[r];
+    const int size = (t == VGR_PLY_FLOAT64 || t == VGR_PLY_INT64) ? 8
+                     : (t == VGR_PLY_INT16 || t == VGR_PLY_UINT16) ? 2
+                     : (t == VGR_PLY_INT8 || t == VGR_PLY_UINT8)   ? 1
+                                                                   : 4;
+    if (t < VGR_PLY_INT8 || t > VGR_PLY_FLOAT64 || layout->offsets[r] < 0 ||
+        layout->offsets[r] + size > layout->row_bytes) {
+      return fail(VGR_ERR_INVALID_ARGUMENT, "PLY property %d lies outside its vertex row", r);
+    }
+  }
+  vgr::PlyParams p{};
+  p.rows = static_cast<const unsigned char*>(vertex_rows);
+  p.count = count;
+  p.layout = *layout;
+  p.means = means;
+  p.scales = scales;
+  p.rotations = rotations;
+  p.opacities = opacities;
+  p.features = features;
+  p.feature_width = feature_width;
+  p.semantic_ids = semantic_ids;
+  vgr::ply_canonicalize_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0,
+                                 static_cast<cudaStream_t>(stream)>>>(p);
+  return vgr::check_launch("PLY canonicalize");
+}
+
+extern "C" int vgr_world_to_opencv_viewmats(const double* world_matrices,
+                                            const int32_t* camera_indices, int64_t count,
+                                            float* viewmats, int64_t viewmat_count,
+                                            int32_t* invalid_index_count, void* stream) {
+  if (!world_matrices || !viewmats || !invalid_index_count) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "camera ingestion arguments must be non-null");
+  }
+  if (count < 0 || count > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "camera count must be in [0, INT_MAX]");
+  if (!camera_indices && count > viewmat_count) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "more world matrices than view matrices");
+  }
+  if (count == 0) return VGR_OK;
+  vgr::world_to_opencv_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0,
+                                static_cast<cudaStream_t>(stream)>>>(
+      world_matrices, camera_indices, count, viewmat_count, viewmats, invalid_index_count);
+  return vgr::check_launch("world to OpenCV view matrices");
+}

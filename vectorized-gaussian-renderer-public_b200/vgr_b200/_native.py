@@ -147,6 +147,19 @@ class VgrParamGrads(ctypes.Structure):
     ]
 
 
+PLY_MAX_PROPERTIES = 64
+
+
+class VgrPlyLayout(ctypes.Structure):
+    _fields_ = [
+        ("row_bytes", _c_i64),
+        ("offsets", _c_i32 * PLY_MAX_PROPERTIES),
+        ("types", _c_i32 * PLY_MAX_PROPERTIES),
+        ("rest_count", _c_i32),
+        ("has_semantic", _c_i32),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
     ("vgr_version", ctypes.c_char_p, []),
@@ -192,6 +205,12 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
             ctypes.POINTER(_c_i64),
         ],
     ),
+    (
+        "vgr_ply_canonicalize",
+        ctypes.c_int,
+        [_c_p, _c_i64, ctypes.POINTER(VgrPlyLayout), _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p],
+    ),
+    ("vgr_world_to_opencv_viewmats", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p]),
     ("vgr_scene_spatial_order_temp_bytes", _c_i64, [_c_i64]),
     ("vgr_scene_spatial_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
     ("vgr_scene_chunk_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
