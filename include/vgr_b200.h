@@ -158,6 +158,10 @@ typedef struct vgr_render_options {
    * ranges, 6 after compositing.  stage_event_count must be 7. */
   void* const* stage_events;
   int32_t stage_event_count;
+  /* Compositor launch (no counterpart in the reference): 0 = one CTA per
+   * (camera, tile); 1 = a resident grid taking (camera, tile) work items from
+   * a device queue. */
+  int32_t persistent_compositor;
 } vgr_render_options;
 
 #define VGR_STAGE_EVENTS 7
@@ -313,6 +317,17 @@ int vgr_ply_canonicalize(const void* vertex_rows, int64_t count, const vgr_ply_l
 int vgr_world_to_opencv_viewmats(const double* world_matrices, const int32_t* camera_indices,
                                  int64_t count, float* viewmats, int64_t viewmat_count,
                                  int32_t* invalid_index_count, void* stream);
+/* Replaces composite_gaussian_and_mesh (hybrid_compositor.py:21-128): the
+ * depth-ordered straight-alpha composite of a Gaussian render and a mesh
+ * render, all [P] / [P,3] float32 pixel-major; mesh_in_front is [P] uint8.
+ * Same validity rules (alpha > min_alpha, finite alpha and depth), result
+ * bit-identical to the reference's float32 tensor expression. */
+int vgr_composite_gaussian_and_mesh(const float* gaussian_rgb, const float* gaussian_alpha,
+                                    const float* gaussian_depth, const float* mesh_rgb,
+                                    const float* mesh_alpha, const float* mesh_depth,
+                                    int64_t pixels, double min_alpha, double depth_epsilon,
+                                    float* rgb, float* alpha, float* depth,
+                                    uint8_t* mesh_in_front, void* stream);
 /* ----------------------------------------------------- differentiable form */
 /* Training form of the camera path: the forward above plus hand-written
  * backward kernels for the compositor and the projection.  No counterpart in

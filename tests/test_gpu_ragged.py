@@ -45,7 +45,7 @@ def _poses(seed: int):
     return view, intr
 
 
-def _setup(tile_size):
+def _setup(tile_size, persistent_compositor=False):
     device = torch.device("cuda")
     backend = CustomCudaBackend(sh_degree=2, output_srgb=False, tile_size=tile_size)
     service = RendererService(backend, height=64, width=64, max_views=1)
@@ -54,7 +54,8 @@ def _setup(tile_size):
         service.load_scene(sid, **scene.to(device).as_kwargs())
     heights = [h for h, _ in RESOLUTIONS]
     widths = [w for _, w in RESOLUTIONS]
-    return RaggedBatch(backend, heights, widths, tile_size=tile_size), device
+    return RaggedBatch(backend, heights, widths, tile_size=tile_size,
+                       persistent_compositor=persistent_compositor), device
 
 
 def _check_against_oracle(ragged, outputs, view, intr, tile_size):
@@ -84,9 +85,9 @@ def _check_against_oracle(ragged, outputs, view, intr, tile_size):
     assert counters["tile_intersections"] == intersections
 
 
-@pytest.mark.parametrize("tile_size", [8, 16])
-def test_ragged_batch_matches_oracle_per_camera(tile_size):
-    ragged, device = _setup(tile_size)
+@pytest.mark.parametrize("tile_size,persistent", [(8, False), (16, False), (16, True)])
+def test_ragged_batch_matches_oracle_per_camera(tile_size, persistent):
+    ragged, device = _setup(tile_size, persistent)
     view, intr = _poses(1)
     vm, km = view.to(device), intr.to(device)
     ids = torch.tensor(SCENE_IDS, dtype=torch.int64, device=device)

@@ -100,3 +100,18 @@ def test_gpu_world_to_opencv_matches_the_usd_convention():
         want[:3, 3] = -(r @ pos)
         torch.testing.assert_close(got[out], want, rtol=1e-6, atol=1e-5)
     assert torch.all(got[4] == -7.0)  # no camera maps to row 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [0, 1])
+def test_gpu_hybrid_composite_matches_reference(case):
+    from vgr_b200.hybrid_compositor import composite_gaussian_and_mesh
+
+    g = np.load(GOLDEN / "hybrid_composite.npz")
+    t = {k: torch.from_numpy(g[f"c{case}_{k}"]).cuda() for k in (
+        "gaussian_rgb", "gaussian_alpha", "gaussian_depth", "mesh_rgb", "mesh_alpha", "mesh_depth")}
+    res = composite_gaussian_and_mesh(
+        t["gaussian_rgb"], t["gaussian_alpha"], t["gaussian_depth"], t["mesh_rgb"], t["mesh_alpha"],
+        t["mesh_depth"], min_alpha=float(g[f"c{case}_min_alpha"]), depth_epsilon=float(g[f"c{case}_depth_epsilon"]))
+    for field in ("rgb", "alpha", "depth", "mesh_in_front"):
+        np.testing.assert_array_equal(getattr(res, field).cpu().numpy(), g[f"c{case}_out_{field}"], err_msg=field)

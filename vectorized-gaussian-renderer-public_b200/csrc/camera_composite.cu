@@ -95,19 +95,15 @@ __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamP
   }
 }
 
+// One work item (one (camera, tile)); every exit is CTA-uniform.
 template <int kTile, bool kFull, bool kTrain>
-__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
-                                  2048 / CompositeGeometry<kTile>::kThreads / 2)
-    composite_kernel(CompositeParams p) {
+__device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t item,
+                                               float4* s_geo, float4* s_cpo, float4* s_col,
+                                               uint32_t* s_mask) {
   using Geo = CompositeGeometry<kTile>;
-  __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
-  __shared__ float4 s_cpo[kCompositeBatch];  // -conic_yy/2, lo, opacity, -
-  __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
-  __shared__ uint32_t s_mask[kCompositeBatch];
-
   CamPlan plan;
   int64_t local_tile;
-  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, blockIdx.x, plan,
+  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, item, plan,
                    local_tile)) {
     return;
   }
@@ -184,6 +180,37 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
 
   if (valid0) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y0, s0);
   if (valid1) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y1, s1);
+}
+
+// One CTA per work item, or (p.persistent) a resident grid whose CTAs take
+// work items from a device queue (ScratchHeader::composite_queue, zeroed by
+// the camera setup) until every (camera, tile) of the frame is done: no
+// CTA is launched for the grid's empty tail, and a CTA that finishes a cheap
+// tile immediately takes the next one.
+template <int kTile, bool kFull, bool kTrain>
+__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
+                                  2048 / CompositeGeometry<kTile>::kThreads / 2)
+    composite_kernel(CompositeParams p) {
+  __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
+  __shared__ float4 s_cpo[kCompositeBatch];  // -conic_yy/2, lo, opacity, -
+  __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
+  __shared__ uint32_t s_mask[kCompositeBatch];
+  __shared__ uint32_t s_item;
+  if (!p.persistent) {
+    composite_item<kTile, kFull, kTrain>(p, blockIdx.x, s_geo, s_cpo, s_col, s_mask);
+    return;
+  }
+  ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
+  const int64_t* tile_prefix = reinterpret_cast<const int64_t*>(p.scratch + p.layout.tile_prefix);
+  const int64_t total = tile_prefix[p.active_count];
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&header->composite_queue, 1u);
+    __syncthreads();
+    const int64_t item = s_item;
+    if (item >= total) break;
+    composite_item<kTile, kFull, kTrain>(p, item, s_geo, s_cpo, s_col, s_mask);
+    __syncthreads();  // shared staging and s_item are reused by the next item
+  }
 }
 
 template __global__ void composite_kernel<4, false, false>(CompositeParams);

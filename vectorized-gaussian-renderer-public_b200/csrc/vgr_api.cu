@@ -197,6 +197,26 @@ extern "C" int vgr_aggregate_chunk_counters(const int64_t* chunk_counters, int64
 
 namespace vgr {
 
+// One CTA per work item, or a resident grid (as many CTAs as fit on the SMs)
+// over the device work queue.
+template <int kTile, bool kFull, bool kTrain>
+void launch_composite(const CompositeParams& cp, int64_t max_items, int sms, cudaStream_t stream) {
+  const int threads = composite_threads(kTile);
+  unsigned grid = static_cast<unsigned>(max_items);
+  if (cp.persistent) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, composite_kernel<kTile, kFull, kTrain>,
+                                                      threads, 0) != cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    const int64_t resident = static_cast<int64_t>(sms) * per_sm;
+    if (resident < max_items) grid = static_cast<unsigned>(resident);
+  }
+  composite_kernel<kTile, kFull, kTrain><<<grid, threads, 0, stream>>>(cp);
+}
+
 int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_outputs* out,
                   const vgr_workspace* ws, const vgr_render_options* opt, void* stream_ptr,
                   int64_t* sorted_buffer_selector, const TrainHooks* train) {
@@ -523,21 +543,21 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     cp.semantic = out->semantic;
     cp.final_transmittance = train ? train->final_transmittance : nullptr;
     cp.last_position = train ? train->last_position : nullptr;
-    const unsigned grid = static_cast<unsigned>(max_items);
+    cp.persistent = opt->persistent_compositor != 0;
     const bool full = opt->full_sensor_output != 0;
     if (train) {
-      if (ts == 16) composite_kernel<16, true, true><<<grid, composite_threads(16), 0, stream>>>(cp);
-      else if (ts == 8) composite_kernel<8, true, true><<<grid, composite_threads(8), 0, stream>>>(cp);
-      else composite_kernel<4, true, true><<<grid, composite_threads(4), 0, stream>>>(cp);
+      if (ts == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);
+      else if (ts == 8) launch_composite<8, true, true>(cp, max_items, sms, stream);
+      else launch_composite<4, true, true>(cp, max_items, sms, stream);
     } else if (ts == 16) {
-      if (full) composite_kernel<16, true, false><<<grid, composite_threads(16), 0, stream>>>(cp);
-      else composite_kernel<16, false, false><<<grid, composite_threads(16), 0, stream>>>(cp);
+      if (full) launch_composite<16, true, false>(cp, max_items, sms, stream);
+      else launch_composite<16, false, false>(cp, max_items, sms, stream);
     } else if (ts == 8) {
-      if (full) composite_kernel<8, true, false><<<grid, composite_threads(8), 0, stream>>>(cp);
-      else composite_kernel<8, false, false><<<grid, composite_threads(8), 0, stream>>>(cp);
+      if (full) launch_composite<8, true, false>(cp, max_items, sms, stream);
+      else launch_composite<8, false, false>(cp, max_items, sms, stream);
     } else {
-      if (full) composite_kernel<4, true, false><<<grid, composite_threads(4), 0, stream>>>(cp);
-      else composite_kernel<4, false, false><<<grid, composite_threads(4), 0, stream>>>(cp);
+      if (full) launch_composite<4, true, false>(cp, max_items, sms, stream);
+      else launch_composite<4, false, false>(cp, max_items, sms, stream);
     }
     if ((rc = check_launch("render: compositor")) != VGR_OK) return rc;
   }

@@ -125,6 +125,7 @@ struct CompositeParams {
   int64_t* semantic;
   float* final_transmittance;  // training: [P] transmittance after the last blended record
   int32_t* last_position;      // training: [P] sorted position one past the last blended record
+  bool persistent;             // resident grid over a device work queue
 };
 
 template <int kTile>

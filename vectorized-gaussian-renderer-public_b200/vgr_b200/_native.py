@@ -116,6 +116,7 @@ class VgrRenderOptions(ctypes.Structure):
         ("sorted_buffer_hint", _c_i32),
         ("stage_events", ctypes.POINTER(_c_p)),
         ("stage_event_count", _c_i32),
+        ("persistent_compositor", _c_i32),
     ]
 
 
@@ -211,6 +212,11 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
         [_c_p, _c_i64, ctypes.POINTER(VgrPlyLayout), _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p],
     ),
     ("vgr_world_to_opencv_viewmats", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p]),
+    (
+        "vgr_composite_gaussian_and_mesh",
+        ctypes.c_int,
+        [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_double, ctypes.c_double, _c_p, _c_p, _c_p, _c_p, _c_p],
+    ),
     ("vgr_scene_spatial_order_temp_bytes", _c_i64, [_c_i64]),
     ("vgr_scene_spatial_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
     ("vgr_scene_chunk_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),

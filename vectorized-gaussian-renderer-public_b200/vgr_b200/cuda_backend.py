@@ -122,6 +122,7 @@ class CustomCudaBackend:
         sh_degree: int | None = None,
         mirror_reference_workspace: bool = False,
         spatial_layout: bool = True,
+        persistent_compositor: bool = False,
     ) -> None:
         if max_visible_records is not None and max_visible_records <= 0:
             raise ValueError("max_visible_records must be positive.")
@@ -229,6 +230,9 @@ class CustomCudaBackend:
         # camera's frustum; every output is unchanged (Gaussians keep their
         # ids).  No counterpart in the reference.
         self.spatial_layout = spatial_layout
+        # Compositor as a resident grid over a device work queue (see
+        # vgr_render_options.persistent_compositor).
+        self.persistent_compositor = persistent_compositor
         self._native = native_module
         self._native_loader = native_loader
         self.allow_cpu_for_tests = allow_cpu_for_tests
@@ -660,6 +664,7 @@ class CustomCudaBackend:
             compact_projection_cache=0,
             sh_degree=-1 if self.sh_degree is None else self.sh_degree,
             sorted_buffer_hint=1,
+            persistent_compositor=int(self.persistent_compositor),
         )
         if self._stage_event_handles is not None:
             options.stage_events = self._stage_event_handles

@@ -48,6 +48,7 @@ class RaggedBatch:
         tile_size: int | None = None,
         full_sensor_output: bool = True,
         headroom: float = 1.25,
+        persistent_compositor: bool = False,
     ) -> None:
         if backend.device is None or not backend._packed_scene:
             raise RuntimeError("RaggedBatch needs an initialized backend with registered scenes.")
@@ -62,6 +63,12 @@ class RaggedBatch:
         self.batch = len(self.heights)
         self.full = bool(full_sensor_output)
         self.headroom = float(headroom)
+        # Compositor as a resident grid over the device work queue of
+        # (camera, tile) items instead of one CTA per item slot (the grid of
+        # a ragged batch is sized for its largest camera).  Off by default:
+        # on the 1,024-camera frame both take 11.0 ms (the empty slots exit at
+        # once and the hardware scheduler balances the rest).
+        self.persistent_compositor = bool(persistent_compositor)
         self.tile_size = int(tile_size or backend.tile_size)
         self._visible_capacity = 0
         self._intersection_capacity = 0
@@ -225,6 +232,7 @@ class RaggedBatch:
             full_sensor_output=int(self.full),
             sh_degree=-1 if b.sh_degree is None else b.sh_degree,
             sorted_buffer_hint=1,
+            persistent_compositor=int(self.persistent_compositor),
         )
         if self._stage_events is not None:
             options.stage_events = self._stage_events
