@@ -75,6 +75,8 @@ def parse_args() -> argparse.Namespace:
                         help="override the LiDAR sensor count (small profiling captures)")
     parser.add_argument("--ragged-frames", type=int, default=20,
                         help="frames of the ragged-batch workload (0: skip)")
+    parser.add_argument("--aux-steps", type=int, default=10,
+                        help="timed steps of PLY ingestion and the hybrid compositor (0: skip)")
     parser.add_argument("--diff-steps", type=int, default=10,
                         help="timed steps of the differentiable-form workload (0: skip)")
     parser.add_argument("--ragged-scale", type=float, default=1.0,
@@ -346,6 +348,81 @@ def lidar_cpu_sample(work, rays_stride: int = 256, threads: int | None = None) -
     seconds = time.perf_counter() - start
     rays = dirs.shape[0]
     return rays / seconds, threads, f"sensor 0, {rays} of {work.ray_directions.shape[0]} rays, full 2M scene"
+
+
+# --------------------------------------------------------------------------- ingestion / hybrid
+def run_aux(args, device, world: int) -> dict:
+    """Scene ingestion and the hybrid compositor, the two HBM-bound passes
+    beside the hot path: PLY canonicalisation of a 1M-Gaussian SH3 vertex
+    block already on the device (248 B read + 240 B written per Gaussian),
+    and the Gaussian/mesh composite of two 64 x 640x480 layers (40 B read +
+    21 B written per pixel)."""
+    import numpy as np
+
+    from vgr_b200 import _native
+    from vgr_b200.hybrid_compositor import composite_gaussian_and_mesh
+    from vgr_b200.ply import PlyVertexBlock, _layout
+
+    peak, peak_source = measured_peaks()
+    steps = max(args.aux_steps, 1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(device)
+    # PLY rows: x y z nx ny nz f_dc_0..2 f_rest_0..44 opacity scale_0..2 rot_0..3, float32.
+    count = 1_000_000
+    names = ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2"] + [f"f_rest_{i}" for i in range(45)]
+    names += ["opacity", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    gen = torch.Generator().manual_seed(17)
+    rows = torch.randn((count, len(names)), generator=gen).to(device)
+    block = PlyVertexBlock(count=count, properties=[(n, "float") for n in names],
+                           body=np.zeros(0, np.uint8), row_bytes=4 * len(names))
+    layout, width = _layout(block)
+    outs = [torch.empty((count, 3), device=device), torch.empty((count, 3), device=device),
+            torch.empty((count, 4), device=device), torch.empty((count,), device=device),
+            torch.empty((count, width), device=device), torch.empty((count,), dtype=torch.int64, device=device)]
+    lib = _native.load_library()
+
+    def ingest() -> None:
+        _native.check(lib.vgr_ply_canonicalize(rows.data_ptr(), count, layout, outs[0].data_ptr(), outs[1].data_ptr(),
+                                               outs[2].data_ptr(), outs[3].data_ptr(), outs[4].data_ptr(), width,
+                                               outs[5].data_ptr(), stream.cuda_stream), "ply")
+
+    for _ in range(3):
+        ingest()
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    for _ in range(steps):
+        ingest()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    ply_ms = start.elapsed_time(stop) / steps
+    ply_bytes = count * (4 * len(names) + 4 * (3 + 3 + 4 + 1 + width) + 8)
+    # Hybrid composite of two layers.
+    b, h, w = 64, 480, 640
+    lay = [torch.rand((b, h, w, c), generator=gen).to(device) for c in (3, 1, 1, 3, 1, 1)]
+    lay[2].mul_(10)
+    lay[5].mul_(10)
+    for _ in range(3):
+        composite_gaussian_and_mesh(*lay)
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    for _ in range(steps):
+        composite_gaussian_and_mesh(*lay)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    hyb_ms = start.elapsed_time(stop) / steps
+    px = b * h * w
+    hyb_bytes = px * (40 + 21)
+    return {
+        "ply_canonicalize": {"gaussians": count, "sh_degree": 3, "ms": round(ply_ms, 4),
+                             "gaussians_per_s": round(count / (ply_ms / 1e3), 1),
+                             "achieved_gbs": round(ply_bytes / (ply_ms / 1e3) / 1e9, 1),
+                             "frac_of_hbm": round(ply_bytes / (ply_ms / 1e3) / 1e9 / peak, 4)},
+        "hybrid_composite": {"pixels": px, "ms": round(hyb_ms, 4),
+                             "mpix_per_s": round(px / (hyb_ms / 1e3) / 1e6, 1),
+                             "achieved_gbs": round(hyb_bytes / (hyb_ms / 1e3) / 1e9, 1),
+                             "frac_of_hbm": round(hyb_bytes / (hyb_ms / 1e3) / 1e9 / peak, 4)},
+        "peak_gbs": peak, "peak_source": peak_source,
+    }
 
 
 def run_lidar(args, device, world: int, with_cpu: bool) -> dict:
@@ -833,6 +910,8 @@ def run_b200(args) -> None:
     if args.lidar_steps > 0:
         lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
+    aux = run_aux(args, device, world) if args.aux_steps > 0 else None
+
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -860,6 +939,7 @@ def run_b200(args) -> None:
             "ragged": ragged,
             "differentiable": differentiable,
             "lidar": lidar,
+            "ingest_and_hybrid": aux,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -70,43 +70,82 @@ struct PlyParams {
   int64_t* semantic_ids;
 };
 
-__global__ void __launch_bounds__(256) ply_canonicalize_kernel(PlyParams p) {
-  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (g >= p.count) return;
-  const unsigned char* row = p.rows + g * p.layout.row_bytes;
+constexpr int kPlyRows = 64;         // vertex rows per CTA
+constexpr int kPlyMaxRowBytes = 512; // VGR_PLY_MAX_PROPERTIES x 8 bytes
+constexpr int kPlyMaxStagedWidth = 64;
+
+// One CTA per kPlyRows vertices: the CTA's rows (contiguous in the body) are
+// staged into shared memory with 16-byte coalesced loads, each thread
+// decodes its row from shared memory, and the feature rows (the bulk of the
+// output) go back through shared memory so that their stores are coalesced
+// too.
+__global__ void __launch_bounds__(kPlyRows) ply_canonicalize_kernel(PlyParams p) {
+  __shared__ __align__(16) unsigned char s_rows[kPlyRows * kPlyMaxRowBytes];
+  __shared__ float s_feat[kPlyRows * kPlyMaxStagedWidth];
   const vgr_ply_layout& l = p.layout;
+  const int64_t g0 = static_cast<int64_t>(blockIdx.x) * kPlyRows;
+  const int rows = static_cast<int>(min(static_cast<int64_t>(kPlyRows), p.count - g0));
+  const int64_t bytes = static_cast<int64_t>(rows) * l.row_bytes;
+  const unsigned char* src = p.rows + g0 * l.row_bytes;  // 16-byte aligned: 64 * row_bytes % 16 == 0
+  const int64_t vec = bytes / 16;
+  for (int64_t i = threadIdx.x; i < vec; i += kPlyRows) {
+    reinterpret_cast<uint4*>(s_rows)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
+  }
+  for (int64_t i = vec * 16 + threadIdx.x; i < bytes; i += kPlyRows) s_rows[i] = src[i];
+  __syncthreads();
+
+  const int t = threadIdx.x;
+  const int64_t g = g0 + t;
+  const bool live = t < rows;
+  const unsigned char* row = s_rows + static_cast<int64_t>(t) * l.row_bytes;
   auto f = [&](int role) {
     return static_cast<float>(read_scalar(row + l.offsets[role], l.types[role]));
   };
-  for (int a = 0; a < 3; ++a) p.means[g * 3 + a] = f(VGR_PLY_X + a);
-  for (int a = 0; a < 3; ++a) p.scales[g * 3 + a] = expf(f(VGR_PLY_SCALE0 + a));
-  const float opacity = f(VGR_PLY_OPACITY);
-  p.opacities[g] = 1.0f / (1.0f + expf(-opacity));
-  float q[4];
-  for (int a = 0; a < 4; ++a) q[a] = f(VGR_PLY_ROT0 + a);
-  const float norm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-  const float eps = 1.1920928955078125e-07f;  // float32 machine epsilon
-  if (norm <= eps) {
-    p.rotations[g * 4 + 0] = 1.0f;
-    p.rotations[g * 4 + 1] = 0.0f;
-    p.rotations[g * 4 + 2] = 0.0f;
-    p.rotations[g * 4 + 3] = 0.0f;
-  } else {
-    for (int a = 0; a < 4; ++a) p.rotations[g * 4 + a] = q[a] / norm;
-  }
-  float* feat = p.features + g * p.feature_width;
-  const float sh_c0 = 0.28209479177387814f;
-  for (int c = 0; c < 3; ++c) feat[c] = fminf(fmaxf(0.5f + sh_c0 * f(VGR_PLY_DC0 + c), 0.0f), 1.0f);
-  // f_rest is stored channel-major ([3, K-1]); features are coefficient-major.
   const int rest = l.rest_count;
   const int per_channel = rest / 3;
-  for (int k = 0; k < per_channel; ++k) {
-    for (int c = 0; c < 3; ++c) {
-      feat[3 + k * 3 + c] = f(VGR_PLY_REST0 + c * per_channel + k);
-    }
+  const int width = static_cast<int>(p.feature_width);
+  float dc[3] = {0.0f, 0.0f, 0.0f};
+  int64_t semantic = 0;
+  if (live) {
+    for (int a = 0; a < 3; ++a) p.means[g * 3 + a] = f(VGR_PLY_X + a);
+    for (int a = 0; a < 3; ++a) p.scales[g * 3 + a] = expf(f(VGR_PLY_SCALE0 + a));
+    p.opacities[g] = 1.0f / (1.0f + expf(-f(VGR_PLY_OPACITY)));
+    float q[4];
+    for (int a = 0; a < 4; ++a) q[a] = f(VGR_PLY_ROT0 + a);
+    const float norm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const float eps = 1.1920928955078125e-07f;  // float32 machine epsilon
+    for (int a = 0; a < 4; ++a) p.rotations[g * 4 + a] = norm <= eps ? (a == 0 ? 1.0f : 0.0f) : q[a] / norm;
+    const float sh_c0 = 0.28209479177387814f;
+    for (int c = 0; c < 3; ++c) dc[c] = fminf(fmaxf(0.5f + sh_c0 * f(VGR_PLY_DC0 + c), 0.0f), 1.0f);
+    if (l.has_semantic) semantic = read_integer(row + l.offsets[VGR_PLY_SEMANTIC], l.types[VGR_PLY_SEMANTIC]);
+    p.semantic_ids[g] = semantic;
   }
-  for (int64_t i = 3 + rest; i < p.feature_width; ++i) feat[i] = 0.0f;
-  p.semantic_ids[g] = l.has_semantic ? read_integer(row + l.offsets[VGR_PLY_SEMANTIC], l.types[VGR_PLY_SEMANTIC]) : 0;
+  // Feature rows: f_rest channel-major ([3, K-1]) -> coefficient-major,
+  // assembled in shared memory and stored with coalesced writes (rows wider
+  // than kPlyMaxStagedWidth are written directly).
+  if (width > kPlyMaxStagedWidth) {
+    if (live) {
+      float* feat = p.features + g * p.feature_width;
+      for (int c = 0; c < 3; ++c) feat[c] = dc[c];
+      for (int k = 0; k < per_channel; ++k) {
+        for (int c = 0; c < 3; ++c) feat[3 + k * 3 + c] = f(VGR_PLY_REST0 + c * per_channel + k);
+      }
+      for (int64_t i = 3 + rest; i < p.feature_width; ++i) feat[i] = 0.0f;
+    }
+    return;
+  }
+  if (live) {
+    float* feat = s_feat + t * width;
+    for (int c = 0; c < 3; ++c) feat[c] = dc[c];
+    for (int k = 0; k < per_channel; ++k) {
+      for (int c = 0; c < 3; ++c) feat[3 + k * 3 + c] = f(VGR_PLY_REST0 + c * per_channel + k);
+    }
+    for (int i = 3 + rest; i < width; ++i) feat[i] = 0.0f;
+  }
+  __syncthreads();
+  float* dst = p.features + g0 * p.feature_width;
+  const int n = rows * width;
+  for (int i = threadIdx.x; i < n; i += kPlyRows) dst[i] = s_feat[i];
 }
 
 __global__ void __launch_bounds__(256) world_to_opencv_kernel(const double* __restrict__ world,
@@ -189,8 +228,15 @@ extern "C" int vgr_ply_canonicalize(const void* vertex_rows, int64_t count,
   p.features = features;
   p.feature_width = feature_width;
   p.semantic_ids = semantic_ids;
-  vgr::ply_canonicalize_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0,
-                                 static_cast<cudaStream_t>(stream)>>>(p);
+  if (layout->row_bytes > vgr::kPlyMaxRowBytes) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "PLY vertex rows above %d bytes are not supported",
+                vgr::kPlyMaxRowBytes);
+  }
+  if ((reinterpret_cast<uintptr_t>(vertex_rows) & 15) != 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "vertex rows must start on a 16-byte boundary");
+  }
+  vgr::ply_canonicalize_kernel<<<static_cast<unsigned>((count + vgr::kPlyRows - 1) / vgr::kPlyRows),
+                                 vgr::kPlyRows, 0, static_cast<cudaStream_t>(stream)>>>(p);
   return vgr::check_launch("PLY canonicalize");
 }
 

@@ -79,4 +79,4 @@ def composite_gaussian_and_mesh(
             ),
             "composite_gaussian_and_mesh",
         )
-    return HybridComposite(rgb=rgb, alpha=alpha, depth=depth, mesh_in_front=front.bool())
+    return HybridComposite(rgb=rgb, alpha=alpha, depth=depth, mesh_in_front=front.view(torch.bool))
