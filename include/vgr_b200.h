@@ -107,7 +107,9 @@ typedef struct vgr_outputs {
 } vgr_outputs;
 
 typedef struct vgr_workspace {
-  void* records;                 /* visible_capacity * VGR_RECORD_BYTES, 16-B aligned */
+  void* records;                 /* visible_capacity * VGR_RECORD_BYTES, 16-B aligned;
+                                  * twice that with ray_gaussian_evaluation (the second
+                                  * half holds the exact-ray extension records) */
   int64_t visible_capacity;
   uint64_t* keys_in;             /* [I] sort keys (tile<<32 | depth bits) */
   uint64_t* keys_out;            /* [I] */
@@ -140,7 +142,8 @@ typedef struct vgr_render_options {
   double covariance_epsilon;
   double semantic_min_alpha;
   int32_t antialiased;
-  int32_t ray_gaussian_evaluation; /* must be 0 (exact-ray mode is not built) */
+  int32_t ray_gaussian_evaluation; /* exact ray-Gaussian evaluation (renderer_cuda.cu:795-948,
+                                    * 2190-2270); records doubles; not with antialiased */
   int32_t tile_size;               /* 4, 8 or 16 */
   int32_t output_srgb;
   int32_t deterministic;           /* accepted; ordering is always deterministic */

@@ -65,6 +65,7 @@ class _Options(ctypes.Structure):
         ("full_sensor_output", _i32),
         ("sh_degree", _i32),
         ("threads", _i32),
+        ("ray_eval", _i32),
     ]
 
 
@@ -162,6 +163,7 @@ def render(
     threads: int = 0,
     with_tiles: bool = False,
     ragged: dict | None = None,
+    ray_gaussian_evaluation: bool = False,
 ) -> OracleResult:
     """Render every active camera on the CPU.  ``ragged`` may carry per-camera
     ``widths``, ``heights``, ``tile_offsets``, ``pixel_offsets`` and
@@ -185,7 +187,8 @@ def render(
     )
     if ragged is None:
         total_pixels = batch * height * width
-        tiles = batch * (-(-height // tile_size)) * (-(-width // tile_size))
+        bin_size = 32 if ray_gaussian_evaluation and tile_size == 16 else tile_size
+        tiles = batch * (-(-height // bin_size)) * (-(-width // bin_size))
         cams = _Cameras(
             _ptr(viewmats), _ptr(intrinsics), _ptr(env), _ptr(camera_scene_ids), _ptr(active),
             batch, 0 if active is None else active.shape[0], None, None, None, None,
@@ -207,6 +210,7 @@ def render(
     opts = _Options(
         height, width, near_plane, far_plane, support_sigma, covariance_epsilon,
         semantic_min_alpha, int(antialiased), tile_size, int(output_srgb), 1, sh_degree, threads,
+        int(ray_gaussian_evaluation),
     )
     rgb = np.zeros((total_pixels, 3), dtype=np.float32)
     depth = np.full((total_pixels,), np.inf, dtype=np.float32)

@@ -17,6 +17,9 @@
  *     :1944-1971 deterministic order (tile, depth bits, Gaussian id)
  *     :1973-2305 front-to-back compositor (RGB, alpha, depth, semantic)
  *     :161-166   sRGB transfer
+ *     :795-948   exact-ray mode: FP64 camera-space precision, ray-ellipse
+ *                cull centre and radius
+ *     :203-245, 2190-2270  exact-ray alpha and blend-then-stop compositing
  * with every floating-point operation written in a fixed order with
  * contraction disabled (built with -ffp-contract=off; fmaf only where a fused
  * multiply-add is intended), and exp/log evaluated by the Cody-Waite/Taylor
@@ -30,6 +33,7 @@
  * real-SH basis of the 3D Gaussian Splatting reference implementation as used
  * by gsplat (parity unpinned by any reference fixture).
  */
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -84,6 +88,7 @@ typedef struct vo_options {
   int32_t full_sensor_output;
   int32_t sh_degree;
   int32_t threads;
+  int32_t ray_eval; /* exact ray-Gaussian evaluation (renderer_cuda.cu:203-245,795-948) */
 } vo_options;
 
 typedef struct vo_stats {
@@ -155,6 +160,14 @@ static float vo_srgb(float v) {
   return 1.055f * p - 0.055f;
 }
 
+/* float -> int with CUDA's conversion semantics (saturating, NaN -> 0);
+ * C leaves out-of-range conversions undefined. */
+static int saturating_int(float x) {
+  if (!(x == x)) return 0;
+  if (x >= 2147483648.0f) return INT_MAX;
+  if (x <= -2147483648.0f) return INT_MIN;
+  return (int)x;
+}
 static int ceil_radius(float x) {
   return x > 0.0f ? (int)fminf(ceilf(x), 2147483520.0f) : 0;
 }
@@ -240,11 +253,14 @@ typedef struct vo_record {
   int64_t gid;
   int radius_x, radius_y;
   int min_tx, min_ty, max_tx, max_ty;
+  /* exact-ray mode: camera-space precision (upper triangle), precision * mean
+   * and mean^T precision mean, all rounded from double */
+  float prec[6], prec_mean[3], mean_prec_mean;
 } vo_record;
 
 static int project(const vo_scene* s, int64_t g, const cam_const* c, float near_plane,
-                   float far_plane, float sigma, float eps, int antialiased, vo_record* out,
-                   float* pxyz) {
+                   float far_plane, float sigma, float eps, int antialiased, int ray_eval,
+                   vo_record* out, float* pxyz) {
   float o = s->opacities[g];
   if (!(o >= ALPHA_THRESHOLD)) return 0;
   const float mx = s->means[g * 3 + 0], my = s->means[g * 3 + 1], mz = s->means[g * 3 + 2];
@@ -294,14 +310,80 @@ static int project(const vo_scene* s, int64_t g, const cam_const* c, float near_
   }
   const float ext_o = sqrtf(2.0f * vo_log(o / ALPHA_THRESHOLD));
   const float ext = fminf(sigma, ext_o);
-  const int rx = ceil_radius(ext * sqrtf(a));
-  const int ry = ceil_radius(ext * sqrtf(cc));
+  int rx = ceil_radius(ext * sqrtf(a));
+  int ry = ceil_radius(ext * sqrtf(cc));
   if (rx <= 0 && ry <= 0) return 0;
+  float cull_x = u, cull_y = v;
+  if (ray_eval) {
+    /* Exact ray evaluation: precision of the camera-space covariance and the
+     * image-plane ellipse where a pixel ray's Mahalanobis distance to the
+     * mean is at most sigma (renderer_cuda.cu:795-948), in double. */
+    const double d00 = c00, d01 = c01, d02 = c02, d11 = c11, d12 = c12, d22 = c22;
+    const double det3 = d00 * (d11 * d22 - d12 * d12) - d01 * (d01 * d22 - d02 * d12) +
+                        d02 * (d01 * d12 - d02 * d11);
+    if (!(det3 > 1.0e-48)) return 0;
+    const double inv3 = 1.0 / det3;
+    const double p00 = (d11 * d22 - d12 * d12) * inv3;
+    const double p01 = (d02 * d12 - d01 * d22) * inv3;
+    const double p02 = (d01 * d12 - d02 * d11) * inv3;
+    const double p11 = (d00 * d22 - d02 * d02) * inv3;
+    const double p12 = (d01 * d02 - d00 * d12) * inv3;
+    const double p22 = (d00 * d11 - d01 * d01) * inv3;
+    const double x = px, y = py, z = pz;
+    const double m0 = p00 * x + p01 * y + p02 * z;
+    const double m1 = p01 * x + p11 * y + p12 * z;
+    const double m2 = p02 * x + p12 * y + p22 * z;
+    const double mpm = x * m0 + y * m1 + z * m2;
+    out->prec[0] = (float)p00;
+    out->prec[1] = (float)p01;
+    out->prec[2] = (float)p02;
+    out->prec[3] = (float)p11;
+    out->prec[4] = (float)p12;
+    out->prec[5] = (float)p22;
+    out->prec_mean[0] = (float)m0;
+    out->prec_mean[1] = (float)m1;
+    out->prec_mean[2] = (float)m2;
+    out->mean_prec_mean = (float)mpm;
+    const double q = mpm - (double)sigma * (double)sigma;
+    const double k00 = q * p00 - m0 * m0, k01 = q * p01 - m0 * m1, k02 = q * p02 - m0 * m2;
+    const double k11 = q * p11 - m1 * m1, k12 = q * p12 - m1 * m2, k22 = q * p22 - m2 * m2;
+    const double kdet = k00 * k11 - k01 * k01;
+    int finite = 0;
+    if (k00 > 0.0 && kdet > 0.0) {
+      const double ikd = 1.0 / kdet;
+      const double cxn = (k01 * k12 - k11 * k02) * ikd;
+      const double cyn = (k01 * k02 - k00 * k12) * ikd;
+      const double scale = -(k22 + k02 * cxn + k12 * cyn);
+      if (scale > 0.0) {
+        const double exn = sqrt(scale * k11 * ikd);
+        const double eyn = sqrt(scale * k00 * ikd);
+        const double cmx = (double)c->fx * cxn + (double)c->cx;
+        const double cmy = (double)c->fy * cyn + (double)c->cy;
+        cull_x = (float)cmx;
+        cull_y = (float)cmy;
+        const int erx = saturating_int(ceilf((float)(fabs((double)c->fx) * exn)));
+        const int ery = saturating_int(ceilf((float)(fabs((double)c->fy) * eyn)));
+        rx = erx > 1 ? erx : 1;
+        ry = ery > 1 ? ery : 1;
+        finite = isfinite(cmx) && isfinite(cmy) && isfinite(exn) && isfinite(eyn);
+      }
+    }
+    if (!finite) {
+      const int full = (int)c->width > (int)c->height ? (int)c->width : (int)c->height;
+      cull_x = 0.5f * c->width;
+      cull_y = 0.5f * c->height;
+      rx = full;
+      ry = full;
+    }
+  }
   const float frx = (float)rx, fry = (float)ry;
-  if (u + frx <= 0.0f || v + fry <= 0.0f || u - frx >= c->width || v - fry >= c->height) return 0;
+  if (cull_x + frx <= 0.0f || cull_y + fry <= 0.0f || cull_x - frx >= c->width ||
+      cull_y - fry >= c->height) {
+    return 0;
+  }
   const float idet = 1.0f / det;
-  out->mean_x = u;
-  out->mean_y = v;
+  out->mean_x = cull_x;
+  out->mean_y = cull_y;
   out->conic0 = cc * idet;
   out->conic1 = (-b) * idet;
   out->conic2 = a * idet;
@@ -392,7 +474,9 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
 #ifdef _OPENMP
   if (opt->threads > 0) omp_set_num_threads(opt->threads);
 #endif
-  const int ts = opt->tile_size;
+  /* Exact-ray mode bins 16-pixel tiles as 32-pixel tiles in the plain form
+   * (renderer_cuda.cu:2670-2676). */
+  const int ts = (opt->ray_eval && opt->tile_size == 16 && !cams->widths) ? 32 : opt->tile_size;
   const float near_f = (float)opt->near_plane, far_f = (float)opt->far_plane;
   const float sigma = (float)opt->support_sigma, eps = (float)opt->covariance_epsilon;
   const float its = 1.0f / (float)ts;
@@ -455,7 +539,7 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
       const int64_t g = si->g_begin + i;
       float p[3];
       vo_record r;
-      if (!project(s, g, &c, near_f, far_f, sigma, eps, opt->antialiased, &r, p)) continue;
+      if (!project(s, g, &c, near_f, far_f, sigma, eps, opt->antialiased, opt->ray_eval, &r, p)) continue;
       if (opt->sh_degree < 0) {
         r.rgb[0] = s->features[g * s->feature_width + 0];
         r.rgb[1] = s->features[g * s->feature_width + 1];
@@ -550,7 +634,43 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
           const float cx = (float)x + 0.5f, cy = (float)y + 0.5f;
           float tr = 1.0f, r = 0.0f, g = 0.0f, b = 0.0f, dep = 0.0f, best_w = -1.0f;
           int64_t best_sem = -1;
-          for (int64_t i = start; i < end; ++i) {
+          if (opt->ray_eval) {
+            /* Exact ray evaluation (renderer_cuda.cu:203-245,2190-2270): the
+             * pixel ray's Mahalanobis distance to each mean, no 1/255 cut or
+             * 0.99 clamp, and the record that takes T to 1e-4 is blended. */
+            const float* in = cams->intrinsics + si->camera * 9;
+            const float ray_x = (cx - in[2]) / in[0];
+            const float ray_y = (cy - in[5]) / in[4];
+            const float s2 = sigma * sigma;
+            for (int64_t i = start; i < end; ++i) {
+              const vo_record* rec = &records[entries[i].record];
+              const float* P = rec->prec;
+              const float rpr = fmaf(2.0f * P[4], ray_y,
+                                     fmaf(P[3] * ray_y, ray_y,
+                                          fmaf(2.0f * P[2], ray_x,
+                                               fmaf((2.0f * P[1]) * ray_x, ray_y, (P[0] * ray_x) * ray_x)))) +
+                                P[5];
+              if (!(rpr > 0.0f)) continue;
+              const float rpm = fmaf(ray_y, rec->prec_mean[1], ray_x * rec->prec_mean[0]) + rec->prec_mean[2];
+              const float m2 = fmaxf(0.0f, rec->mean_prec_mean - (rpm * rpm) / rpr);
+              if (m2 > s2 || m2 > 174.0f) continue; /* exp below float range: no contribution */
+              const float al = fminf(1.0f, rec->opacity * vo_exp(-0.5f * m2));
+              if (!(al > 0.0f)) continue;
+              const float next_t = tr * (1.0f - al);
+              const float w = tr * al;
+              r = fmaf(w, rec->rgb[0], r);
+              g = fmaf(w, rec->rgb[1], g);
+              b = fmaf(w, rec->rgb[2], b);
+              dep = fmaf(w, rec->depth, dep);
+              if (w > best_w) {
+                best_w = w;
+                best_sem = s->semantic_ids[rec->gid];
+              }
+              tr = next_t;
+              if (next_t <= TRANSMITTANCE_THRESHOLD) break;
+            }
+          }
+          for (int64_t i = start; i < end && !opt->ray_eval; ++i) {
             const vo_record* rec = &records[entries[i].record];
             const float dx = cx - rec->mean_x;
             const float dy = cy - rec->mean_y;

@@ -48,7 +48,9 @@ def render_reference(ref, case, device):
     batch = rig.viewmats.shape[0]
     h, w = rig.height, rig.width
     ts = opts.get("tile_size", 16)
-    tiles = batch * (-(-h // ts)) * (-(-w // ts))
+    ray = opts.get("ray_gaussian_evaluation", False)
+    bin_size = 32 if ray and ts == 16 else ts  # renderer_cuda.cu:2670-2676
+    tiles = batch * (-(-h // bin_size)) * (-(-w // bin_size))
     visible_cap = batch * sum(counts)
     isect_cap = max(visible_cap * 64, 1024)
     deterministic = opts.get("deterministic", True)
@@ -81,8 +83,8 @@ def render_reference(ref, case, device):
         torch.zeros((1,), dtype=i64, device=device),
         torch.zeros((1,), dtype=i32, device=device),
         torch.zeros((1,), dtype=f32, device=device),
-        torch.zeros((1, 6), dtype=f32, device=device),
-        torch.zeros((1, 4), dtype=f32, device=device),
+        torch.zeros((visible_cap if ray else 1, 6), dtype=f32, device=device),
+        torch.zeros((visible_cap if ray else 1, 4), dtype=f32, device=device),
     ]
     out = [
         torch.zeros((batch, h, w, 3), dtype=f32, device=device),
@@ -111,7 +113,7 @@ def render_reference(ref, case, device):
         opts.get("covariance_epsilon", 0.3),
         opts.get("rasterize_mode", "classic") == "antialiased",
         opts.get("semantic_min_alpha", 0.01),
-        False,
+        ray,
         ts,
         4096,
         64,
@@ -144,11 +146,14 @@ def render_reference(ref, case, device):
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--out", type=Path, default=Path(__file__).resolve().parent)
+    parser.add_argument("--cases", nargs="*", default=None, help="subset of case names")
     args = parser.parse_args()
     device = torch.device("cuda")
     ref = load_reference_module("vgr_reference_camera")
     args.out.mkdir(parents=True, exist_ok=True)
     for name, case in CASES.items():
+        if args.cases and name not in args.cases:
+            continue
         result = render_reference(ref, case, device)
         path = args.out / f"camera_{name}.npz"
         np.savez_compressed(path, **result)

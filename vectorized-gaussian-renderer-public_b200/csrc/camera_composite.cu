@@ -213,6 +213,153 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Exact-ray compositor (renderer_cuda.cu:203-245 and 2190-2270): every pixel
+// casts the camera ray d = (nx, ny, 1), nx = (x + 0.5 - cx) / fx, and each
+// record in (depth, Gaussian id) order contributes alpha = min(1, o
+// exp(-m^2/2)) with m^2 = max(0, m^T P m - (d^T P m)^2 / d^T P d), the
+// squared Mahalanobis distance from the mean to the ray, for m^2 <= sigma^2.
+// No 1/255 cut and no 0.99 clamp; the record that takes T to <= 1e-4 is
+// blended and then the pixel stops.  Same CTA and pixel layout as the
+// screen-space compositor, without its warp footprint masks (the record's
+// ellipse is the tile cover itself).  A terminated pixel's ray_y becomes NaN,
+// so every later d^T P d is NaN and fails the > 0 test.
+// ---------------------------------------------------------------------------
+template <bool kFull>
+__device__ __forceinline__ void blend_ray(PixelState& s, float& ray_y, float alpha, int32_t pos,
+                                          const float4& col) {
+  const float next_t = fmul(s.transmittance, fsub(1.0f, alpha));
+  const float w = fmul(s.transmittance, alpha);
+  s.r = ffma(w, col.x, s.r);
+  s.g = ffma(w, col.y, s.g);
+  s.b = ffma(w, col.z, s.b);
+  if (kFull) {
+    s.depth = ffma(w, col.w, s.depth);
+    if (w > s.best_weight) {
+      s.best_weight = w;
+      s.best_pos = pos;
+    }
+  }
+  s.transmittance = next_t;
+  if (next_t <= kTransmittanceThreshold) {
+    s.done = true;
+    ray_y = __int_as_float(0x7fc00000);
+  }
+}
+
+// alpha of one record on one ray (0 when it does not contribute); rx_terms
+// carries the ray_x products shared by the thread's two pixels.
+__device__ __forceinline__ float ray_alpha(const float4& p0, const float4& p1, const float4& p2,
+                                           float ray_x, float ray_y, float t_xx, float t_xy,
+                                           float t_x, float t_m, float s2) {
+  // d^T P d = P00 x^2 + 2 P01 x y + 2 P02 x + P11 y^2 + 2 P12 y + P22
+  const float rpr = fadd(
+      ffma(fmul(2.0f, p1.x), ray_y,
+           ffma(fmul(p0.w, ray_y), ray_y, ffma(t_x, ray_x, ffma(t_xy, ray_y, t_xx)))),
+      p1.y);
+  if (!(rpr > 0.0f)) return 0.0f;
+  const float rpm = fadd(ffma(ray_y, p1.w, t_m), p2.x);
+  const float m2 = fmaxf(0.0f, fsub(p2.y, fdiv(fmul(rpm, rpm), rpr)));
+  // m^2 > 174 would take exp below the float range of the polynomial exp:
+  // alpha < 2e-38, no contribution.
+  if (!(m2 <= s2) || !(m2 <= 174.0f)) return 0.0f;
+  return fminf(1.0f, fmul(p2.z, vexp(fmul(-0.5f, m2))));
+}
+
+template <int kTile, bool kFull>
+__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
+                                  2048 / CompositeGeometry<kTile>::kThreads / 2)
+    composite_ray_kernel(CompositeParams p) {
+  using Geo = CompositeGeometry<kTile>;
+  __shared__ float4 s_p0[kCompositeBatch];   // P00, P01, P02, P11
+  __shared__ float4 s_p1[kCompositeBatch];   // P12, P22, Pm0, Pm1
+  __shared__ float4 s_p2[kCompositeBatch];   // Pm2, mPm, opacity, -
+  __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
+  CamPlan plan;
+  int64_t local_tile;
+  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, blockIdx.x, plan,
+                   local_tile)) {
+    return;
+  }
+  const int tile_y = static_cast<int>(local_tile / plan.tiles_x);
+  const int tile_x = static_cast<int>(local_tile - static_cast<int64_t>(tile_y) * plan.tiles_x);
+  const int64_t global_tile = plan.tile_base + local_tile;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int lx = lane % Geo::kBlockW;
+  const int ly = lane / Geo::kBlockW;
+  const bool lane_used = ly < Geo::kLaneRows;
+  const int pixel_x = tile_x * kTile + (warp % Geo::kWarpsX) * Geo::kBlockW + lx;
+  const int pixel_y0 = tile_y * kTile + (warp / Geo::kWarpsX) * Geo::kBlockH + ly;
+  const int pixel_y1 = pixel_y0 + Geo::kLaneRows;
+  const bool valid0 = lane_used && pixel_x < plan.width && pixel_y0 < plan.height;
+  const bool valid1 = lane_used && pixel_x < plan.width && pixel_y1 < plan.height;
+  const float kNaN = __int_as_float(0x7fc00000);
+  const float* in = p.intrinsics + static_cast<int64_t>(plan.camera) * 9;
+  const float fx = in[0], cxi = in[2], fy = in[4], cyi = in[5];
+  const float ray_x = fdiv(fsub(fadd(static_cast<float>(pixel_x), 0.5f), cxi), fx);
+  float ray_y0 = valid0 ? fdiv(fsub(fadd(static_cast<float>(pixel_y0), 0.5f), cyi), fy) : kNaN;
+  float ray_y1 = valid1 ? fdiv(fsub(fadd(static_cast<float>(pixel_y1), 0.5f), cyi), fy) : kNaN;
+  const float s2 = fmul(p.support_sigma, p.support_sigma);
+
+  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid0};
+  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid1};
+  bool warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
+
+  const int64_t range_start = p.tile_starts[global_tile];
+  const int64_t range_end = p.tile_ends[global_tile];
+  if (range_start >= 0 && range_end > range_start) {
+    for (int64_t chunk = range_start; chunk < range_end; chunk += kCompositeBatch) {
+      const int n = static_cast<int>(min(static_cast<int64_t>(kCompositeBatch), range_end - chunk));
+      for (int j = tid; j < n; j += Geo::kThreads) {
+        const int32_t r = p.values[chunk + j];
+        const Record& rec = p.records[r];
+        const float4 e2 = p.ray_ext[static_cast<int64_t>(r) * 3 + 2];
+        s_p0[j] = p.ray_ext[static_cast<int64_t>(r) * 3 + 0];
+        s_p1[j] = p.ray_ext[static_cast<int64_t>(r) * 3 + 1];
+        s_p2[j] = make_float4(e2.x, e2.y, rec.b.y, 0.0f);
+        s_col[j] = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
+      }
+      __syncthreads();
+      if (!warp_done) {
+        const int32_t chunk_pos = static_cast<int32_t>(chunk);
+        for (int j = 0; j < n; ++j) {
+          const float4 p0 = s_p0[j];
+          const float4 p1 = s_p1[j];
+          const float4 p2 = s_p2[j];
+          const float t_xx = fmul(fmul(p0.x, ray_x), ray_x);
+          const float t_xy = fmul(fmul(2.0f, p0.y), ray_x);
+          const float t_x = fmul(2.0f, p0.z);
+          const float t_m = fmul(ray_x, p1.z);
+          const float a0 = ray_alpha(p0, p1, p2, ray_x, ray_y0, t_xx, t_xy, t_x, t_m, s2);
+          const float a1 = ray_alpha(p0, p1, p2, ray_x, ray_y1, t_xx, t_xy, t_x, t_m, s2);
+          if (a0 > 0.0f || a1 > 0.0f) {
+            const float4 col = s_col[j];
+            if (a0 > 0.0f) blend_ray<kFull>(s0, ray_y0, a0, chunk_pos + j, col);
+            if (a1 > 0.0f) blend_ray<kFull>(s1, ray_y1, a1, chunk_pos + j, col);
+          }
+          if ((j & 31) == 31 && __all_sync(0xffffffffu, s0.done && s1.done)) break;
+        }
+        warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
+      }
+      if (__syncthreads_count(!(s0.done && s1.done)) == 0) break;
+    }
+  }
+  if (valid0) write_pixel<kFull, false>(p, plan, pixel_x, pixel_y0, s0);
+  if (valid1) write_pixel<kFull, false>(p, plan, pixel_x, pixel_y1, s1);
+}
+
+template __global__ void composite_ray_kernel<4, false>(CompositeParams);
+template __global__ void composite_ray_kernel<4, true>(CompositeParams);
+template __global__ void composite_ray_kernel<8, false>(CompositeParams);
+template __global__ void composite_ray_kernel<8, true>(CompositeParams);
+template __global__ void composite_ray_kernel<16, false>(CompositeParams);
+template __global__ void composite_ray_kernel<16, true>(CompositeParams);
+template __global__ void composite_ray_kernel<32, false>(CompositeParams);
+template __global__ void composite_ray_kernel<32, true>(CompositeParams);
+
 template __global__ void composite_kernel<4, false, false>(CompositeParams);
 template __global__ void composite_kernel<4, true, false>(CompositeParams);
 template __global__ void composite_kernel<8, false, false>(CompositeParams);

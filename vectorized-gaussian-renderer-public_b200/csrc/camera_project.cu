@@ -134,9 +134,14 @@ struct Projected {
   float cov_a, cov_b, cov_c;
   float px, py, pz;
   int radius_x, radius_y;
+  // Exact-ray mode: camera-space precision (upper triangle), precision times
+  // the camera-space mean, and mean^T precision mean, rounded from double.
+  float prec[6], prec_mean[3], mean_prec_mean;
 };
 
-// EWA projection of one Gaussian (renderer_cuda.cu:287-490 screen-space path).
+// EWA projection of one Gaussian (renderer_cuda.cu:287-490 screen-space path;
+// with kRay the exact-ray additions of renderer_cuda.cu:795-948).
+template <bool kRay>
 __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means,
                                                  const float* __restrict__ covariances,
                                                  const float* __restrict__ opacities,
@@ -159,7 +164,7 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
 
   const float* s = covariances + g * 6;
   const float s00 = s[0], s01 = s[1], s02 = s[2], s11 = s[3], s12 = s[4], s22 = s[5];
-  {
+  if (!kRay) {
     // Early off-screen cull, conservative so that it never drops a record
     // the full test below keeps.  The x-row of the Jacobian has squared norm
     // (fx/z)^2 (1 + clamp(x/z)^2) <= (fx/z)^2 (1 + L^2), the camera-space
@@ -226,18 +231,89 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
   }
   const float ext_o = fsqrt(fmul(2.0f, vlog(fdiv(o, kAlphaThreshold))));
   const float ext = fminf(support_sigma, ext_o);
-  const int rx = ceil_radius(fmul(ext, fsqrt(a)));
-  const int ry = ceil_radius(fmul(ext, fsqrt(cc)));
+  int rx = ceil_radius(fmul(ext, fsqrt(a)));
+  int ry = ceil_radius(fmul(ext, fsqrt(cc)));
   if (rx <= 0 && ry <= 0) return false;
+  float cull_x = u, cull_y = v;
+  if (kRay) {
+    // Precision of the camera-space covariance, and the image-plane ellipse
+    // where a pixel ray's Mahalanobis distance to the mean is at most sigma:
+    // the rays x = (nx, ny, 1) t with (m^T P d)^2 / (d^T P d) >= m^T P m -
+    // sigma^2 form the conic d^T K d <= 0, K = (m^T P m - sigma^2) P -
+    // (P m)(P m)^T, whose centre and extents (in normalised coordinates)
+    // give the record's cull centre and tile radius.  A degenerate or
+    // unbounded ellipse falls back to the whole image.
+    const double d00 = c00, d01 = c01, d02 = c02, d11 = c11, d12 = c12, d22 = c22;
+    const double det3 = dadd(dsub(dmul(d00, dsub(dmul(d11, d22), dmul(d12, d12))),
+                                  dmul(d01, dsub(dmul(d01, d22), dmul(d02, d12)))),
+                             dmul(d02, dsub(dmul(d01, d12), dmul(d02, d11))));
+    if (!(det3 > 1.0e-48)) return false;
+    const double inv3 = ddiv(1.0, det3);
+    const double p00 = dmul(dsub(dmul(d11, d22), dmul(d12, d12)), inv3);
+    const double p01 = dmul(dsub(dmul(d02, d12), dmul(d01, d22)), inv3);
+    const double p02 = dmul(dsub(dmul(d01, d12), dmul(d02, d11)), inv3);
+    const double p11 = dmul(dsub(dmul(d00, d22), dmul(d02, d02)), inv3);
+    const double p12 = dmul(dsub(dmul(d01, d02), dmul(d00, d12)), inv3);
+    const double p22 = dmul(dsub(dmul(d00, d11), dmul(d01, d01)), inv3);
+    const double x = px, y = py, z = pz;
+    const double m0 = dadd(dadd(dmul(p00, x), dmul(p01, y)), dmul(p02, z));
+    const double m1 = dadd(dadd(dmul(p01, x), dmul(p11, y)), dmul(p12, z));
+    const double m2 = dadd(dadd(dmul(p02, x), dmul(p12, y)), dmul(p22, z));
+    const double mpm = dadd(dadd(dmul(x, m0), dmul(y, m1)), dmul(z, m2));
+    out->prec[0] = static_cast<float>(p00);
+    out->prec[1] = static_cast<float>(p01);
+    out->prec[2] = static_cast<float>(p02);
+    out->prec[3] = static_cast<float>(p11);
+    out->prec[4] = static_cast<float>(p12);
+    out->prec[5] = static_cast<float>(p22);
+    out->prec_mean[0] = static_cast<float>(m0);
+    out->prec_mean[1] = static_cast<float>(m1);
+    out->prec_mean[2] = static_cast<float>(m2);
+    out->mean_prec_mean = static_cast<float>(mpm);
+    const double sg = static_cast<double>(support_sigma);
+    const double q = dsub(mpm, dmul(sg, sg));
+    const double k00 = dsub(dmul(q, p00), dmul(m0, m0));
+    const double k01 = dsub(dmul(q, p01), dmul(m0, m1));
+    const double k02 = dsub(dmul(q, p02), dmul(m0, m2));
+    const double k11 = dsub(dmul(q, p11), dmul(m1, m1));
+    const double k12 = dsub(dmul(q, p12), dmul(m1, m2));
+    const double k22 = dsub(dmul(q, p22), dmul(m2, m2));
+    const double kdet = dsub(dmul(k00, k11), dmul(k01, k01));
+    bool finite = false;
+    if (k00 > 0.0 && kdet > 0.0) {
+      const double ikd = ddiv(1.0, kdet);
+      const double cxn = dmul(dsub(dmul(k01, k12), dmul(k11, k02)), ikd);
+      const double cyn = dmul(dsub(dmul(k01, k02), dmul(k00, k12)), ikd);
+      const double scale = -dadd(dadd(k22, dmul(k02, cxn)), dmul(k12, cyn));
+      if (scale > 0.0) {
+        const double exn = dsqrt(dmul(dmul(scale, k11), ikd));
+        const double eyn = dsqrt(dmul(dmul(scale, k00), ikd));
+        const double cmx = dadd(dmul(static_cast<double>(c.fx), cxn), static_cast<double>(c.cx));
+        const double cmy = dadd(dmul(static_cast<double>(c.fy), cyn), static_cast<double>(c.cy));
+        cull_x = static_cast<float>(cmx);
+        cull_y = static_cast<float>(cmy);
+        rx = max(1, static_cast<int>(ceilf(static_cast<float>(dmul(fabs(static_cast<double>(c.fx)), exn)))));
+        ry = max(1, static_cast<int>(ceilf(static_cast<float>(dmul(fabs(static_cast<double>(c.fy)), eyn)))));
+        finite = isfinite(cmx) && isfinite(cmy) && isfinite(exn) && isfinite(eyn);
+      }
+    }
+    if (!finite) {
+      const int full = max(static_cast<int>(c.width), static_cast<int>(c.height));
+      cull_x = fmul(0.5f, c.width);
+      cull_y = fmul(0.5f, c.height);
+      rx = full;
+      ry = full;
+    }
+  }
   const float frx = static_cast<float>(rx);
   const float fry = static_cast<float>(ry);
-  if (fadd(u, frx) <= 0.0f || fadd(v, fry) <= 0.0f || fsub(u, frx) >= c.width ||
-      fsub(v, fry) >= c.height) {
+  if (fadd(cull_x, frx) <= 0.0f || fadd(cull_y, fry) <= 0.0f || fsub(cull_x, frx) >= c.width ||
+      fsub(cull_y, fry) >= c.height) {
     return false;
   }
   const float idet = fdiv(1.0f, det);
-  out->mean_x = u;
-  out->mean_y = v;
+  out->mean_x = cull_x;
+  out->mean_y = cull_y;
   out->conic0 = fmul(cc, idet);
   out->conic1 = fmul(-b, idet);
   out->conic2 = fmul(a, idet);
@@ -401,7 +477,10 @@ __device__ __forceinline__ bool chunk_outside_frustum(const CamConst& c, float4 
   return false;
 }
 
-template <int kShDegree>
+// kRay: exact-ray records (renderer_cuda.cu:795-948) - no early or chunk
+// frustum cull (the ellipse cull decides), and each record's precision terms
+// go to the extension records p.ray_ext[3 r .. 3 r + 2].
+template <int kShDegree, bool kRay>
 __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
   __shared__ uint16_t s_slot[kProjectChunk];       // rank -> task slot
@@ -449,7 +528,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           const CamPlan& plan = plans[slot];
           const int scene_slot = plan.scene_slot;
           live = plan.camera >= 0 && scene_slot >= 0 && chunk * kProjectChunk < plan.g_count;
-          if (live && p.chunk_bounds) {
+          if (live && p.chunk_bounds && !kRay) {
             const int64_t ci = p.chunk_offsets[scene_slot] + chunk;
             live = !chunk_outside_frustum(cam_consts[slot], p.chunk_bounds[ci * 2],
                                           p.chunk_bounds[ci * 2 + 1], p.near_plane, p.far_plane,
@@ -496,6 +575,8 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
     bool vis[kProjectRounds];
     uint32_t ntiles[kProjectRounds], rect_min[kProjectRounds], rect_size[kProjectRounds];
     int32_t radius_x[kProjectRounds], radius_y[kProjectRounds];
+    float ray_terms[kRay ? kProjectRounds : 1][10];
+    uint32_t ray_rank[kRay ? kProjectRounds : 1];
     const float its = 1.0f / static_cast<float>(p.tile_size);
 #pragma unroll
     for (int round = 0; round < kProjectRounds; ++round) {
@@ -509,7 +590,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       Projected pr;
       if (live && local < plan.g_count) {
         const int64_t g = plan.g_begin + local;
-        vis[round] = project_gaussian(p.means, p.covariances, p.opacities, g, s_cam, p.near_plane,
+        vis[round] = project_gaussian<kRay>(p.means, p.covariances, p.opacities, g, s_cam, p.near_plane,
                                       p.far_plane, p.support_sigma, p.cov_eps, p.antialiased, &pr);
         if (vis[round]) {
           const float frx = static_cast<float>(pr.radius_x);
@@ -528,6 +609,13 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           rect_size[round] = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
           radius_x[round] = pr.radius_x;
           radius_y[round] = pr.radius_y;
+          if (kRay) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) ray_terms[kRay ? round : 0][k] = pr.prec[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ray_terms[kRay ? round : 0][6 + k] = pr.prec_mean[k];
+            ray_terms[kRay ? round : 0][9] = pr.mean_prec_mean;
+          }
           float rgb[3];
           if (kShDegree < 0) {
             rgb[0] = p.features[g * p.feature_width + 0];
@@ -596,6 +684,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         s_prefix[rank] = static_cast<uint32_t>(excl > 0x7fffffffull ? 0x7fffffffull : excl);
         s_radii[rank * 2 + 0] = radius_x[round];
         s_radii[rank * 2 + 1] = radius_y[round];
+        if (kRay) ray_rank[kRay ? round : 0] = rank;
       }
       block_vis += rv;
       block_isect += rt;
@@ -631,6 +720,19 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         const uint32_t rank = i / 3;
         const uint64_t r = base_vis + rank;
         if (r < vcap) dst[r * 3 + (i - rank * 3)] = src[s_slot[rank] * 3 + (i - rank * 3)];
+      }
+      if (kRay) {
+        // Extension records: each thread writes its own visible Gaussians'.
+#pragma unroll
+        for (int round = 0; round < kProjectRounds; ++round) {
+          const uint64_t r = base_vis + ray_rank[kRay ? round : 0];
+          if (vis[round] && r < vcap) {
+            const float* t = ray_terms[kRay ? round : 0];
+            p.ray_ext[r * 3 + 0] = make_float4(t[0], t[1], t[2], t[3]);
+            p.ray_ext[r * 3 + 1] = make_float4(t[4], t[5], t[6], t[7]);
+            p.ray_ext[r * 3 + 2] = make_float4(t[8], t[9], 0.0f, 0.0f);
+          }
+        }
       }
       if (p.record_map) {
         // Training: record index of each visible (slot, Gaussian), for the
@@ -704,10 +806,15 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   }
 }
 
-template __global__ void project_emit_kernel<-1>(ProjectParams);
-template __global__ void project_emit_kernel<0>(ProjectParams);
-template __global__ void project_emit_kernel<1>(ProjectParams);
-template __global__ void project_emit_kernel<2>(ProjectParams);
-template __global__ void project_emit_kernel<3>(ProjectParams);
+template __global__ void project_emit_kernel<-1, false>(ProjectParams);
+template __global__ void project_emit_kernel<0, false>(ProjectParams);
+template __global__ void project_emit_kernel<1, false>(ProjectParams);
+template __global__ void project_emit_kernel<2, false>(ProjectParams);
+template __global__ void project_emit_kernel<3, false>(ProjectParams);
+template __global__ void project_emit_kernel<-1, true>(ProjectParams);
+template __global__ void project_emit_kernel<0, true>(ProjectParams);
+template __global__ void project_emit_kernel<1, true>(ProjectParams);
+template __global__ void project_emit_kernel<2, true>(ProjectParams);
+template __global__ void project_emit_kernel<3, true>(ProjectParams);
 
 }  // namespace vgr

@@ -62,7 +62,7 @@ int device_sms(int* sms) {
     if (cudaDeviceGetAttribute(&g_occ.sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
       return fail(VGR_ERR_CUDA, "cudaDeviceGetAttribute(MultiProcessorCount) failed");
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3, false>,
                                                   kProjectThreads, 0);
     // The onesweep partition (LBVH Morton sort) needs more than the default
     // 48 KB of dynamic shared memory.
@@ -225,6 +225,7 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   }
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   const bool ragged = cams->widths != nullptr;
+  const bool ray = opt->ray_gaussian_evaluation != 0;
   if (!ragged && (opt->height <= 0 || opt->width <= 0)) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "height and width must be positive");
   }
@@ -267,10 +268,6 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   if (opt->compact_projection_cache) {
     return fail(VGR_ERR_UNSUPPORTED, "compact_projection_cache requires tile_size=1");
   }
-  if (opt->ray_gaussian_evaluation) {
-    return fail(VGR_ERR_UNSUPPORTED,
-                "ray_gaussian_evaluation (exact-ray mode) is not provided by this build");
-  }
   if (opt->antialiased && opt->ray_gaussian_evaluation) {
     return fail(VGR_ERR_INVALID_ARGUMENT,
                 "antialiased rasterization is incompatible with exact-ray evaluation");
@@ -303,6 +300,11 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     return fail(VGR_ERR_INVALID_ARGUMENT, "output tensors must be non-null");
   }
 
+  // Exact-ray mode bins the plain form's 16-pixel tiles as 32-pixel tiles
+  // (renderer_cuda.cu:2670-2676): ray ellipses are wide, so larger bins
+  // cut duplicate keys; every pixel still sees the same records in order.
+  // The ragged form's tile offsets are the caller's, in tile_size tiles.
+  const int bin = (ray && ts == 16 && !ragged) ? 32 : ts;
   int64_t tiles_per_image = 0;
   int64_t global_tiles = 0;
   int tiles_x = 0, tiles_y = 0;
@@ -314,8 +316,8 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     global_tiles = cams->total_tiles;
     tiles_per_image = 0;
   } else {
-    tiles_x = static_cast<int>((opt->width + ts - 1) / ts);
-    tiles_y = static_cast<int>((opt->height + ts - 1) / ts);
+    tiles_x = static_cast<int>((opt->width + bin - 1) / bin);
+    tiles_y = static_cast<int>((opt->height + bin - 1) / bin);
     tiles_per_image = static_cast<int64_t>(tiles_x) * tiles_y;
     global_tiles = cams->batch * tiles_per_image;
     if (tiles_x > 65535 || tiles_y > 65535) {
@@ -407,7 +409,7 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     sp.pixel_offsets = cams->pixel_offsets;
     sp.width = static_cast<int>(opt->width);
     sp.height = static_cast<int>(opt->height);
-    sp.tile_size = ts;
+    sp.tile_size = bin;
     sp.viewmats = cams->viewmats;
     sp.intrinsics = cams->intrinsics;
     sp.env_xforms = cams->env_xforms;
@@ -443,7 +445,7 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     pp.support_sigma = static_cast<float>(opt->gaussian_support_sigma);
     pp.cov_eps = static_cast<float>(opt->covariance_epsilon);
     pp.antialiased = opt->antialiased != 0;
-    pp.tile_size = ts;
+    pp.tile_size = bin;
     pp.records = ws->records;
     pp.visible_capacity = ws->visible_capacity;
     pp.keys = ws->keys_in;
@@ -476,12 +478,24 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     int64_t pgrid = static_cast<int64_t>(sms) * g_occ.project_blocks;
     if (pgrid > vblocks) pgrid = vblocks;
     if (pgrid < 1) pgrid = 1;
-    switch (opt->sh_degree) {
-      case -1: project_emit_kernel<-1><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
-      case 0: project_emit_kernel<0><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
-      case 1: project_emit_kernel<1><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
-      case 2: project_emit_kernel<2><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
-      default: project_emit_kernel<3><<<static_cast<unsigned>(pgrid), kProjectThreads, 0, stream>>>(pp); break;
+    const unsigned pg = static_cast<unsigned>(pgrid);
+    if (ray) {
+      pp.ray_ext = static_cast<float4*>(ws->records) + ws->visible_capacity * 3;
+      switch (opt->sh_degree) {
+        case -1: project_emit_kernel<-1, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+      }
+    } else {
+      switch (opt->sh_degree) {
+        case -1: project_emit_kernel<-1, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+      }
     }
     if ((rc = check_launch("render: projection")) != VGR_OK) return rc;
     mark(2);
@@ -545,7 +559,25 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     cp.last_position = train ? train->last_position : nullptr;
     cp.persistent = opt->persistent_compositor != 0;
     const bool full = opt->full_sensor_output != 0;
-    if (train) {
+    if (ray) {
+      cp.ray_ext = static_cast<const float4*>(ws->records) + ws->visible_capacity * 3;
+      cp.intrinsics = cams->intrinsics;
+      cp.support_sigma = static_cast<float>(opt->gaussian_support_sigma);
+      const unsigned grid = static_cast<unsigned>(max_items);
+      if (bin == 32) {
+        if (full) composite_ray_kernel<32, true><<<grid, composite_threads(32), 0, stream>>>(cp);
+        else composite_ray_kernel<32, false><<<grid, composite_threads(32), 0, stream>>>(cp);
+      } else if (ts == 16) {
+        if (full) composite_ray_kernel<16, true><<<grid, composite_threads(16), 0, stream>>>(cp);
+        else composite_ray_kernel<16, false><<<grid, composite_threads(16), 0, stream>>>(cp);
+      } else if (ts == 8) {
+        if (full) composite_ray_kernel<8, true><<<grid, composite_threads(8), 0, stream>>>(cp);
+        else composite_ray_kernel<8, false><<<grid, composite_threads(8), 0, stream>>>(cp);
+      } else {
+        if (full) composite_ray_kernel<4, true><<<grid, composite_threads(4), 0, stream>>>(cp);
+        else composite_ray_kernel<4, false><<<grid, composite_threads(4), 0, stream>>>(cp);
+      }
+    } else if (train) {
       if (ts == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);
       else if (ts == 8) launch_composite<8, true, true>(cp, max_items, sms, stream);
       else launch_composite<4, true, true>(cp, max_items, sms, stream);

@@ -71,6 +71,7 @@ struct ProjectParams {
   const int32_t* gaussian_ids; // reported id of packed Gaussian g, or null (g itself)
   const float4* chunk_bounds;  // [C,2] per-chunk bounds, or null (no chunk culling)
   const int64_t* chunk_offsets;// [S+1] first chunk of each registered scene
+  float4* ray_ext;             // exact-ray mode: [V,3] extension records, else null
 };
 
 struct SortParams {
@@ -126,6 +127,10 @@ struct CompositeParams {
   float* final_transmittance;  // training: [P] transmittance after the last blended record
   int32_t* last_position;      // training: [P] sorted position one past the last blended record
   bool persistent;             // resident grid over a device work queue
+  // Exact-ray mode.
+  const float4* ray_ext;       // [V,3] (P00,P01,P02,P11), (P12,P22,Pm0,Pm1), (Pm2,mPm,-,-)
+  const float* intrinsics;     // [B,3,3]
+  float support_sigma;
 };
 
 template <int kTile>
@@ -270,7 +275,7 @@ struct ProjectBackwardParams {
 };
 
 __global__ void camera_setup_kernel(SetupParams p);
-template <int kShDegree>
+template <int kShDegree, bool kRay>
 __global__ void project_emit_kernel(ProjectParams p);
 __global__ void sort_histogram_kernel(SortParams p);
 __global__ void sort_onesweep_kernel(SortParams p);
@@ -279,6 +284,8 @@ __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
 template <int kTile, bool kFull, bool kTrain>
 __global__ void composite_kernel(CompositeParams p);
+template <int kTile, bool kFull>
+__global__ void composite_ray_kernel(CompositeParams p);
 
 __global__ void train_activate_kernel(TrainActivateParams p);
 __global__ void zero_record_grads_kernel(float4* grads, const int64_t* counters, int64_t capacity);
@@ -289,6 +296,6 @@ template <int kShDegree>
 __global__ void project_backward_kernel(ProjectBackwardParams p);
 
 // Threads per compositor CTA (two pixels per thread, 8x8-pixel warp blocks).
-constexpr int composite_threads(int tile) { return tile >= 16 ? 128 : 32; }
+constexpr int composite_threads(int tile) { return tile >= 32 ? 512 : tile >= 16 ? 128 : 32; }
 
 }  // namespace vgr

@@ -29,6 +29,9 @@ int check_train_options(const vgr_render_options* opt) {
   if (opt->antialiased) {
     return fail(VGR_ERR_UNSUPPORTED, "the differentiable form does not provide antialiased=1");
   }
+  if (opt->ray_gaussian_evaluation) {
+    return fail(VGR_ERR_UNSUPPORTED, "the differentiable form does not provide ray_gaussian_evaluation=1");
+  }
   if (opt->reuse_projection) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "the differentiable form projects every frame");
   }

@@ -194,8 +194,6 @@ class CustomCudaBackend:
                 "The dense per-pixel compact path (tile_size < 4 / compact_projection_cache) is "
                 "not provided by the B200 backend; use tile_size 4, 8 or 16."
             )
-        if ray_gaussian_evaluation:
-            raise ValueError("ray_gaussian_evaluation (exact-ray mode) is not provided by the B200 backend.")
 
         self.max_visible_records = max_visible_records
         self.max_intersections = max_intersections
@@ -207,7 +205,7 @@ class CustomCudaBackend:
         self.covariance_epsilon = covariance_epsilon
         self._rasterize_mode: Literal["classic", "antialiased"] = rasterize_mode
         self.semantic_min_alpha = semantic_min_alpha
-        self.ray_gaussian_evaluation = ray_gaussian_evaluation
+        self._ray_gaussian_evaluation = bool(ray_gaussian_evaluation)
         self.tile_size = tile_size
         self.depth_bucket_count = depth_bucket_count
         self.depth_bucket_group_size = min(depth_bucket_group_size, depth_bucket_count)
@@ -623,6 +621,12 @@ class CustomCudaBackend:
             semantic=outputs["semantic_id"].data_ptr() if full else None,
         )
         mirror = self.mirror_reference_workspace
+        record_rows = self._allocated_visible_capacity * (2 if self._ray_gaussian_evaluation else 1)
+        if ws["records"].shape[0] < record_rows:
+            # Exact-ray mode switched on after allocation: its extension
+            # records follow the records.
+            ws["records"] = torch.empty((record_rows, _native.RECORD_BYTES // 4), dtype=torch.float32,
+                                        device=self.device)
         native_ws = _native.VgrWorkspace(
             records=ws["records"].data_ptr(),
             visible_capacity=self._allocated_visible_capacity,
@@ -654,7 +658,7 @@ class CustomCudaBackend:
             covariance_epsilon=self.covariance_epsilon,
             semantic_min_alpha=self.semantic_min_alpha,
             antialiased=int(self.rasterize_mode == "antialiased"),
-            ray_gaussian_evaluation=0,
+            ray_gaussian_evaluation=int(self._ray_gaussian_evaluation),
             tile_size=self.tile_size,
             output_srgb=int(self.output_srgb),
             deterministic=int(self.deterministic),
@@ -799,7 +803,9 @@ class CustomCudaBackend:
             raise ValueError("Intersection capacity exceeds the int32 implementation limit.")
         tiles = self._global_tiles()
         specs: dict[str, tuple[tuple[int, ...], torch.dtype]] = {
-            "records": ((visible, _native.RECORD_BYTES // 4), torch.float32),
+            # Exact-ray mode stores an extension record after the records.
+            "records": ((visible * (2 if self._ray_gaussian_evaluation else 1), _native.RECORD_BYTES // 4),
+                        torch.float32),
             "keys_in": ((intersections,), torch.uint64),
             "keys_out": ((intersections,), torch.uint64),
             "values_in": ((intersections,), torch.int32),
@@ -1103,8 +1109,24 @@ class CustomCudaBackend:
     def rasterize_mode(self, value: Literal["classic", "antialiased"]) -> None:
         if value not in ("classic", "antialiased"):
             raise ValueError("rasterize_mode must be 'classic' or 'antialiased'.")
+        if value == "antialiased" and self._ray_gaussian_evaluation:
+            raise ValueError("rasterize_mode='antialiased' is incompatible with ray_gaussian_evaluation=True.")
         if value != self._rasterize_mode:
             self._rasterize_mode = value
+            self.invalidate_projection_cache()
+
+    @property
+    def ray_gaussian_evaluation(self) -> bool:
+        """Exact ray-Gaussian evaluation (renderer_cuda.cu:795-948,2190-2270)."""
+        return self._ray_gaussian_evaluation
+
+    @ray_gaussian_evaluation.setter
+    def ray_gaussian_evaluation(self, value: bool) -> None:
+        value = bool(value)
+        if value and self._rasterize_mode == "antialiased":
+            raise ValueError("rasterize_mode='antialiased' is incompatible with ray_gaussian_evaluation=True.")
+        if value != self._ray_gaussian_evaluation:
+            self._ray_gaussian_evaluation = value
             self.invalidate_projection_cache()
 
     @property

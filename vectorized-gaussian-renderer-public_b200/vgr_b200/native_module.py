@@ -50,6 +50,8 @@ WORKSPACE_TENSORS = 24
     K_COUNTERS,
     K_SORT_TEMP,
 ) = range(15)
+K_VISIBLE_RAY_PRECISIONS = 22
+K_VISIBLE_RAY_PRECISION_MEANS = 23
 
 
 def _check(cond: bool, *message: object) -> None:
@@ -261,16 +263,24 @@ def _scratch_and_records(
     sort_temp: torch.Tensor,
     need: int,
     visible_capacity: int,
+    intersection_capacity: int,
+    record_bytes: int = _native.RECORD_BYTES,
 ) -> tuple[torch.Tensor, int, int, int]:
     """Carve (scratch, records) from sort_temp, or from a cached private buffer.
 
+    A visible record covers at least one tile, so min(visible, intersection
+    capacity) records always suffice.  record_bytes is the storage per visible
+    record (twice RECORD_BYTES in exact-ray mode, whose extension records
+    follow the records).
     Returns (storage, scratch_bytes, records_offset, record_capacity).
     """
+    records = max(1, min(visible_capacity, intersection_capacity))
     aligned = (need + 255) // 256 * 256
     available = sort_temp.numel() - aligned
-    if available >= _native.RECORD_BYTES:
-        return sort_temp, need, aligned, min(visible_capacity, available // _native.RECORD_BYTES)
-    size = aligned + visible_capacity * _native.RECORD_BYTES
+    if available >= records * record_bytes:
+        return sort_temp, need, aligned, records
+    visible_capacity = records
+    size = aligned + visible_capacity * record_bytes
     key = (sort_temp.device, size)
     storage = _private_scratch.get(key)
     if storage is None:
@@ -400,13 +410,22 @@ def render(
     )
     _check(workspace[K_COUNTERS].numel() >= 5, "counters workspace must contain at least five int64 values")
 
-    tiles_x = -(-width // tile_size)
-    tiles_y = -(-height // tile_size)
+    # Exact-ray mode bins 16-pixel tiles as 32-pixel tiles (renderer_cuda.cu:2670-2676).
+    bin_tile = 32 if ray_gaussian_evaluation and tile_size == 16 else tile_size
+    tiles_x = -(-width // bin_tile)
+    tiles_y = -(-height // bin_tile)
     global_tiles = batch * tiles_x * tiles_y
     visible_capacity = workspace[K_VISIBLE_DEPTHS].numel()
     intersection_capacity = workspace[K_KEYS_IN].numel()
     _check(visible_capacity > 0, "visible capacity must be positive")
     _check(intersection_capacity > 0, "intersection capacity must be positive")
+    if ray_gaussian_evaluation:
+        # Workspace contract of the exact-ray path (renderer_cuda.cu:2721-2730);
+        # this build keeps the precision terms in its own extension records.
+        _check(workspace[K_VISIBLE_RAY_PRECISIONS].numel() >= visible_capacity * 6,
+               "visible ray-precision workspace is too small")
+        _check(workspace[K_VISIBLE_RAY_PRECISION_MEANS].numel() >= visible_capacity * 4,
+               "visible ray precision-mean workspace is too small")
 
     lib = _native.load_library()
     need = _native.check_size(
@@ -419,7 +438,8 @@ def render(
         "render scratch",
     )
     storage, scratch_bytes, records_offset, record_capacity = _scratch_and_records(
-        workspace[K_SORT_TEMP], need, visible_capacity
+        workspace[K_SORT_TEMP], need, visible_capacity, intersection_capacity,
+        _native.RECORD_BYTES * (2 if ray_gaussian_evaluation else 1),
     )
     mirror = (
         workspace[K_VISIBLE_MEANS2D].numel() >= 2 * record_capacity

@@ -133,7 +133,7 @@ class RaggedBatch:
             "ragged render scratch",
         )
         self.workspace = {
-            "records": torch.empty((visible, 12), device=dev, dtype=torch.float32),
+            "records": torch.empty((self._record_rows(visible), 12), device=dev, dtype=torch.float32),
             "keys_in": torch.empty((intersections,), device=dev, dtype=torch.uint64),
             "keys_out": torch.empty((intersections,), device=dev, dtype=torch.uint64),
             "values_in": torch.empty((intersections,), device=dev, dtype=torch.int32),
@@ -145,6 +145,10 @@ class RaggedBatch:
         }
         self._visible_capacity = visible
         self._intersection_capacity = intersections
+
+    def _record_rows(self, visible: int) -> int:
+        # Exact-ray mode stores an extension record after the records.
+        return visible * (2 if self.backend.ray_gaussian_evaluation else 1)
 
     def reserve(self, *, visible_records: int, tile_intersections: int) -> None:
         """Allocate the workspace for at least these counts (no render)."""
@@ -180,6 +184,9 @@ class RaggedBatch:
         b = self.backend
         lib = _native.load_library()
         ws = self.workspace
+        if ws["records"].shape[0] < self._record_rows(self._visible_capacity):
+            ws["records"] = torch.empty((self._record_rows(self._visible_capacity), 12), device=self.device,
+                                        dtype=torch.float32)
         scene = b.native_scene()
         cams = _native.VgrCameras(
             viewmats=viewmats.data_ptr(),
@@ -226,6 +233,7 @@ class RaggedBatch:
             covariance_epsilon=b.covariance_epsilon,
             semantic_min_alpha=b.semantic_min_alpha,
             antialiased=int(b.rasterize_mode == "antialiased"),
+            ray_gaussian_evaluation=int(b.ray_gaussian_evaluation),
             tile_size=self.tile_size,
             output_srgb=int(b.output_srgb),
             deterministic=int(b.deterministic),
