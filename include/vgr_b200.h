@@ -131,7 +131,19 @@ typedef struct vgr_workspace {
   int32_t* visible_camera_ids;   /* [V] */
   int32_t* visible_gaussian_ids; /* [V] */
   int32_t* visible_radii;        /* [V,2] */
+  /* Dense mode (tile_size 1) only, else NULL: optical-thickness bounds by
+   * depth bucket per 4x4-pixel cell, and the depth cutoff per 16-pixel tile. */
+  float* depth_tau;              /* [B * ceil(H/4) * ceil(W/4) * VGR_DENSE_DEPTH_BUCKETS],
+                                  * 16-byte aligned */
+  int64_t depth_tau_capacity;    /* elements */
+  int32_t* tile_cutoff;          /* [T16] */
+  int64_t tile_cutoff_capacity;  /* elements */
 } vgr_workspace;
+
+/* Depth buckets of dense mode's optical-thickness cutoff (16 per octave of
+ * depth above near_plane). */
+#define VGR_DENSE_DEPTH_BUCKETS 256
+#define VGR_DENSE_CELL 4
 
 typedef struct vgr_render_options {
   int64_t height;                 /* plain-form resolution */
@@ -144,13 +156,15 @@ typedef struct vgr_render_options {
   int32_t antialiased;
   int32_t ray_gaussian_evaluation; /* exact ray-Gaussian evaluation (renderer_cuda.cu:795-948,
                                     * 2190-2270); records doubles; not with antialiased */
-  int32_t tile_size;               /* 4, 8 or 16 */
+  int32_t tile_size;               /* 4, 8 or 16; 1 = dense mode (the reference's per-pixel
+                                    * path): 16-pixel tiles with an optical-thickness depth
+                                    * cutoff (renderer_cuda.cu:1093-1400,1658-1689) */
   int32_t output_srgb;
   int32_t deterministic;           /* accepted; ordering is always deterministic */
   int32_t full_sensor_output;
   int32_t fixed_capacity_sort;     /* accepted; the sort is always device-bounded */
   int32_t reuse_projection;        /* composite only, from the last sorted lists */
-  int32_t compact_projection_cache;/* must be 0 (dense 1x1 path is not built) */
+  int32_t compact_projection_cache;/* tile_size 1 only; dense mode always projects twice */
   int32_t sh_degree;               /* -1: features[0..2] are linear RGB (reference);
                                       0..3: real spherical harmonics, [G,(d+1)^2*3] */
   int32_t sorted_buffer_hint;      /* reuse_projection: 1 if sorted data lives in *_out */

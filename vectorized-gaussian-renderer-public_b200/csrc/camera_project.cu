@@ -477,10 +477,59 @@ __device__ __forceinline__ bool chunk_outside_frustum(const CamConst& c, float4 
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// Dense mode: optical-thickness depth cutoff (renderer_cuda.cu:247-258,
+// 1093-1300, 1658-1689, restructured per tile).  The compositor stops a pixel
+// once its transmittance reaches 1e-4, i.e. once sum(-ln(1 - alpha)) >= ln 1e4.
+// Pass 1 adds, for every (record, tile) of the cover, a lower bound of the
+// record's optical thickness that holds at every pixel of the tile to the
+// tile's depth bucket; a tile's cutoff is the first bucket where the bound
+// reaches ln 1e4, and pass 2 emits no key behind it.  Every pixel of the tile
+// has terminated before the first culled record, so the images are those of
+// the plain path, bit for bit.
+// ---------------------------------------------------------------------------
+
+// 0.999 * sum_{k=1..8} a^k / k, a lower bound of -ln(1 - a) (the series of
+// -ln(1 - a) has positive terms; the factor absorbs float rounding).
+__device__ __forceinline__ float conservative_tau(float a) {
+  float term = a, sum = a;
+#pragma unroll
+  for (int k = 2; k <= 8; ++k) {
+    term *= a;
+    sum += term * (1.0f / static_cast<float>(k));
+  }
+  return sum * 0.999f;
+}
+
+// Lower bound of the compositor's alpha over the pixel centres [x0, x1] x
+// [y0, y1]: the conic's quadratic form is convex, so its maximum over the box
+// is at a corner; a relative and absolute margin covers the compositor's own
+// rounding of q and exp.  0 when some pixel may fall below 1/255 or past the
+// power >= -20 cut.
+__device__ __forceinline__ float tile_alpha_lower_bound(float mx, float my, float c0, float c1,
+                                                        float c2, float o, float x0, float x1,
+                                                        float y0, float y1) {
+  float qmax = 0.0f;
+#pragma unroll
+  for (int corner = 0; corner < 4; ++corner) {
+    const float dx = ((corner & 1) ? x1 : x0) - mx;
+    const float dy = ((corner & 2) ? y1 : y0) - my;
+    const float t0 = c0 * dx * dx, t1 = 2.0f * c1 * dx * dy, t2 = c2 * dy * dy;
+    const float q = t0 + t1 + t2 + 1.0e-5f * (fabsf(t0) + fabsf(t1) + fabsf(t2)) + 1.0e-4f;
+    qmax = fmaxf(qmax, q);
+  }
+  const float power = -0.5f * qmax;
+  if (!(power >= -20.0f)) return 0.0f;
+  const float a = fminf(kMaxAlpha, o * vexp(power) * 0.99999f);
+  return a >= kAlphaThreshold * 1.0001f ? a : 0.0f;
+}
+
 // kRay: exact-ray records (renderer_cuda.cu:795-948) - no early or chunk
 // frustum cull (the ellipse cull decides), and each record's precision terms
 // go to the extension records p.ray_ext[3 r .. 3 r + 2].
-template <int kShDegree, bool kRay>
+// kMode (ProjectMode): plain fused projection + emission, or one of the two
+// dense-mode passes.
+template <int kShDegree, bool kRay, int kMode>
 __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
   __shared__ uint16_t s_slot[kProjectChunk];       // rank -> task slot
@@ -604,6 +653,58 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           const int ntx = max(0, max_tx - min_tx);
           const int nty = max(0, max_ty - min_ty);
           ntiles[round] = static_cast<uint32_t>(ntx) * static_cast<uint32_t>(nty);
+          if (kMode == kProjectDenseTau) {
+            // Pass 1: optical-thickness lower bounds into the record's depth
+            // bucket of the kDenseSubtile cells inside its core, the box of
+            // the ellipse where alpha >= kDenseMinAlpha; nothing is emitted.
+            // Leaving the fainter rim out only lowers the bounds.
+            const int bucket = dense_bucket(pr.depth, p.near_bits);
+            const float qc = 2.0f * __logf(pr.opacity * (1.0f / kDenseMinAlpha));
+            const int64_t sub_base = static_cast<int64_t>(plan.camera) * p.sub_x * p.sub_y;
+            constexpr float kCell = static_cast<float>(kDenseSubtile);
+            const float hx = qc > 0.0f ? sqrtf(qc * pr.cov_a) : -1.0f;
+            const float hy = qc > 0.0f ? sqrtf(qc * pr.cov_c) : -1.0f;
+            // Cells whose pixel centres [4s + 0.5, 4s + 3.5] lie in the box.
+            const int sx0 = max(0, ceil_clamped((pr.mean_x - hx - 0.5f) * (1.0f / kCell)));
+            const int sx1 = min(p.sub_x - 1, floor_clamped((pr.mean_x + hx - 3.5f) * (1.0f / kCell)));
+            const int sy0 = max(0, ceil_clamped((pr.mean_y - hy - 0.5f) * (1.0f / kCell)));
+            const int sy1 = min(p.sub_y - 1, floor_clamped((pr.mean_y + hy - 3.5f) * (1.0f / kCell)));
+            for (int sy = sy0; hy >= 0.0f && sy <= sy1; ++sy) {
+              const float y0 = static_cast<float>(sy) * kCell + 0.5f;
+              const float y1 = fminf(y0 + kCell - 1.0f, static_cast<float>(plan.height) - 0.5f);
+              for (int sx = sx0; sx <= sx1; ++sx) {
+                const float x0 = static_cast<float>(sx) * kCell + 0.5f;
+                const float x1 = fminf(x0 + kCell - 1.0f, static_cast<float>(plan.width) - 0.5f);
+                const float a = tile_alpha_lower_bound(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1,
+                                                       pr.conic2, pr.opacity, x0, x1, y0, y1);
+                if (a > 0.0f) {
+                  const int64_t cell = sub_base + static_cast<int64_t>(sy) * p.sub_x + sx;
+                  atomicAdd(p.depth_tau + cell * kDenseBuckets + bucket, conservative_tau(a));
+                }
+              }
+            }
+            vis[round] = false;
+            ntiles[round] = 0;
+          } else if (kMode == kProjectDenseCull) {
+            // Pass 2: only the tiles whose cutoff bucket is not in front of
+            // the record; a record left with none is not emitted.
+            const int bucket = dense_bucket(pr.depth, p.near_bits);
+            uint32_t kept = 0;
+            for (int ty = min_ty; ty < min_ty + nty; ++ty) {
+              const int64_t row = plan.tile_base + static_cast<int64_t>(ty) * plan.tiles_x;
+              for (int tx = min_tx; tx < min_tx + ntx; ++tx) kept += bucket <= p.tile_cutoff[row + tx];
+            }
+            ntiles[round] = kept;
+            if (kept == 0) vis[round] = false;
+          }
+        }
+        if (vis[round]) {
+          const float frx = static_cast<float>(pr.radius_x);
+          const float fry = static_cast<float>(pr.radius_y);
+          const int min_tx = max(0, floor_clamped(fsub(fmul(pr.mean_x, its), fmul(frx, its))));
+          const int min_ty = max(0, floor_clamped(fsub(fmul(pr.mean_y, its), fmul(fry, its))));
+          const int ntx = max(0, min(plan.tiles_x, ceil_clamped(fadd(fmul(pr.mean_x, its), fmul(frx, its)))) - min_tx);
+          const int nty = max(0, min(plan.tiles_y, ceil_clamped(fadd(fmul(pr.mean_y, its), fmul(fry, its)))) - min_ty);
           rect_min[round] = static_cast<uint32_t>(min(min_tx, 65535)) |
                             (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
           rect_size[round] = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
@@ -771,7 +872,39 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         limit = room < nisect ? room : nisect;
       }
       const int64_t tiles_x = plan.tiles_x;
-      for (uint32_t j = tid; j < limit; j += kProjectThreads) {
+      if (kMode == kProjectDenseCull) {
+        // Dense mode: each record's kept tiles in rect order, one thread per
+        // record (the kept tiles are not a dense range of the rect).
+        for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
+          const uint64_t r = base_vis + i;
+          const float depth = s_rec[s_slot[i]].b.z;
+          const int bucket = dense_bucket(depth, p.near_bits);
+          const uint32_t ntx = s_rect_size[i] & 0xffffu;
+          const uint32_t nty = s_rect_size[i] >> 16;
+          const uint32_t min_tx = s_rect_min[i] & 0xffffu;
+          const uint32_t min_ty = s_rect_min[i] >> 16;
+          uint32_t j = s_prefix[i];
+          for (uint32_t ty = min_ty; ty < min_ty + nty; ++ty) {
+            for (uint32_t tx = min_tx; tx < min_tx + ntx; ++tx) {
+              const uint64_t tile = static_cast<uint64_t>(plan.tile_base) + static_cast<uint64_t>(ty) * tiles_x + tx;
+              if (bucket > p.tile_cutoff[tile]) continue;
+              if (j < limit) {
+                uint64_t key = ~0ull;
+                int32_t value = 0;
+                if (r < vcap) {
+                  key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(depth));
+                  value = static_cast<int32_t>(r);
+                  if (tile < static_cast<uint64_t>(p.tile_count)) atomicAdd(p.tile_counts + tile, 1u);
+                }
+                p.keys[base_isect + j] = key;
+                p.values[base_isect + j] = value;
+              }
+              ++j;
+            }
+          }
+        }
+      }
+      for (uint32_t j = tid; j < limit && kMode != kProjectDenseCull; j += kProjectThreads) {
         // Owner record: last i with s_prefix[i] <= j.
         uint32_t lo = 0, hi = nvis;  // invariant s_prefix[lo] <= j < s_prefix[hi]
         while (hi - lo > 1) {
@@ -806,15 +939,66 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   }
 }
 
-template __global__ void project_emit_kernel<-1, false>(ProjectParams);
-template __global__ void project_emit_kernel<0, false>(ProjectParams);
-template __global__ void project_emit_kernel<1, false>(ProjectParams);
-template __global__ void project_emit_kernel<2, false>(ProjectParams);
-template __global__ void project_emit_kernel<3, false>(ProjectParams);
-template __global__ void project_emit_kernel<-1, true>(ProjectParams);
-template __global__ void project_emit_kernel<0, true>(ProjectParams);
-template __global__ void project_emit_kernel<1, true>(ProjectParams);
-template __global__ void project_emit_kernel<2, true>(ProjectParams);
-template __global__ void project_emit_kernel<3, true>(ProjectParams);
+#define VGR_PROJECT_VARIANTS(RAY, MODE)                                   \
+  template __global__ void project_emit_kernel<-1, RAY, MODE>(ProjectParams); \
+  template __global__ void project_emit_kernel<0, RAY, MODE>(ProjectParams);  \
+  template __global__ void project_emit_kernel<1, RAY, MODE>(ProjectParams);  \
+  template __global__ void project_emit_kernel<2, RAY, MODE>(ProjectParams);  \
+  template __global__ void project_emit_kernel<3, RAY, MODE>(ProjectParams);
+VGR_PROJECT_VARIANTS(false, kProjectPlain)
+VGR_PROJECT_VARIANTS(true, kProjectPlain)
+VGR_PROJECT_VARIANTS(false, kProjectDenseTau)
+VGR_PROJECT_VARIANTS(false, kProjectDenseCull)
+#undef VGR_PROJECT_VARIANTS
+
+// Depth cutoff (renderer_cuda.cu:1658-1689): one warp per cell scans its
+// kDenseBuckets optical-thickness bounds (8 per lane) for the first bucket
+// where the running sum reaches ln 1e4 (the compositor's T <= 1e-4 stop), or
+// the last bucket; a tile's cutoff is the largest of its cells'.  Thread 0
+// of block 0 also rewinds the projection ticket for the second pass.
+__global__ void __launch_bounds__(256) dense_cutoff_kernel(DenseCutoffParams p) {
+  constexpr float kStopTau = 9.210340371976184f;  // ln(1e4)
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header)->project_queue = 0u;
+  }
+  const int lane = threadIdx.x & 31;
+  const int64_t cell = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (cell >= p.sub_count) return;
+  const float4* row = reinterpret_cast<const float4*>(p.depth_tau + cell * kDenseBuckets) + lane * 2;
+  const float4 a = row[0], b = row[1];
+  const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  float local = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) local += v[k];
+  float incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float n = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += n;
+  }
+  int first = kDenseBuckets;
+  if (incl >= kStopTau) {
+    float run = incl - local;
+    for (int k = 0; k < 8; ++k) {
+      run += v[k];
+      if (run >= kStopTau) {
+        first = lane * 8 + k;
+        break;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+  if (lane == 0) {
+    const int64_t per_image = static_cast<int64_t>(p.sub_x) * p.sub_y;
+    const int64_t image = cell / per_image;
+    const int64_t local = cell - image * per_image;
+    const int sy = static_cast<int>(local / p.sub_x);
+    const int sx = static_cast<int>(local - static_cast<int64_t>(sy) * p.sub_x);
+    const int per_tile = p.tile_size / kDenseSubtile;
+    const int64_t tile = image * p.tiles_per_image + static_cast<int64_t>(sy / per_tile) * p.tiles_x + sx / per_tile;
+    atomicMax(p.tile_cutoff + tile, first < kDenseBuckets ? first : kDenseBuckets - 1);
+  }
+}
 
 }  // namespace vgr

@@ -33,6 +33,8 @@ thread_local OccupancyCache g_occ;
 }  // namespace
 
 static_assert(vgr::kProjectChunk == VGR_PROJECT_CHUNK, "projection chunk of the C ABI");
+static_assert(vgr::kDenseBuckets == VGR_DENSE_DEPTH_BUCKETS, "dense depth buckets of the C ABI");
+static_assert(vgr::kDenseSubtile == VGR_DENSE_CELL, "dense optical-thickness cell of the C ABI");
 
 namespace vgr {
 
@@ -62,7 +64,7 @@ int device_sms(int* sms) {
     if (cudaDeviceGetAttribute(&g_occ.sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
       return fail(VGR_ERR_CUDA, "cudaDeviceGetAttribute(MultiProcessorCount) failed");
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3, false>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ.project_blocks, project_emit_kernel<3, false, kProjectPlain>,
                                                   kProjectThreads, 0);
     // The onesweep partition (LBVH Morton sort) needs more than the default
     // 48 KB of dynamic shared memory.
@@ -259,14 +261,14 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   if (ts <= 0 || ts > 16 || (ts & (ts - 1)) != 0) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "tile_size must be a power of two in [1, 16]");
   }
-  if (ts < 4) {
-    return fail(VGR_ERR_UNSUPPORTED,
-                "tile_size=%d selects the dense per-pixel path, which this build does not provide; "
-                "use tile_size 4, 8 or 16",
-                ts);
+  if (ts == 2) {
+    return fail(VGR_ERR_UNSUPPORTED, "tile_size=2 is not provided; use 1 (dense mode), 4, 8 or 16");
   }
-  if (opt->compact_projection_cache) {
-    return fail(VGR_ERR_UNSUPPORTED, "compact_projection_cache requires tile_size=1");
+  if (opt->compact_projection_cache && ts != 1) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "compact_projection_cache requires tile_size=1");
+  }
+  if (opt->compact_projection_cache && opt->ray_gaussian_evaluation) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "compact_projection_cache supports only screen-space evaluation");
   }
   if (opt->antialiased && opt->ray_gaussian_evaluation) {
     return fail(VGR_ERR_INVALID_ARGUMENT,
@@ -304,7 +306,20 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   // (renderer_cuda.cu:2670-2676): ray ellipses are wide, so larger bins
   // cut duplicate keys; every pixel still sees the same records in order.
   // The ragged form's tile offsets are the caller's, in tile_size tiles.
-  const int bin = (ray && ts == 16 && !ragged) ? 32 : ts;
+  // Dense mode (tile_size 1, the reference's per-pixel path) runs on
+  // 16-pixel tiles with the optical-thickness depth cutoff; each pixel sees
+  // the same records in the same order, so images equal the plain path's.
+  const bool dense = ts == 1;
+  if (dense && (ray || ragged || train)) {
+    return fail(VGR_ERR_UNSUPPORTED,
+                "dense mode (tile_size=1) is provided for the plain screen-space forward render");
+  }
+  if (dense && !opt->reuse_projection &&
+      (!ws->depth_tau || !ws->tile_cutoff || (reinterpret_cast<uintptr_t>(ws->depth_tau) & 15) != 0)) {
+    return fail(VGR_ERR_INVALID_ARGUMENT,
+                "dense mode needs depth_tau (16-byte aligned) and tile_cutoff workspaces");
+  }
+  const int bin = dense ? 16 : (ray && ts == 16 && !ragged) ? 32 : ts;
   int64_t tiles_per_image = 0;
   int64_t global_tiles = 0;
   int tiles_x = 0, tiles_y = 0;
@@ -479,22 +494,68 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     if (pgrid > vblocks) pgrid = vblocks;
     if (pgrid < 1) pgrid = 1;
     const unsigned pg = static_cast<unsigned>(pgrid);
-    if (ray) {
+    if (dense) {
+      const int sub_x = static_cast<int>((opt->width + kDenseSubtile - 1) / kDenseSubtile);
+      const int sub_y = static_cast<int>((opt->height + kDenseSubtile - 1) / kDenseSubtile);
+      const int64_t cells = cams->batch * sub_x * sub_y;
+      if (ws->depth_tau_capacity < cells * kDenseBuckets || ws->tile_cutoff_capacity < global_tiles) {
+        return fail(VGR_ERR_INVALID_ARGUMENT, "dense-mode workspaces are too small for the pixel grid");
+      }
+      if (cells > 0 &&
+          (cudaMemsetAsync(ws->depth_tau, 0, static_cast<size_t>(cells) * kDenseBuckets * 4, stream) != cudaSuccess ||
+           cudaMemsetAsync(ws->tile_cutoff, 0, static_cast<size_t>(global_tiles) * 4, stream) != cudaSuccess)) {
+        return check_launch("render: clear depth buckets", 0);
+      }
+      pp.depth_tau = ws->depth_tau;
+      pp.tile_cutoff = ws->tile_cutoff;
+      pp.sub_x = sub_x;
+      pp.sub_y = sub_y;
+      pp.near_bits = [](float f) { uint32_t u; memcpy(&u, &f, 4); return u; }(near_f);
+      switch (opt->sh_degree) {
+        case -1: project_emit_kernel<-1, false, kProjectDenseTau><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, false, kProjectDenseTau><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, false, kProjectDenseTau><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, false, kProjectDenseTau><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, false, kProjectDenseTau><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+      }
+      if ((rc = check_launch("render: dense optical thickness")) != VGR_OK) return rc;
+      DenseCutoffParams dp{};
+      dp.scratch = scratch;
+      dp.layout = layout;
+      dp.depth_tau = ws->depth_tau;
+      dp.tile_cutoff = ws->tile_cutoff;
+      dp.sub_count = cells;
+      dp.sub_x = sub_x;
+      dp.sub_y = sub_y;
+      dp.tiles_x = tiles_x;
+      dp.tiles_per_image = tiles_per_image;
+      dp.tile_size = bin;
+      const int64_t cblocks = (cells * 32 + 255) / 256;
+      dense_cutoff_kernel<<<static_cast<unsigned>(cblocks > 0 ? cblocks : 1), 256, 0, stream>>>(dp);
+      if ((rc = check_launch("render: dense cutoff")) != VGR_OK) return rc;
+      switch (opt->sh_degree) {
+        case -1: project_emit_kernel<-1, false, kProjectDenseCull><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, false, kProjectDenseCull><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, false, kProjectDenseCull><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, false, kProjectDenseCull><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, false, kProjectDenseCull><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+      }
+    } else if (ray) {
       pp.ray_ext = static_cast<float4*>(ws->records) + ws->visible_capacity * 3;
       switch (opt->sh_degree) {
-        case -1: project_emit_kernel<-1, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 0: project_emit_kernel<0, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 1: project_emit_kernel<1, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 2: project_emit_kernel<2, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        default: project_emit_kernel<3, true><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case -1: project_emit_kernel<-1, true, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, true, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, true, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, true, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, true, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
       }
     } else {
       switch (opt->sh_degree) {
-        case -1: project_emit_kernel<-1, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 0: project_emit_kernel<0, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 1: project_emit_kernel<1, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        case 2: project_emit_kernel<2, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
-        default: project_emit_kernel<3, false><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case -1: project_emit_kernel<-1, false, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 0: project_emit_kernel<0, false, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 1: project_emit_kernel<1, false, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        case 2: project_emit_kernel<2, false, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
+        default: project_emit_kernel<3, false, kProjectPlain><<<pg, kProjectThreads, 0, stream>>>(pp); break;
       }
     }
     if ((rc = check_launch("render: projection")) != VGR_OK) return rc;
@@ -567,10 +628,10 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
       if (bin == 32) {
         if (full) composite_ray_kernel<32, true><<<grid, composite_threads(32), 0, stream>>>(cp);
         else composite_ray_kernel<32, false><<<grid, composite_threads(32), 0, stream>>>(cp);
-      } else if (ts == 16) {
+      } else if (bin == 16) {
         if (full) composite_ray_kernel<16, true><<<grid, composite_threads(16), 0, stream>>>(cp);
         else composite_ray_kernel<16, false><<<grid, composite_threads(16), 0, stream>>>(cp);
-      } else if (ts == 8) {
+      } else if (bin == 8) {
         if (full) composite_ray_kernel<8, true><<<grid, composite_threads(8), 0, stream>>>(cp);
         else composite_ray_kernel<8, false><<<grid, composite_threads(8), 0, stream>>>(cp);
       } else {
@@ -578,13 +639,13 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
         else composite_ray_kernel<4, false><<<grid, composite_threads(4), 0, stream>>>(cp);
       }
     } else if (train) {
-      if (ts == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);
-      else if (ts == 8) launch_composite<8, true, true>(cp, max_items, sms, stream);
+      if (bin == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);
+      else if (bin == 8) launch_composite<8, true, true>(cp, max_items, sms, stream);
       else launch_composite<4, true, true>(cp, max_items, sms, stream);
-    } else if (ts == 16) {
+    } else if (bin == 16) {
       if (full) launch_composite<16, true, false>(cp, max_items, sms, stream);
       else launch_composite<16, false, false>(cp, max_items, sms, stream);
-    } else if (ts == 8) {
+    } else if (bin == 8) {
       if (full) launch_composite<8, true, false>(cp, max_items, sms, stream);
       else launch_composite<8, false, false>(cp, max_items, sms, stream);
     } else {

@@ -72,6 +72,41 @@ struct ProjectParams {
   const float4* chunk_bounds;  // [C,2] per-chunk bounds, or null (no chunk culling)
   const int64_t* chunk_offsets;// [S+1] first chunk of each registered scene
   float4* ray_ext;             // exact-ray mode: [V,3] extension records, else null
+  // Dense mode (optical-thickness depth cutoff).
+  float* depth_tau;            // [B * sub-tiles, kDenseBuckets] optical-thickness lower bounds
+  const int32_t* tile_cutoff;  // [T] last depth bucket a tile can still blend
+  uint32_t near_bits;          // float bits of near_plane (bucket origin)
+  int sub_x, sub_y;            // sub-tile grid of one image (kDenseSubtile pixels)
+};
+
+// Projection kernel variants: the plain fused projection + emission, and the
+// two passes of dense mode (accumulate per-tile optical thickness by depth
+// bucket; then project again and emit only keys in front of each tile's
+// cutoff).
+enum ProjectMode : int { kProjectPlain = 0, kProjectDenseTau = 1, kProjectDenseCull = 2 };
+
+// Dense mode depth buckets: a monotone integer map of the depth's float bits,
+// 16 buckets per octave above near_plane (bits >> 19), clamped to 256.
+constexpr int kDenseBuckets = 256;
+constexpr int kDenseSubtile = 4;  // pixels per side of the optical-thickness cells
+constexpr float kDenseMinAlpha = 0.25f;  // cells below this alpha bound add nothing
+constexpr int kDenseBucketShift = 19;
+__device__ __forceinline__ int dense_bucket(float depth, uint32_t near_bits) {
+  const uint32_t bits = __float_as_uint(depth);
+  const uint32_t d = bits > near_bits ? (bits - near_bits) >> kDenseBucketShift : 0u;
+  return d < static_cast<uint32_t>(kDenseBuckets) ? static_cast<int>(d) : kDenseBuckets - 1;
+}
+
+struct DenseCutoffParams {
+  unsigned char* scratch;
+  ScratchLayout layout;
+  const float* depth_tau;      // [B * sub_x * sub_y, kDenseBuckets]
+  int32_t* tile_cutoff;        // [T], zeroed before the launch
+  int64_t sub_count;           // B * sub_x * sub_y
+  int sub_x, sub_y;            // sub-tiles per image row / column
+  int tiles_x;                 // tiles per image row
+  int64_t tiles_per_image;
+  int tile_size;               // pixels per tile side (a multiple of kDenseSubtile)
 };
 
 struct SortParams {
@@ -275,8 +310,9 @@ struct ProjectBackwardParams {
 };
 
 __global__ void camera_setup_kernel(SetupParams p);
-template <int kShDegree, bool kRay>
+template <int kShDegree, bool kRay, int kMode>
 __global__ void project_emit_kernel(ProjectParams p);
+__global__ void dense_cutoff_kernel(DenseCutoffParams p);
 __global__ void sort_histogram_kernel(SortParams p);
 __global__ void sort_onesweep_kernel(SortParams p);
 __global__ void tile_scan_kernel(BucketParams p);

@@ -21,6 +21,8 @@ VGR_ERR_SCRATCH_TOO_SMALL = -3
 VGR_ERR_UNSUPPORTED = -4
 RECORD_BYTES = 48
 PROJECT_CHUNK = 512
+DENSE_DEPTH_BUCKETS = 256
+DENSE_CELL = 4
 STAGE_EVENTS = 7
 
 _c_i64 = ctypes.c_int64
@@ -91,6 +93,10 @@ class VgrWorkspace(ctypes.Structure):
         ("visible_camera_ids", _c_p),
         ("visible_gaussian_ids", _c_p),
         ("visible_radii", _c_p),
+        ("depth_tau", _c_p),
+        ("depth_tau_capacity", _c_i64),
+        ("tile_cutoff", _c_p),
+        ("tile_cutoff_capacity", _c_i64),
     ]
 
 

@@ -14,9 +14,11 @@ every mode, and a workspace of 48-byte packed records instead of the
 reference's structure-of-arrays visible tensors (those can be mirrored with
 ``mirror_reference_workspace=True`` for tools that read them).
 
-Modes the reference offers that this build does not provide raise
-ValueError at construction: the dense 1x1 compact path
-(``compact_projection_cache``, ``tile_size`` < 4) and exact-ray evaluation.
+``tile_size=1`` (the reference's dense per-pixel path, with or without
+``compact_projection_cache``) selects dense mode: 16-pixel tiles whose keys
+are culled behind a per-tile optical-thickness depth cutoff, with the images
+of the plain path.  ``ray_gaussian_evaluation=True`` selects exact-ray
+evaluation.
 """
 
 from __future__ import annotations
@@ -188,12 +190,10 @@ class CustomCudaBackend:
             raise ValueError("max_workspace_bytes must be positive when set.")
         if sh_degree is not None and sh_degree not in (0, 1, 2, 3):
             raise ValueError("sh_degree must be None (linear RGB features) or in [0, 3].")
-        # Modes of the reference that this build does not provide.
-        if compact_projection_cache or tile_size < 4:
-            raise ValueError(
-                "The dense per-pixel compact path (tile_size < 4 / compact_projection_cache) is "
-                "not provided by the B200 backend; use tile_size 4, 8 or 16."
-            )
+        if tile_size == 2:
+            raise ValueError("tile_size=2 is not provided; use 1 (dense mode), 4, 8 or 16.")
+        if tile_size == 1 and ray_gaussian_evaluation:
+            raise ValueError("dense mode (tile_size=1) renders screen-space evaluation only.")
 
         self.max_visible_records = max_visible_records
         self.max_intersections = max_intersections
@@ -648,6 +648,10 @@ class CustomCudaBackend:
             visible_camera_ids=ws["visible_camera_ids"].data_ptr() if mirror else None,
             visible_gaussian_ids=ws["visible_gaussian_ids"].data_ptr() if mirror else None,
             visible_radii=ws["visible_radii"].data_ptr() if mirror else None,
+            depth_tau=ws["depth_tau"].data_ptr() if self.tile_size == 1 else None,
+            depth_tau_capacity=ws["depth_tau"].numel(),
+            tile_cutoff=ws["tile_cutoff"].data_ptr() if self.tile_size == 1 else None,
+            tile_cutoff_capacity=ws["tile_cutoff"].numel(),
         )
         options = _native.VgrRenderOptions(
             height=self._height,
@@ -665,7 +669,7 @@ class CustomCudaBackend:
             full_sensor_output=int(full),
             fixed_capacity_sort=int(self.fixed_capacity_sort),
             reuse_projection=int(reuse),
-            compact_projection_cache=0,
+            compact_projection_cache=int(self.compact_projection_cache),
             sh_degree=-1 if self.sh_degree is None else self.sh_degree,
             sorted_buffer_hint=1,
             persistent_compositor=int(self.persistent_compositor),
@@ -771,10 +775,18 @@ class CustomCudaBackend:
         return counters
 
     # ----------------------------------------------------------------- workspace
+    def _dense_cells(self) -> int:
+        """Optical-thickness cells of dense mode (4x4 pixels) over the batch."""
+        assert self._workspace_config is not None
+        physical, height, width, _ = self._workspace_config
+        cell = _native.DENSE_CELL
+        return physical * math.ceil(height / cell) * math.ceil(width / cell)
+
     def _global_tiles(self) -> int:
         assert self._workspace_config is not None
         physical, height, width, _ = self._workspace_config
-        return physical * math.ceil(height / self.tile_size) * math.ceil(width / self.tile_size)
+        bin_size = self.bin_tile_size
+        return physical * math.ceil(height / bin_size) * math.ceil(width / bin_size)
 
     def _scratch_bytes(self, intersections: int, active: int) -> int:
         lib = _native.load_library()
@@ -810,6 +822,11 @@ class CustomCudaBackend:
             "keys_out": ((intersections,), torch.uint64),
             "values_in": ((intersections,), torch.int32),
             "values_out": ((intersections,), torch.int32),
+            # Dense mode: optical-thickness bounds per (tile, depth bucket) and
+            # the per-tile depth cutoff.
+            "depth_tau": ((self._dense_cells() * _native.DENSE_DEPTH_BUCKETS if self.tile_size == 1 else 1,),
+                          torch.float32),
+            "tile_cutoff": ((tiles if self.tile_size == 1 else 1,), torch.int32),
             "tile_starts": ((tiles,), torch.int32),
             "tile_ends": ((tiles,), torch.int32),
             "counters": ((len(COUNTER_NAMES),), torch.int64),
@@ -1092,6 +1109,13 @@ class CustomCudaBackend:
 
     @property
     def bin_tile_size(self) -> int:
+        """Pixel size of the tiles keys are binned in: dense mode (tile_size 1)
+        runs on 16-pixel tiles with its depth cutoff; exact-ray mode bins
+        16-pixel tiles as 32 (renderer_cuda.cu:2670-2676)."""
+        if self.tile_size == 1:
+            return 16
+        if self._ray_gaussian_evaluation and self.tile_size == 16:
+            return 32
         return self.tile_size
 
     @property
@@ -1125,9 +1149,16 @@ class CustomCudaBackend:
         value = bool(value)
         if value and self._rasterize_mode == "antialiased":
             raise ValueError("rasterize_mode='antialiased' is incompatible with ray_gaussian_evaluation=True.")
+        if value and self.tile_size == 1:
+            raise ValueError("dense mode (tile_size=1) renders screen-space evaluation only.")
         if value != self._ray_gaussian_evaluation:
+            tiles_before = self._global_tiles() if self._workspace_config is not None else None
             self._ray_gaussian_evaluation = value
             self.invalidate_projection_cache()
+            if tiles_before is not None and self._global_tiles() != tiles_before and self.workspace:
+                # The tile grid changed (16-pixel tiles bin as 32 in exact-ray mode).
+                self._install_workspace(self._allocated_visible_capacity, self._allocated_intersection_capacity,
+                                        reason="ray-mode-switch")
 
     @property
     def capacity_stats(self) -> dict[str, Any]:

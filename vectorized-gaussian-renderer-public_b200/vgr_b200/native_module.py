@@ -257,6 +257,16 @@ def aggregate_chunk_counters(
 
 
 _private_scratch: dict[tuple[torch.device, int], torch.Tensor] = {}
+_private_buffers: dict[tuple, torch.Tensor] = {}
+
+
+def _private_buffer(key: tuple, numel: int, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
+    """A cached device buffer of at least ``numel`` elements."""
+    buf = _private_buffers.get(key)
+    if buf is None or buf.numel() < numel or buf.dtype != dtype:
+        buf = torch.empty((max(numel, 1),), dtype=dtype, device=device)
+        _private_buffers[key] = buf
+    return buf
 
 
 def _scratch_and_records(
@@ -410,8 +420,11 @@ def render(
     )
     _check(workspace[K_COUNTERS].numel() >= 5, "counters workspace must contain at least five int64 values")
 
-    # Exact-ray mode bins 16-pixel tiles as 32-pixel tiles (renderer_cuda.cu:2670-2676).
-    bin_tile = 32 if ray_gaussian_evaluation and tile_size == 16 else tile_size
+    # Exact-ray mode bins 16-pixel tiles as 32-pixel tiles (renderer_cuda.cu:2670-2676);
+    # dense mode (tile_size 1) runs on 16-pixel tiles with its depth cutoff.
+    _check(not (tile_size == 1 and ray_gaussian_evaluation),
+           "dense mode (tile_size=1) renders screen-space evaluation only in this build")
+    bin_tile = 32 if ray_gaussian_evaluation and tile_size == 16 else 16 if tile_size == 1 else tile_size
     tiles_x = -(-width // bin_tile)
     tiles_y = -(-height // bin_tile)
     global_tiles = batch * tiles_x * tiles_y
@@ -479,6 +492,14 @@ def render(
         semantic=_ptr(semantic) if full_sensor_output else None,
     )
     base = storage.data_ptr()
+    depth_tau = tile_cutoff = None
+    if tile_size == 1:
+        # The reference aliases its depth-bucket workspace with sort_temp,
+        # which holds this build's records and scratch: private buffers.
+        cells = batch * -(-height // _native.DENSE_CELL) * -(-width // _native.DENSE_CELL)
+        depth_tau = _private_buffer(("depth_tau", means.device), cells * _native.DENSE_DEPTH_BUCKETS,
+                                    torch.float32, means.device)
+        tile_cutoff = _private_buffer(("tile_cutoff", means.device), global_tiles, torch.int32, means.device)
     native_workspace = _native.VgrWorkspace(
         records=base + records_offset,
         visible_capacity=record_capacity,
@@ -500,6 +521,10 @@ def render(
         visible_camera_ids=_ptr(workspace[K_VISIBLE_CAMERA_IDS]) if mirror else None,
         visible_gaussian_ids=_ptr(workspace[K_VISIBLE_GAUSSIAN_IDS]) if mirror else None,
         visible_radii=_ptr(workspace[K_VISIBLE_RADII]) if mirror else None,
+        depth_tau=None if depth_tau is None else depth_tau.data_ptr(),
+        depth_tau_capacity=0 if depth_tau is None else depth_tau.numel(),
+        tile_cutoff=None if tile_cutoff is None else tile_cutoff.data_ptr(),
+        tile_cutoff_capacity=0 if tile_cutoff is None else tile_cutoff.numel(),
     )
     options = _native.VgrRenderOptions(
         height=height,
