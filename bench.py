@@ -77,6 +77,8 @@ def parse_args() -> argparse.Namespace:
                         help="frames of the ragged-batch workload (0: skip)")
     parser.add_argument("--aux-steps", type=int, default=10,
                         help="timed steps of PLY ingestion and the hybrid compositor (0: skip)")
+    parser.add_argument("--mode-steps", type=int, default=5,
+                        help="frames per dense-mode / exact-ray measurement (0 skips)")
     parser.add_argument("--diff-steps", type=int, default=10,
                         help="timed steps of the differentiable-form workload (0: skip)")
     parser.add_argument("--ragged-scale", type=float, default=1.0,
@@ -422,6 +424,61 @@ def run_aux(args, device, world: int) -> dict:
                              "achieved_gbs": round(hyb_bytes / (hyb_ms / 1e3) / 1e9, 1),
                              "frac_of_hbm": round(hyb_bytes / (hyb_ms / 1e3) / 1e9 / peak, 4)},
         "peak_gbs": peak, "peak_source": peak_source,
+    }
+
+
+def run_modes(args, device) -> dict:
+    """The two alternative evaluation modes against the plain path, device
+    time per frame with a fresh projection each frame (projection cache off):
+    dense mode (tile_size=1, optical-thickness depth cutoff) on a deep scene
+    (2M fairly opaque Gaussians, 32 cameras 320x240 orbiting inside the
+    cloud's depth range, ~90% of tile keys hidden behind saturated pixels),
+    and exact-ray evaluation on the batched 1M-Gaussian SH3 workload."""
+    from vgr_b200 import CustomCudaBackend, RendererService
+    from vgr_b200.workloads import batched_workload, orbit_cameras, synthetic_scene
+
+    steps = max(args.mode_steps, 1)
+
+    def frame_ms(scene, rig, **kw):
+        backend = CustomCudaBackend(output_srgb=False, enable_projection_cache=False, **kw)
+        svc = RendererService(backend, height=rig.height, width=rig.width, max_views=rig.viewmats.shape[0])
+        svc.initialize(stage=None, device=device)
+        svc.load_scene(1, **scene.to(device).as_kwargs())
+        vm, k = rig.viewmats.to(device), rig.intrinsics.to(device)
+        ids = torch.ones((vm.shape[0],), dtype=torch.int64, device=device)
+        for _ in range(3):
+            svc.render(vm, k, ids)
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(steps):
+            svc.render(vm, k, ids)
+        stop.record()
+        torch.cuda.synchronize(device)
+        counters = backend.read_counters()
+        out = {"ms": round(start.elapsed_time(stop) / steps, 3),
+               "mpix_per_s": round(rig.viewmats.shape[0] * rig.height * rig.width
+                                   / (start.elapsed_time(stop) / steps / 1e3) / 1e6, 1),
+               "visible_records": counters["visible_gaussians"], "tile_keys": counters["tile_intersections"]}
+        svc.shutdown()
+        return out
+
+    deep = synthetic_scene(2_000_000, seed=7, mean_half_extent=2.0, log_scale_mean=-3.0)
+    deep.opacities.clamp_(min=0.5)
+    deep_rig = orbit_cameras(32, seed=3, radius=6.0, width=320, height=240, focal=260.0)
+    plain = frame_ms(deep, deep_rig, tile_size=16)
+    dense = frame_ms(deep, deep_rig, tile_size=1)
+    del deep
+    scene, rig = batched_workload()
+    screen = frame_ms(scene, rig, tile_size=16, sh_degree=3)
+    ray = frame_ms(scene, rig, tile_size=16, sh_degree=3, ray_gaussian_evaluation=True)
+    return {
+        "dense_mode": {"workload": "deep-2m-32x320x240 (2M Gaussians, opacity >= 0.5, 32 cameras)",
+                       "plain_tile16": plain, "dense_tile1": dense,
+                       "speedup": round(plain["ms"] / dense["ms"], 3)},
+        "exact_ray": {"workload": "batched-1m-sh3 (64 cameras 640x480)", "screen_space": screen,
+                      "exact_ray": ray, "ray_over_screen_time": round(ray["ms"] / screen["ms"], 3)},
+        "steps": steps,
     }
 
 
@@ -911,6 +968,7 @@ def run_b200(args) -> None:
         lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     aux = run_aux(args, device, world) if args.aux_steps > 0 else None
+    modes = run_modes(args, device) if args.mode_steps > 0 and world == 1 else None
 
     if rank == 0:
         line = {
@@ -940,6 +998,7 @@ def run_b200(args) -> None:
             "differentiable": differentiable,
             "lidar": lidar,
             "ingest_and_hybrid": aux,
+            "modes": modes,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -644,6 +644,13 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
             const float s2 = sigma * sigma;
             for (int64_t i = start; i < end; ++i) {
               const vo_record* rec = &records[entries[i].record];
+              /* Only pixels inside the box of the record's ray ellipse
+               * (radius + 1 px around its centre; 16-bit, 32767 unbounded). */
+              const int bx = (rec->radius_x < 32766 ? rec->radius_x : 32766) + 1;
+              const int by = (rec->radius_y < 32766 ? rec->radius_y : 32766) + 1;
+              const float hx = bx >= 32767 ? INFINITY : (float)bx;
+              const float hy = by >= 32767 ? INFINITY : (float)by;
+              if (fabsf(cx - rec->mean_x) > hx || fabsf(cy - rec->mean_y) > hy) continue;
               const float* P = rec->prec;
               const float rpr = fmaf(2.0f * P[4], ray_y,
                                      fmaf(P[3] * ray_y, ray_y,

@@ -224,6 +224,10 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
 // screen-space compositor, without its warp footprint masks (the record's
 // ellipse is the tile cover itself).  A terminated pixel's ray_y becomes NaN,
 // so every later d^T P d is NaN and fails the > 0 test.
+// Each record is evaluated only at pixels inside the box of its ray ellipse
+// (radius + 1 px around the ellipse centre, record c.w): outside it the exact
+// m^2 exceeds sigma^2, so this drops only float-cancellation artefacts, and it
+// lets each warp skip the records whose box misses its 8x8 block.
 // ---------------------------------------------------------------------------
 template <bool kFull>
 __device__ __forceinline__ void blend_ray(PixelState& s, float& ray_y, float alpha, int32_t pos,
@@ -247,11 +251,12 @@ __device__ __forceinline__ void blend_ray(PixelState& s, float& ray_y, float alp
   }
 }
 
-// alpha of one record on one ray (0 when it does not contribute); rx_terms
-// carries the ray_x products shared by the thread's two pixels.
+// alpha of one record on one ray (0 when it does not contribute); t_*
+// carry the ray_x products shared by the thread's two pixels.
 __device__ __forceinline__ float ray_alpha(const float4& p0, const float4& p1, const float4& p2,
                                            float ray_x, float ray_y, float t_xx, float t_xy,
                                            float t_x, float t_m, float s2) {
+  if (!(ray_y == ray_y)) return 0.0f;  // terminated or outside the record's box
   // d^T P d = P00 x^2 + 2 P01 x y + 2 P02 x + P11 y^2 + 2 P12 y + P22
   const float rpr = fadd(
       ffma(fmul(2.0f, p1.x), ray_y,
@@ -259,7 +264,14 @@ __device__ __forceinline__ float ray_alpha(const float4& p0, const float4& p1, c
       p1.y);
   if (!(rpr > 0.0f)) return 0.0f;
   const float rpm = fadd(ffma(ray_y, p1.w, t_m), p2.x);
-  const float m2 = fmaxf(0.0f, fsub(p2.y, fdiv(fmul(rpm, rpm), rpr)));
+  const float rpm2 = fmul(rpm, rpm);
+  if (rpr < 1.0e30f) {
+    // Fast rejection: the approximate quotient is within 3 ulp of the IEEE
+    // one, so with this margin a rejected ray has the exact m^2 > sigma^2 too.
+    const float qa = __fdividef(rpm2, rpr);
+    if (fsub(p2.y, qa) > s2 + 1.0e-6f * (fabsf(qa) + s2)) return 0.0f;
+  }
+  const float m2 = fmaxf(0.0f, fsub(p2.y, fdiv(rpm2, rpr)));
   // m^2 > 174 would take exp below the float range of the polynomial exp:
   // alpha < 2e-38, no contribution.
   if (!(m2 <= s2) || !(m2 <= 174.0f)) return 0.0f;
@@ -275,6 +287,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   __shared__ float4 s_p1[kCompositeBatch];   // P12, P22, Pm0, Pm1
   __shared__ float4 s_p2[kCompositeBatch];   // Pm2, mPm, opacity, -
   __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
+  __shared__ float4 s_box[kCompositeBatch];  // centre x, centre y, half-extent x, y
+  __shared__ uint32_t s_mask[kCompositeBatch];
   CamPlan plan;
   int64_t local_tile;
   if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, blockIdx.x, plan,
@@ -299,9 +313,14 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   const float kNaN = __int_as_float(0x7fc00000);
   const float* in = p.intrinsics + static_cast<int64_t>(plan.camera) * 9;
   const float fx = in[0], cxi = in[2], fy = in[4], cyi = in[5];
-  const float ray_x = fdiv(fsub(fadd(static_cast<float>(pixel_x), 0.5f), cxi), fx);
-  float ray_y0 = valid0 ? fdiv(fsub(fadd(static_cast<float>(pixel_y0), 0.5f), cyi), fy) : kNaN;
-  float ray_y1 = valid1 ? fdiv(fsub(fadd(static_cast<float>(pixel_y1), 0.5f), cyi), fy) : kNaN;
+  const float cx = fadd(static_cast<float>(pixel_x), 0.5f);
+  const float cy0 = fadd(static_cast<float>(pixel_y0), 0.5f);
+  const float cy1 = fadd(static_cast<float>(pixel_y1), 0.5f);
+  const float ray_x = fdiv(fsub(cx, cxi), fx);
+  float ray_y0 = valid0 ? fdiv(fsub(cy0, cyi), fy) : kNaN;
+  float ray_y1 = valid1 ? fdiv(fsub(cy1, cyi), fy) : kNaN;
+  const float tile_x0 = static_cast<float>(tile_x * kTile);
+  const float tile_y0 = static_cast<float>(tile_y * kTile);
   const float s2 = fmul(p.support_sigma, p.support_sigma);
 
   PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid0};
@@ -321,28 +340,55 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
         s_p1[j] = p.ray_ext[static_cast<int64_t>(r) * 3 + 1];
         s_p2[j] = make_float4(e2.x, e2.y, rec.b.y, 0.0f);
         s_col[j] = make_float4(rec.c.x, rec.c.y, rec.c.z, rec.b.z);
+        const uint32_t bits = __float_as_uint(rec.c.w);
+        const float hx = (bits & 0xffffu) >= 32767u ? __int_as_float(0x7f800000)
+                                                    : static_cast<float>(bits & 0xffffu);
+        const float hy = (bits >> 16) >= 32767u ? __int_as_float(0x7f800000) : static_cast<float>(bits >> 16);
+        s_box[j] = make_float4(rec.a.x, rec.a.y, hx, hy);
+        uint32_t mask = 0;
+#pragma unroll
+        for (int w = 0; w < Geo::kWarps; ++w) {
+          const float bx0 = tile_x0 + static_cast<float>((w % Geo::kWarpsX) * Geo::kBlockW) + 0.5f;
+          const float by0 = tile_y0 + static_cast<float>((w / Geo::kWarpsX) * Geo::kBlockH) + 0.5f;
+          const float bx1 = bx0 + static_cast<float>(Geo::kBlockW - 1);
+          const float by1 = by0 + static_cast<float>(Geo::kBlockH - 1);
+          const bool hit = !(fsub(bx0, rec.a.x) > hx || fsub(rec.a.x, bx1) > hx ||
+                             fsub(by0, rec.a.y) > hy || fsub(rec.a.y, by1) > hy);
+          mask |= hit ? (1u << w) : 0u;
+        }
+        s_mask[j] = mask;
       }
       __syncthreads();
       if (!warp_done) {
         const int32_t chunk_pos = static_cast<int32_t>(chunk);
-        for (int j = 0; j < n; ++j) {
-          const float4 p0 = s_p0[j];
-          const float4 p1 = s_p1[j];
-          const float4 p2 = s_p2[j];
-          const float t_xx = fmul(fmul(p0.x, ray_x), ray_x);
-          const float t_xy = fmul(fmul(2.0f, p0.y), ray_x);
-          const float t_x = fmul(2.0f, p0.z);
-          const float t_m = fmul(ray_x, p1.z);
-          const float a0 = ray_alpha(p0, p1, p2, ray_x, ray_y0, t_xx, t_xy, t_x, t_m, s2);
-          const float a1 = ray_alpha(p0, p1, p2, ray_x, ray_y1, t_xx, t_xy, t_x, t_m, s2);
-          if (a0 > 0.0f || a1 > 0.0f) {
-            const float4 col = s_col[j];
-            if (a0 > 0.0f) blend_ray<kFull>(s0, ray_y0, a0, chunk_pos + j, col);
-            if (a1 > 0.0f) blend_ray<kFull>(s1, ray_y1, a1, chunk_pos + j, col);
+        for (int base = 0; base < n && !warp_done; base += 32) {
+          const uint32_t m = (base + lane < n) ? s_mask[base + lane] : 0u;
+          uint32_t bits = __ballot_sync(0xffffffffu, (m >> warp) & 1u);
+          while (bits) {
+            const int j = base + __ffs(bits) - 1;
+            bits &= bits - 1;
+            const float4 box = s_box[j];
+            const bool in_x = !(fabsf(fsub(cx, box.x)) > box.z);
+            const float y0 = (in_x && !(fabsf(fsub(cy0, box.y)) > box.w)) ? ray_y0 : kNaN;
+            const float y1 = (in_x && !(fabsf(fsub(cy1, box.y)) > box.w)) ? ray_y1 : kNaN;
+            if (!(y0 == y0) && !(y1 == y1)) continue;
+            const float4 p0 = s_p0[j];
+            const float4 p1 = s_p1[j];
+            const float4 p2 = s_p2[j];
+            const float t_xx = fmul(fmul(p0.x, ray_x), ray_x);
+            const float t_xy = fmul(fmul(2.0f, p0.y), ray_x);
+            const float t_x = fmul(2.0f, p0.z);
+            const float t_m = fmul(ray_x, p1.z);
+            const float a0 = ray_alpha(p0, p1, p2, ray_x, y0, t_xx, t_xy, t_x, t_m, s2);
+            const float a1 = ray_alpha(p0, p1, p2, ray_x, y1, t_xx, t_xy, t_x, t_m, s2);
+            if (a0 > 0.0f || a1 > 0.0f) {
+              const float4 col = s_col[j];
+              if (a0 > 0.0f) blend_ray<kFull>(s0, ray_y0, a0, chunk_pos + j, col);
+              if (a1 > 0.0f) blend_ray<kFull>(s1, ray_y1, a1, chunk_pos + j, col);
+            }
           }
-          if ((j & 31) == 31 && __all_sync(0xffffffffu, s0.done && s1.done)) break;
+          warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
         }
-        warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
       }
       if (__syncthreads_count(!(s0.done && s1.done)) == 0) break;
     }

@@ -732,9 +732,14 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           staged.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
           const int32_t id = p.gaussian_ids ? p.gaussian_ids[g] : static_cast<int32_t>(g);
           staged.b = make_float4(pr.conic2, pr.opacity, pr.depth, __int_as_float(id));
-          staged.c = make_float4(
-              rgb[0], rgb[1], rgb[2],
-              __uint_as_float(footprint_box(pr.opacity, pr.cov_a, pr.cov_b, pr.cov_c)));
+          // c.w: the screen-space alpha footprint, or in exact-ray mode the
+          // half-extents (radius + 1 px, 16-bit each, 32767 = unbounded) of
+          // the ray ellipse's box around its centre.
+          const uint32_t box =
+              kRay ? static_cast<uint32_t>(min(pr.radius_x, 32766) + 1) |
+                         (static_cast<uint32_t>(min(pr.radius_y, 32766) + 1) << 16)
+                   : footprint_box(pr.opacity, pr.cov_a, pr.cov_b, pr.cov_c);
+          staged.c = make_float4(rgb[0], rgb[1], rgb[2], __uint_as_float(box));
         }
       }
     }
