@@ -307,36 +307,28 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
           for (int f = 0; f < kRecordGradCount; ++f) g[f] = 0.0f;
           backward_pixel(q0, c0, oe0, e0, col, dx, dy0, g);
           backward_pixel(q1, c1, oe1, e1, col, dx, dy1, g);
-          const bool hit = c0 || c1;
+          // Transposed warp sum: four halving exchanges leave lane l with a
+          // partial sum of term (l >> 1) over 16 lanes, the last one adds the
+          // other half; 16 shuffles instead of 5 per term.  (Direct shared
+          // atomics for records that touch few lanes measured slower: the
+          // lanes' adds to one record serialise.)
           float* dst = s_grad + j * kGradStride;
-          if (__popc(hits) <= 4) {
-            // At most four pixel pairs touched the record: add their terms
-            // directly.
-            if (hit) {
+          float v[16];
 #pragma unroll
-              for (int f = 0; f < kRecordGradCount; ++f) atomicAdd(dst + f, g[f]);
+          for (int f = 0; f < 16; ++f) v[f] = f < kRecordGradCount ? g[f] : 0.0f;
+#pragma unroll
+          for (int half = 8; half >= 1; half >>= 1) {
+            const bool upper = (lane & (half * 2)) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+              const float send = upper ? v[i] : v[i + half];
+              const float keep = upper ? v[i + half] : v[i];
+              v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half * 2);
             }
-          } else {
-            // Transposed warp sum: four halving exchanges leave lane l with
-            // a partial sum of term (l >> 1) over 16 lanes, the last one
-            // adds the other half; 16 shuffles instead of 5 per term.
-            float v[16];
-#pragma unroll
-            for (int f = 0; f < 16; ++f) v[f] = f < kRecordGradCount ? g[f] : 0.0f;
-#pragma unroll
-            for (int half = 8; half >= 1; half >>= 1) {
-              const bool upper = (lane & (half * 2)) != 0;
-#pragma unroll
-              for (int i = 0; i < half; ++i) {
-                const float send = upper ? v[i] : v[i + half];
-                const float keep = upper ? v[i + half] : v[i];
-                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half * 2);
-              }
-            }
-            v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-            const int term = lane >> 1;
-            if ((lane & 1) == 0 && term < kRecordGradCount) atomicAdd(dst + term, v[0]);
           }
+          v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+          const int term = lane >> 1;
+          if ((lane & 1) == 0 && term < kRecordGradCount) atomicAdd(dst + term, v[0]);
         }
       }
     }
