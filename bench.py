@@ -79,6 +79,8 @@ def parse_args() -> argparse.Namespace:
                         help="timed steps of PLY ingestion and the hybrid compositor (0: skip)")
     parser.add_argument("--mode-steps", type=int, default=5,
                         help="frames per dense-mode / exact-ray measurement (0 skips)")
+    parser.add_argument("--mode-cameras", type=int, default=None,
+                        help="cameras of both mode workloads (default 32 deep-scene, 64 batched; small for ncu)")
     parser.add_argument("--diff-steps", type=int, default=10,
                         help="timed steps of the differentiable-form workload (0: skip)")
     parser.add_argument("--ragged-scale", type=float, default=1.0,
@@ -465,18 +467,18 @@ def run_modes(args, device) -> dict:
 
     deep = synthetic_scene(2_000_000, seed=7, mean_half_extent=2.0, log_scale_mean=-3.0)
     deep.opacities.clamp_(min=0.5)
-    deep_rig = orbit_cameras(32, seed=3, radius=6.0, width=320, height=240, focal=260.0)
+    deep_rig = orbit_cameras(args.mode_cameras or 32, seed=3, radius=6.0, width=320, height=240, focal=260.0)
     plain = frame_ms(deep, deep_rig, tile_size=16)
     dense = frame_ms(deep, deep_rig, tile_size=1)
     del deep
-    scene, rig = batched_workload()
+    scene, rig = batched_workload(cameras=args.mode_cameras or 64)
     screen = frame_ms(scene, rig, tile_size=16, sh_degree=3)
     ray = frame_ms(scene, rig, tile_size=16, sh_degree=3, ray_gaussian_evaluation=True)
     return {
-        "dense_mode": {"workload": "deep-2m-32x320x240 (2M Gaussians, opacity >= 0.5, 32 cameras)",
+        "dense_mode": {"workload": f"deep-2m-{deep_rig.viewmats.shape[0]}x320x240 (2M Gaussians, opacity >= 0.5)",
                        "plain_tile16": plain, "dense_tile1": dense,
                        "speedup": round(plain["ms"] / dense["ms"], 3)},
-        "exact_ray": {"workload": "batched-1m-sh3 (64 cameras 640x480)", "screen_space": screen,
+        "exact_ray": {"workload": f"batched-1m-sh3 ({rig.viewmats.shape[0]} cameras 640x480)", "screen_space": screen,
                       "exact_ray": ray, "ray_over_screen_time": round(ray["ms"] / screen["ms"], 3)},
         "steps": steps,
     }

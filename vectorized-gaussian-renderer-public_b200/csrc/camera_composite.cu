@@ -278,7 +278,11 @@ __device__ __forceinline__ float ray_alpha(const float4& p0, const float4& p1, c
   return fminf(1.0f, fmul(p2.z, vexp(fmul(-0.5f, m2))));
 }
 
-template <int kTile, bool kFull>
+// kSplit: CTAs per bin side.  A 32-pixel bin (16-pixel tiles in exact-ray
+// mode) is composited by four 16-pixel CTAs that read the same sorted list:
+// smaller CTAs wait less at the batch barriers, and each pixel still sees
+// its bin's records in the same order.
+template <int kTile, bool kFull, int kSplit>
 __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
                                   2048 / CompositeGeometry<kTile>::kThreads / 2)
     composite_ray_kernel(CompositeParams p) {
@@ -291,13 +295,18 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   __shared__ uint32_t s_mask[kCompositeBatch];
   CamPlan plan;
   int64_t local_tile;
-  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, blockIdx.x, plan,
+  const int64_t item = blockIdx.x / (kSplit * kSplit);
+  const int quad = static_cast<int>(blockIdx.x - item * (kSplit * kSplit));
+  if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, item, plan,
                    local_tile)) {
     return;
   }
-  const int tile_y = static_cast<int>(local_tile / plan.tiles_x);
-  const int tile_x = static_cast<int>(local_tile - static_cast<int64_t>(tile_y) * plan.tiles_x);
+  const int bin_y = static_cast<int>(local_tile / plan.tiles_x);
+  const int bin_x = static_cast<int>(local_tile - static_cast<int64_t>(bin_y) * plan.tiles_x);
   const int64_t global_tile = plan.tile_base + local_tile;
+  const int origin_x = (bin_x * kSplit + quad % kSplit) * kTile;
+  const int origin_y = (bin_y * kSplit + quad / kSplit) * kTile;
+  if (origin_x >= plan.width || origin_y >= plan.height) return;  // quadrant past the image edge
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -305,8 +314,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   const int lx = lane % Geo::kBlockW;
   const int ly = lane / Geo::kBlockW;
   const bool lane_used = ly < Geo::kLaneRows;
-  const int pixel_x = tile_x * kTile + (warp % Geo::kWarpsX) * Geo::kBlockW + lx;
-  const int pixel_y0 = tile_y * kTile + (warp / Geo::kWarpsX) * Geo::kBlockH + ly;
+  const int pixel_x = origin_x + (warp % Geo::kWarpsX) * Geo::kBlockW + lx;
+  const int pixel_y0 = origin_y + (warp / Geo::kWarpsX) * Geo::kBlockH + ly;
   const int pixel_y1 = pixel_y0 + Geo::kLaneRows;
   const bool valid0 = lane_used && pixel_x < plan.width && pixel_y0 < plan.height;
   const bool valid1 = lane_used && pixel_x < plan.width && pixel_y1 < plan.height;
@@ -319,8 +328,8 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   const float ray_x = fdiv(fsub(cx, cxi), fx);
   float ray_y0 = valid0 ? fdiv(fsub(cy0, cyi), fy) : kNaN;
   float ray_y1 = valid1 ? fdiv(fsub(cy1, cyi), fy) : kNaN;
-  const float tile_x0 = static_cast<float>(tile_x * kTile);
-  const float tile_y0 = static_cast<float>(tile_y * kTile);
+  const float tile_x0 = static_cast<float>(origin_x);
+  const float tile_y0 = static_cast<float>(origin_y);
   const float s2 = fmul(p.support_sigma, p.support_sigma);
 
   PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid0};
@@ -397,14 +406,14 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   if (valid1) write_pixel<kFull, false>(p, plan, pixel_x, pixel_y1, s1);
 }
 
-template __global__ void composite_ray_kernel<4, false>(CompositeParams);
-template __global__ void composite_ray_kernel<4, true>(CompositeParams);
-template __global__ void composite_ray_kernel<8, false>(CompositeParams);
-template __global__ void composite_ray_kernel<8, true>(CompositeParams);
-template __global__ void composite_ray_kernel<16, false>(CompositeParams);
-template __global__ void composite_ray_kernel<16, true>(CompositeParams);
-template __global__ void composite_ray_kernel<32, false>(CompositeParams);
-template __global__ void composite_ray_kernel<32, true>(CompositeParams);
+template __global__ void composite_ray_kernel<4, false, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<4, true, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<8, false, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<8, true, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<16, false, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<16, true, 1>(CompositeParams);
+template __global__ void composite_ray_kernel<16, false, 2>(CompositeParams);
+template __global__ void composite_ray_kernel<16, true, 2>(CompositeParams);
 
 template __global__ void composite_kernel<4, false, false>(CompositeParams);
 template __global__ void composite_kernel<4, true, false>(CompositeParams);

@@ -626,17 +626,19 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
       cp.support_sigma = static_cast<float>(opt->gaussian_support_sigma);
       const unsigned grid = static_cast<unsigned>(max_items);
       if (bin == 32) {
-        if (full) composite_ray_kernel<32, true><<<grid, composite_threads(32), 0, stream>>>(cp);
-        else composite_ray_kernel<32, false><<<grid, composite_threads(32), 0, stream>>>(cp);
+        if (max_items * 4 > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "raster grid exceeds CUDA limit");
+        const unsigned grid4 = static_cast<unsigned>(max_items * 4);
+        if (full) composite_ray_kernel<16, true, 2><<<grid4, composite_threads(16), 0, stream>>>(cp);
+        else composite_ray_kernel<16, false, 2><<<grid4, composite_threads(16), 0, stream>>>(cp);
       } else if (bin == 16) {
-        if (full) composite_ray_kernel<16, true><<<grid, composite_threads(16), 0, stream>>>(cp);
-        else composite_ray_kernel<16, false><<<grid, composite_threads(16), 0, stream>>>(cp);
+        if (full) composite_ray_kernel<16, true, 1><<<grid, composite_threads(16), 0, stream>>>(cp);
+        else composite_ray_kernel<16, false, 1><<<grid, composite_threads(16), 0, stream>>>(cp);
       } else if (bin == 8) {
-        if (full) composite_ray_kernel<8, true><<<grid, composite_threads(8), 0, stream>>>(cp);
-        else composite_ray_kernel<8, false><<<grid, composite_threads(8), 0, stream>>>(cp);
+        if (full) composite_ray_kernel<8, true, 1><<<grid, composite_threads(8), 0, stream>>>(cp);
+        else composite_ray_kernel<8, false, 1><<<grid, composite_threads(8), 0, stream>>>(cp);
       } else {
-        if (full) composite_ray_kernel<4, true><<<grid, composite_threads(4), 0, stream>>>(cp);
-        else composite_ray_kernel<4, false><<<grid, composite_threads(4), 0, stream>>>(cp);
+        if (full) composite_ray_kernel<4, true, 1><<<grid, composite_threads(4), 0, stream>>>(cp);
+        else composite_ray_kernel<4, false, 1><<<grid, composite_threads(4), 0, stream>>>(cp);
       }
     } else if (train) {
       if (bin == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);

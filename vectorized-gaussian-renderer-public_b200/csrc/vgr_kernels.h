@@ -320,7 +320,7 @@ __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
 template <int kTile, bool kFull, bool kTrain>
 __global__ void composite_kernel(CompositeParams p);
-template <int kTile, bool kFull>
+template <int kTile, bool kFull, int kSplit>
 __global__ void composite_ray_kernel(CompositeParams p);
 
 __global__ void train_activate_kernel(TrainActivateParams p);
