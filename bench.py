@@ -764,14 +764,18 @@ def run_differentiable(args, device, world: int) -> dict:
     target = [t.clone() for t in renderer.forward_native(*(work.targets[k].to(device) for k in names), view, intr)]
     t_rgb, t_depth = target[0], target[1]
 
-    def step() -> None:
-        rgb, depth, _ = renderer.render(*(params[k] for k in names), view, intr)
-        loss = photometric_loss(rgb, depth, t_rgb, t_depth, 0.1)
-        loss.backward()
-        if world > 1:
-            allreduce_gradients([params[k].grad for k in names])
-        for p in params.values():
-            p.grad = None
+    def step_with(r):
+        def step() -> None:
+            rgb, depth, _ = r.render(*(params[k] for k in names), view, intr)
+            loss = photometric_loss(rgb, depth, t_rgb, t_depth, 0.1)
+            loss.backward()
+            if world > 1:
+                allreduce_gradients([params[k].grad for k in names])
+            for p in params.values():
+                p.grad = None
+        return step
+
+    step = step_with(renderer)
 
     stream = torch.cuda.current_stream(device)
     for _ in range(max(args.warmup, 3)):
@@ -810,6 +814,25 @@ def run_differentiable(args, device, world: int) -> dict:
     stop.record(stream)
     torch.cuda.synchronize(device)
     bwd_ms = start.elapsed_time(stop) / steps
+    # The same step under a list memory budget of a quarter of the frame's
+    # lists: the forward renders camera chunks and the backward recomputes
+    # each chunk's sorted lists.
+    lc = renderer.last_counters
+    full_lists = 24 * lc["tile_intersections"] + 96 * lc["visible_gaussians"] + \
+        4 * work.params["means"].shape[0] * rig.viewmats.shape[0]
+    budgeted = DifferentiableRenderer(height=rig.height, width=rig.width, sh_degree=3, device=device,
+                                      list_budget_bytes=full_lists // 4, capacity_check="deferred")
+    budget_step = step_with(budgeted)
+    for _ in range(3):
+        budget_step()
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    for _ in range(steps):
+        budget_step()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    budget_ms = max_over_ranks(start.elapsed_time(stop), world, device) / steps
+    budget_chunks = len(budgeted._pending["chunks"])
     pixels = rig.viewmats.shape[0] * rig.height * rig.width
     return {
         "metric": DIFF_METRIC,
@@ -821,6 +844,9 @@ def run_differentiable(args, device, world: int) -> dict:
         "backward_kernels_ms": round(bwd_ms, 3),
         "fwd_bwd_over_fwd": round(step_ms / fwd_ms, 3),
         "target_fwd_bwd_over_fwd": 2.5,
+        "list_budget": {"budget_bytes": int(full_lists // 4), "full_lists_bytes": int(full_lists),
+                        "camera_chunks": budget_chunks, "ms_per_iter": round(budget_ms, 3),
+                        "mode": "lists beyond the budget are recomputed in the backward, not kept"},
         "gradients": "hand-written CUDA backward; float64 autograd + central-difference checks in tests",
         "parallelism": f"data-parallel x{world} (gradient all-reduce per step)" if world > 1 else "single-gpu",
         "capacity_check": "deferred: each forward's counters are read back asynchronously and checked "

@@ -230,3 +230,34 @@ def test_gpu_deferred_capacity_check_raises_and_regrows():
     rgb, depth, alpha = deferred.render(*(params[k] for k in NAMES), view.cuda(), intr.cuda())
     rgb.sum().backward()
     assert torch.isfinite(params["means"].grad).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("capacity_check", ["sync", "deferred"])
+def test_gpu_list_budget_recomputes_chunks_with_the_same_gradients(capacity_check):
+    # A budget far below one camera's lists: the forward renders one camera
+    # at a time and the backward recomputes each camera's sorted lists.
+    from vgr_b200.differentiable import DifferentiableRenderer
+
+    scene = _scene(77, count=400, sh_degree=3)
+    view, intr = _cameras(5, seed=78)
+    weights = tuple(w.float().cuda() for w in _weights(5, seed=79))
+    results = []
+    for budget in (None, 1):
+        renderer = DifferentiableRenderer(height=SIZE, width=SIZE, sh_degree=3, tile_size=8,
+                                          list_budget_bytes=budget, capacity_check=capacity_check)
+        params = {k: v.cuda().requires_grad_(True) for k, v in scene.items()}
+        for _ in range(3):  # later frames use the learned per-camera size (and deferred checks)
+            for p in params.values():
+                p.grad = None
+            out = renderer.render(*(params[k] for k in NAMES), view.cuda(), intr.cuda())
+            weighted_loss(*out, weights).backward()
+        results.append(([t.detach().clone() for t in out], {k: params[k].grad.clone() for k in NAMES},
+                        renderer._pending["chunks"]))
+    (out_a, grads_a, chunks_a), (out_b, grads_b, chunks_b) = results
+    assert chunks_a == [(0, 5)] and len(chunks_b) == 5
+    for a, b in zip(out_a, out_b):
+        assert torch.equal(a, b)  # the forward is the same render, camera by camera
+    for name in NAMES:
+        # Per-camera partial sums added in another order: float rounding only.
+        torch.testing.assert_close(grads_b[name], grads_a[name], rtol=1e-4, atol=1e-6)

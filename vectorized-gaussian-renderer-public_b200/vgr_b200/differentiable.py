@@ -16,6 +16,15 @@ stream; there is no CPU fallback.
 One frame is in flight per renderer: the backward reads the forward's sorted
 lists and per-pixel state from the renderer's workspace, so call
 ``backward`` (or let autograd do it) before the next ``render``.
+
+Memory budget (``list_budget_bytes``): the lists a frame keeps for its
+backward (24 B per tile intersection, 96 B per visible record, 4 B per
+(camera, Gaussian) record-map entry) grow with the batch.  When a batch's
+lists would exceed the budget, the forward renders the cameras in chunks
+whose lists fit, keeping only the per-pixel state (final transmittance and
+last blended position, 8 B per pixel), and the backward recomputes each
+chunk's lists (projection, emission, sort) before its backward kernels,
+summing the chunks' parameter gradients.
 """
 
 from __future__ import annotations
@@ -51,6 +60,7 @@ class DifferentiableRenderer:
         headroom: float = 1.25,
         capacity_check: str = "sync",
         device: torch.device | str | None = None,
+        list_budget_bytes: int | None = None,
     ) -> None:
         if height <= 0 or width <= 0:
             raise ValueError("height and width must be positive")
@@ -60,6 +70,11 @@ class DifferentiableRenderer:
             raise ValueError("tile_size must be 4, 8 or 16")
         if capacity_check not in ("sync", "deferred"):
             raise ValueError("capacity_check must be 'sync' or 'deferred'")
+        if list_budget_bytes is not None and list_budget_bytes <= 0:
+            raise ValueError("list_budget_bytes must be positive when set")
+        self.list_budget_bytes = list_budget_bytes
+        self._bytes_per_camera: float | None = None
+        self._calibrated_cameras = 0
         self.capacity_check = capacity_check
         self.height = int(height)
         self.width = int(width)
@@ -140,9 +155,11 @@ class DifferentiableRenderer:
         tiles = b * math.ceil(self.height / ts) * math.ceil(self.width / ts)
         pixels = b * self.height * self.width
         if self._visible_capacity == 0:
-            # Every (camera, Gaussian) pair can be visible at most once.
-            self._visible_capacity = min(b * g, _INT32_MAX)
-            self._intersection_capacity = min(max(4 * b * g, 1024), _INT32_MAX)
+            # Every (camera, Gaussian) pair can be visible at most once (with a
+            # list budget the first render is one camera; capacity grows).
+            cams = 1 if self.list_budget_bytes is not None else b
+            self._visible_capacity = min(cams * g, _INT32_MAX)
+            self._intersection_capacity = min(max(4 * cams * g, 1024), _INT32_MAX)
         key = (g, b, device)
         if self._key == key:
             return
@@ -174,7 +191,7 @@ class DifferentiableRenderer:
         for name in ("values_in", "values_out"):
             self._ensure(name, (i,), torch.int32, device)
 
-    def _structs(self, means, features, viewmats, intrinsics, rgb, depth, alpha):
+    def _structs(self, means, features, viewmats, intrinsics, rgb, depth, alpha, cam0: int = 0):
         ws = self._ws
         g = means.shape[0]
         b = viewmats.shape[0]
@@ -239,9 +256,10 @@ class DifferentiableRenderer:
             sh_degree=self.sh_degree,
             sorted_buffer_hint=1,
         )
+        px0 = cam0 * self.height * self.width  # per-pixel state of this camera range
         state = _native.VgrTrainState(
-            final_transmittance=ws["final_transmittance"].data_ptr(),
-            last_position=ws["last_position"].data_ptr(),
+            final_transmittance=ws["final_transmittance"][px0:].data_ptr(),
+            last_position=ws["last_position"][px0:].data_ptr(),
             record_map=ws["record_map"].data_ptr(),
             record_map_capacity=ws["record_map"].numel(),
             record_grads=ws["record_grads"].data_ptr(),
@@ -270,30 +288,78 @@ class DifferentiableRenderer:
         rgb = torch.empty((b, self.height, self.width, 3), dtype=torch.float32, device=device)
         depth = torch.empty((b, self.height, self.width, 1), dtype=torch.float32, device=device)
         alpha = torch.empty((b, self.height, self.width, 1), dtype=torch.float32, device=device)
+        tensors = (means, log_scales, rotations, opacity_logits, features, viewmats, intrinsics)
+        chunks = self._camera_chunks(b)
+        self._reserve_host_counters(len(chunks))
         counter_event = None
+        for slot, (s, e) in enumerate(chunks):
+            event = self._render_range(tensors, (rgb, depth, alpha), s, e, allow_deferred=True, slot=slot)
+            counter_event = event or counter_event
+        self._frame += 1
+        self._pending = {
+            "frame": self._frame,
+            "tensors": tensors,
+            "outputs": (rgb, depth, alpha),
+            "counter_event": counter_event,
+            "chunks": chunks,
+        }
+        return rgb, depth, alpha
+
+    def _reserve_host_counters(self, slots: int) -> None:
+        """Pinned host rows for the deferred counter copies of one frame's
+        camera chunks (sized before any copy of the frame is queued)."""
+        if self._host_counters is None or self._host_counters.shape[0] < slots:
+            self._host_counters = torch.zeros((max(slots, 8), 5), dtype=torch.int64, pin_memory=True)
+
+    def _camera_chunks(self, b: int) -> list[tuple[int, int]]:
+        """Camera ranges whose kept lists fit the memory budget (one range
+        without a budget).  The per-camera size is learned from the counters
+        of earlier renders; the first budgeted render uses one camera."""
+        if self.list_budget_bytes is None:
+            return [(0, b)]
+        per = 1 if self._bytes_per_camera is None else max(
+            1, min(b, int(self.list_budget_bytes // max(self._bytes_per_camera, 1.0))))
+        return [(s, min(b, s + per)) for s in range(0, b, per)]
+
+    def _render_range(self, tensors, outputs, s: int, e: int, *, allow_deferred: bool, cam_offset: int = 0,
+                      slot: int = 0):
+        """Training forward of cameras [cam_offset + s, cam_offset + e) into
+        the outputs' rows [s, e) and the per-pixel state of those cameras'
+        pixels; grows the capacity and re-renders on overflow (synchronously
+        unless deferred checks apply)."""
+        means, _, _, _, features, viewmats, intrinsics = tensors
+        rgb, depth, alpha = (t[s:e] for t in outputs)
+        c0, c1 = cam_offset + s, cam_offset + e
+        device = means.device
+        stream = torch.cuda.current_stream(device).cuda_stream
         for _attempt in range(8):
             scene, cams, outs, native_ws, options, state = self._structs(
-                means, features, viewmats, intrinsics, rgb, depth, alpha
+                means, features, viewmats[c0:c1], intrinsics[c0:c1], rgb, depth, alpha, cam0=c0
             )
             selector = _native._c_i64(1)
             _native.check(
                 self._lib.vgr_render_train(scene, cams, outs, native_ws, options, state, stream, selector),
                 "render_train",
             )
-            if self.capacity_check == "deferred" and self._calibrated:
+            # Deferred only for camera ranges no larger than a checked one: a
+            # wider range (a budget's chunk size learned from one camera)
+            # is checked synchronously and grows the capacity first.
+            if (allow_deferred and self.capacity_check == "deferred" and self._calibrated
+                    and e - s <= self._calibrated_cameras):
                 # Checked by the backward (or the next forward), which waits
                 # only for this forward, not for the work queued after it.
-                if self._host_counters is None:
-                    self._host_counters = torch.empty(5, dtype=torch.int64, pin_memory=True)
-                self._host_counters.copy_(self._ws["counters"], non_blocking=True)
+                self._host_counters[slot].copy_(self._ws["counters"], non_blocking=True)
                 counter_event = torch.cuda.Event()
                 counter_event.record(torch.cuda.current_stream(device))
-                break
+                return counter_event
             counters = self._ws["counters"].tolist()
             self.last_counters = {"visible_gaussians": counters[0], "tile_intersections": counters[1]}
             if counters[0] <= self._visible_capacity and counters[1] <= self._intersection_capacity:
                 self._calibrated = True
-                break
+                self._calibrated_cameras = max(self._calibrated_cameras, e - s)
+                self._bytes_per_camera = (24.0 * counters[1] + 96.0 * counters[0]
+                                          + 4.0 * means.shape[0] * (e - s)) / (e - s)
+                return None
             self._visible_capacity = min(max(self._visible_capacity, int(counters[0] * self.headroom) + 1), _INT32_MAX)
             self._intersection_capacity = min(
                 max(self._intersection_capacity, int(counters[1] * self.headroom) + 1), _INT32_MAX
@@ -301,16 +367,7 @@ class DifferentiableRenderer:
             if counters[1] > _INT32_MAX:
                 raise RuntimeError("tile intersections exceed the int32 implementation limit")
             self._grow(device)
-        else:
-            raise RuntimeError("render_train: capacity did not converge")
-        self._frame += 1
-        self._pending = {
-            "frame": self._frame,
-            "tensors": (means, log_scales, rotations, opacity_logits, features, viewmats, intrinsics),
-            "outputs": (rgb, depth, alpha),
-            "counter_event": counter_event,
-        }
-        return rgb, depth, alpha
+        raise RuntimeError("render_train: capacity did not converge")
 
     def check_capacity(self) -> None:
         """Deferred capacity check of the last forward: raises when it
@@ -322,8 +379,15 @@ class DifferentiableRenderer:
             return
         event.synchronize()
         pending["counter_event"] = None
-        counters = self._host_counters.tolist()
-        self.last_counters = {"visible_gaussians": counters[0], "tile_intersections": counters[1]}
+        self._raise_on_overflow(len(pending.get("chunks", [(0, 0)])), f"frame {pending['frame']}")
+
+    def _raise_on_overflow(self, slots: int, what: str) -> None:
+        """Check the counters the deferred renders copied to the host (one
+        row per camera chunk); grow and raise when any overflowed."""
+        rows = self._host_counters[:slots].tolist()
+        counters = [max(r[0] for r in rows), max(r[1] for r in rows)]
+        last = rows[-1]
+        self.last_counters = {"visible_gaussians": last[0], "tile_intersections": last[1]}
         if counters[0] <= self._visible_capacity and counters[1] <= self._intersection_capacity:
             return
         self._visible_capacity = min(max(self._visible_capacity, int(counters[0] * self.headroom) + 1), _INT32_MAX)
@@ -333,7 +397,7 @@ class DifferentiableRenderer:
         self._grow(self._pending["outputs"][0].device)
         self._calibrated = False
         raise RuntimeError(
-            f"frame {pending['frame']} overflowed the record or intersection capacity "
+            f"{what} overflowed the record or intersection capacity "
             f"({counters[0]} records, {counters[1]} intersections); its outputs are invalid. "
             "Capacity has been grown: render the frame again."
         )
@@ -357,33 +421,62 @@ class DifferentiableRenderer:
         grad_rgb = grad_rgb.contiguous()
         grad_depth = grad_depth.contiguous() if grad_depth is not None else None
         grad_alpha = grad_alpha.contiguous() if grad_alpha is not None else None
-        d_means = torch.empty((g, 3), dtype=torch.float32, device=device)
-        d_log_scales = torch.empty((g, 3), dtype=torch.float32, device=device)
-        d_rotations = torch.empty((g, 4), dtype=torch.float32, device=device)
-        d_logits = torch.empty((g,), dtype=torch.float32, device=device)
-        d_features = torch.empty_like(features)
-        scene, cams, outs, native_ws, options, state = self._structs(
-            means, features, viewmats, intrinsics, rgb, depth, alpha
-        )
+        chunks = pending.get("chunks", [(0, viewmats.shape[0])])
         params = _native.VgrTrainParams(
             log_scales=log_scales.data_ptr(), rotations=rotations.data_ptr(),
             opacity_logits=opacity_logits.data_ptr(),
         )
-        grads = _native.VgrOutputGrads(
-            rgb=grad_rgb.data_ptr(),
-            depth=grad_depth.data_ptr() if grad_depth is not None else None,
-            alpha=grad_alpha.data_ptr() if grad_alpha is not None else None,
-        )
-        out = _native.VgrParamGrads(
-            means=d_means.data_ptr(), log_scales=d_log_scales.data_ptr(), rotations=d_rotations.data_ptr(),
-            opacity_logits=d_logits.data_ptr(), features=d_features.data_ptr(),
-        )
         stream = torch.cuda.current_stream(device).cuda_stream
-        _native.check(
-            self._lib.vgr_render_backward(scene, params, cams, outs, native_ws, options, state, grads, out, stream),
-            "render_backward",
-        )
-        return d_means, d_log_scales, d_rotations, d_logits, d_features
+
+        def backward_range(s: int, e: int, fwd):
+            d = (torch.empty((g, 3), dtype=torch.float32, device=device),
+                 torch.empty((g, 3), dtype=torch.float32, device=device),
+                 torch.empty((g, 4), dtype=torch.float32, device=device),
+                 torch.empty((g,), dtype=torch.float32, device=device),
+                 torch.empty_like(features))
+            scene, cams, outs, native_ws, options, state = self._structs(
+                means, features, viewmats[s:e], intrinsics[s:e], *fwd, cam0=s
+            )
+            grads = _native.VgrOutputGrads(
+                rgb=grad_rgb[s:e].data_ptr(),
+                depth=grad_depth[s:e].data_ptr() if grad_depth is not None else None,
+                alpha=grad_alpha[s:e].data_ptr() if grad_alpha is not None else None,
+            )
+            out = _native.VgrParamGrads(
+                means=d[0].data_ptr(), log_scales=d[1].data_ptr(), rotations=d[2].data_ptr(),
+                opacity_logits=d[3].data_ptr(), features=d[4].data_ptr(),
+            )
+            _native.check(
+                self._lib.vgr_render_backward(scene, params, cams, outs, native_ws, options, state, grads, out,
+                                              stream),
+                "render_backward",
+            )
+            return d
+
+        if len(chunks) == 1:
+            s, e = chunks[0]
+            return backward_range(s, e, (rgb[s:e], depth[s:e], alpha[s:e]))
+        # Lists beyond the budget were not kept: recompute each chunk's lists
+        # (its forward again, into scratch outputs: the same values bit for
+        # bit, and the same per-pixel state) before its backward.
+        totals = None
+        tensors = pending["tensors"]
+        per = max(e - s for s, e in chunks)
+        scratch = (torch.empty((per,) + tuple(rgb.shape[1:]), dtype=rgb.dtype, device=device),
+                   torch.empty((per,) + tuple(depth.shape[1:]), dtype=depth.dtype, device=device),
+                   torch.empty((per,) + tuple(alpha.shape[1:]), dtype=alpha.dtype, device=device))
+        self._reserve_host_counters(len(chunks))
+        event = None
+        for slot, (s, e) in enumerate(chunks):
+            fwd = tuple(t[: e - s] for t in scratch)
+            event = self._render_range(tensors, fwd, 0, e - s, allow_deferred=True, cam_offset=s,
+                                       slot=slot) or event
+            part = backward_range(s, e, fwd)
+            totals = part if totals is None else tuple(t.add_(p) for t, p in zip(totals, part))
+        if event is not None:
+            event.synchronize()
+            self._raise_on_overflow(len(chunks), f"the backward of frame {frame}")
+        return totals
 
     @property
     def frame(self) -> int:
