@@ -640,7 +640,7 @@ def run_ragged(args, device, world: int) -> dict:
     ragged = RaggedBatch(backend, work.heights, work.widths)
     outputs = ragged.outputs()
     view = poses[0].clone()
-    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16))
+    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16, 32))
     counters = ragged.calibrate(view, intr, scene_ids, outputs)
     graph = ragged.capture(view, intr, scene_ids, outputs)
     stream = torch.cuda.current_stream(device)

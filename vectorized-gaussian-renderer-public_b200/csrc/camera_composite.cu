@@ -95,21 +95,28 @@ __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamP
   }
 }
 
-// One work item (one (camera, tile)); every exit is CTA-uniform.
-template <int kTile, bool kFull, bool kTrain>
-__device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t item,
+// One work item (one (camera, tile), or with kSplit > 1 one kTile-pixel
+// quadrant of a (kSplit * kTile)-pixel tile whose sorted list the quadrants
+// share); every exit is CTA-uniform.
+template <int kTile, bool kFull, bool kTrain, int kSplit>
+__device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t work,
                                                float4* s_geo, float4* s_cpo, float4* s_col,
                                                uint32_t* s_mask) {
   using Geo = CompositeGeometry<kTile>;
   CamPlan plan;
   int64_t local_tile;
+  const int64_t item = work / (kSplit * kSplit);
+  const int quad = static_cast<int>(work - item * (kSplit * kSplit));
   if (!locate_tile(p.scratch, p.layout, p.active_count, p.tiles_per_camera_hint, item, plan,
                    local_tile)) {
     return;
   }
-  const int tile_y = static_cast<int>(local_tile / plan.tiles_x);
-  const int tile_x = static_cast<int>(local_tile - static_cast<int64_t>(tile_y) * plan.tiles_x);
+  const int bin_y = static_cast<int>(local_tile / plan.tiles_x);
+  const int bin_x = static_cast<int>(local_tile - static_cast<int64_t>(bin_y) * plan.tiles_x);
   const int64_t global_tile = plan.tile_base + local_tile;
+  const int tile_x = bin_x * kSplit + quad % kSplit;  // in kTile units
+  const int tile_y = bin_y * kSplit + quad / kSplit;
+  if (tile_x * kTile >= plan.width || tile_y * kTile >= plan.height) return;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -187,7 +194,7 @@ __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t
 // the camera setup) until every (camera, tile) of the frame is done: no
 // CTA is launched for the grid's empty tail, and a CTA that finishes a cheap
 // tile immediately takes the next one.
-template <int kTile, bool kFull, bool kTrain>
+template <int kTile, bool kFull, bool kTrain, int kSplit>
 __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
                                   2048 / CompositeGeometry<kTile>::kThreads / 2)
     composite_kernel(CompositeParams p) {
@@ -197,18 +204,18 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
   __shared__ uint32_t s_mask[kCompositeBatch];
   __shared__ uint32_t s_item;
   if (!p.persistent) {
-    composite_item<kTile, kFull, kTrain>(p, blockIdx.x, s_geo, s_cpo, s_col, s_mask);
+    composite_item<kTile, kFull, kTrain, kSplit>(p, blockIdx.x, s_geo, s_cpo, s_col, s_mask);
     return;
   }
   ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
   const int64_t* tile_prefix = reinterpret_cast<const int64_t*>(p.scratch + p.layout.tile_prefix);
-  const int64_t total = tile_prefix[p.active_count];
+  const int64_t total = tile_prefix[p.active_count] * (kSplit * kSplit);
   while (true) {
     if (threadIdx.x == 0) s_item = atomicAdd(&header->composite_queue, 1u);
     __syncthreads();
     const int64_t item = s_item;
     if (item >= total) break;
-    composite_item<kTile, kFull, kTrain>(p, item, s_geo, s_cpo, s_col, s_mask);
+    composite_item<kTile, kFull, kTrain, kSplit>(p, item, s_geo, s_cpo, s_col, s_mask);
     __syncthreads();  // shared staging and s_item are reused by the next item
   }
 }
@@ -415,14 +422,16 @@ template __global__ void composite_ray_kernel<16, true, 1>(CompositeParams);
 template __global__ void composite_ray_kernel<16, false, 2>(CompositeParams);
 template __global__ void composite_ray_kernel<16, true, 2>(CompositeParams);
 
-template __global__ void composite_kernel<4, false, false>(CompositeParams);
-template __global__ void composite_kernel<4, true, false>(CompositeParams);
-template __global__ void composite_kernel<8, false, false>(CompositeParams);
-template __global__ void composite_kernel<8, true, false>(CompositeParams);
-template __global__ void composite_kernel<16, false, false>(CompositeParams);
-template __global__ void composite_kernel<16, true, false>(CompositeParams);
-template __global__ void composite_kernel<4, true, true>(CompositeParams);
-template __global__ void composite_kernel<8, true, true>(CompositeParams);
-template __global__ void composite_kernel<16, true, true>(CompositeParams);
+template __global__ void composite_kernel<4, false, false, 1>(CompositeParams);
+template __global__ void composite_kernel<4, true, false, 1>(CompositeParams);
+template __global__ void composite_kernel<8, false, false, 1>(CompositeParams);
+template __global__ void composite_kernel<8, true, false, 1>(CompositeParams);
+template __global__ void composite_kernel<16, false, false, 1>(CompositeParams);
+template __global__ void composite_kernel<16, true, false, 1>(CompositeParams);
+template __global__ void composite_kernel<16, false, false, 2>(CompositeParams);
+template __global__ void composite_kernel<16, true, false, 2>(CompositeParams);
+template __global__ void composite_kernel<4, true, true, 1>(CompositeParams);
+template __global__ void composite_kernel<8, true, true, 1>(CompositeParams);
+template __global__ void composite_kernel<16, true, true, 1>(CompositeParams);
 
 }  // namespace vgr

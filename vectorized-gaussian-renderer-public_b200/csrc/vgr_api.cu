@@ -201,13 +201,16 @@ namespace vgr {
 
 // One CTA per work item, or a resident grid (as many CTAs as fit on the SMs)
 // over the device work queue.
-template <int kTile, bool kFull, bool kTrain>
+// kSplit > 1: each (kSplit * kTile)-pixel tile is composited as kSplit^2
+// kTile-pixel quadrants (one work item each).
+template <int kTile, bool kFull, bool kTrain, int kSplit = 1>
 void launch_composite(const CompositeParams& cp, int64_t max_items, int sms, cudaStream_t stream) {
   const int threads = composite_threads(kTile);
+  max_items *= kSplit * kSplit;
   unsigned grid = static_cast<unsigned>(max_items);
   if (cp.persistent) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, composite_kernel<kTile, kFull, kTrain>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, composite_kernel<kTile, kFull, kTrain, kSplit>,
                                                       threads, 0) != cudaSuccess ||
         per_sm < 1) {
       cudaGetLastError();
@@ -216,7 +219,7 @@ void launch_composite(const CompositeParams& cp, int64_t max_items, int sms, cud
     const int64_t resident = static_cast<int64_t>(sms) * per_sm;
     if (resident < max_items) grid = static_cast<unsigned>(resident);
   }
-  composite_kernel<kTile, kFull, kTrain><<<grid, threads, 0, stream>>>(cp);
+  composite_kernel<kTile, kFull, kTrain, kSplit><<<grid, threads, 0, stream>>>(cp);
 }
 
 int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_outputs* out,
@@ -258,8 +261,8 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     return fail(VGR_ERR_INVALID_ARGUMENT, "semantic_min_alpha must be finite and in [0, 1]");
   }
   const int ts = opt->tile_size;
-  if (ts <= 0 || ts > 16 || (ts & (ts - 1)) != 0) {
-    return fail(VGR_ERR_INVALID_ARGUMENT, "tile_size must be a power of two in [1, 16]");
+  if (ts <= 0 || ts > 32 || (ts & (ts - 1)) != 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "tile_size must be a power of two in [1, 32]");
   }
   if (ts == 2) {
     return fail(VGR_ERR_UNSUPPORTED, "tile_size=2 is not provided; use 1 (dense mode), 4, 8 or 16");
@@ -320,6 +323,9 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
                 "dense mode needs depth_tau (16-byte aligned) and tile_cutoff workspaces");
   }
   const int bin = dense ? 16 : (ray && ts == 16 && !ragged) ? 32 : ts;
+  if (train && bin == 32) {
+    return fail(VGR_ERR_UNSUPPORTED, "the differentiable form renders tile_size 4, 8 or 16");
+  }
   int64_t tiles_per_image = 0;
   int64_t global_tiles = 0;
   int tiles_x = 0, tiles_y = 0;
@@ -644,6 +650,10 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
       if (bin == 16) launch_composite<16, true, true>(cp, max_items, sms, stream);
       else if (bin == 8) launch_composite<8, true, true>(cp, max_items, sms, stream);
       else launch_composite<4, true, true>(cp, max_items, sms, stream);
+    } else if (bin == 32) {
+      if (max_items * 4 > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "raster grid exceeds CUDA limit");
+      if (full) launch_composite<16, true, false, 2>(cp, max_items, sms, stream);
+      else launch_composite<16, false, false, 2>(cp, max_items, sms, stream);
     } else if (bin == 16) {
       if (full) launch_composite<16, true, false>(cp, max_items, sms, stream);
       else launch_composite<16, false, false>(cp, max_items, sms, stream);

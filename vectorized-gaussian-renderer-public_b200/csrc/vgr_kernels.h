@@ -318,7 +318,7 @@ __global__ void sort_onesweep_kernel(SortParams p);
 __global__ void tile_scan_kernel(BucketParams p);
 __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
-template <int kTile, bool kFull, bool kTrain>
+template <int kTile, bool kFull, bool kTrain, int kSplit>
 __global__ void composite_kernel(CompositeParams p);
 template <int kTile, bool kFull, int kSplit>
 __global__ void composite_ray_kernel(CompositeParams p);

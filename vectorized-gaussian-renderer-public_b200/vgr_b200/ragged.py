@@ -89,8 +89,8 @@ class RaggedBatch:
 
     # ------------------------------------------------------------ layout
     def _set_tiles(self, tile_size: int) -> None:
-        if tile_size not in (4, 8, 16):
-            raise ValueError("tile_size must be 4, 8 or 16.")
+        if tile_size not in (4, 8, 16, 32):
+            raise ValueError("tile_size must be 4, 8, 16 or 32.")
         self.tile_size = tile_size
         offsets = [0]
         most = 0
@@ -334,7 +334,7 @@ def autotune_tile_size(
     scene_ids: torch.Tensor,
     outputs: dict[str, torch.Tensor],
     *,
-    candidates: Sequence[int] = (8, 16),
+    candidates: Sequence[int] = (8, 16, 32),
     repeats: int = 3,
     cache: dict[Any, int] | None = None,
 ) -> int:
