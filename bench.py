@@ -640,7 +640,8 @@ def run_ragged(args, device, world: int) -> dict:
     ragged = RaggedBatch(backend, work.heights, work.widths)
     outputs = ragged.outputs()
     view = poses[0].clone()
-    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16, 32))
+    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16, 32),
+                              persistent_candidates=(False, True))
     counters = ragged.calibrate(view, intr, scene_ids, outputs)
     graph = ragged.capture(view, intr, scene_ids, outputs)
     stream = torch.cuda.current_stream(device)
@@ -720,6 +721,7 @@ def run_ragged(args, device, world: int) -> dict:
         "speedup_vs_plain": round(ragged_value / plain_value, 3),
         "rgb_max_abs_vs_plain": max_abs,
         "tile_size": tile,
+        "persistent_compositor": bool(ragged.persistent_compositor),
         "autotune_ms": {str(k): round(v, 3) for k, v in ragged.autotune_ms.items()},
         "stage_ms": ragged_stages,
         "cuda_graph": True,

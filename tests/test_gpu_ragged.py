@@ -130,8 +130,12 @@ def test_autotuner_picks_a_candidate_and_caches_it():
     ids = torch.tensor(SCENE_IDS, dtype=torch.int64, device=device)
     outputs = ragged.outputs()
     cache = {}
-    tile = autotune_tile_size(ragged, vm, km, ids, outputs, candidates=(8, 16), cache=cache)
-    assert tile in (8, 16) and ragged.tile_size == tile and len(cache) == 1
-    assert autotune_tile_size(ragged, vm, km, ids, outputs, cache=cache) == tile
+    kw = {"candidates": (8, 16, 32), "persistent_candidates": (False, True), "cache": cache}
+    tile = autotune_tile_size(ragged, vm, km, ids, outputs, **kw)
+    persistent = ragged.persistent_compositor
+    assert tile in (8, 16, 32) and ragged.tile_size == tile and len(cache) == 1
+    assert len(ragged.autotune_ms) == 6
+    assert autotune_tile_size(ragged, vm, km, ids, outputs, **kw) == tile
+    assert ragged.persistent_compositor == persistent and len(cache) == 1
     ragged.render(vm, km, ids, outputs)
     _check_against_oracle(ragged, outputs, view, intr, tile)

@@ -335,42 +335,52 @@ def autotune_tile_size(
     outputs: dict[str, torch.Tensor],
     *,
     candidates: Sequence[int] = (8, 16, 32),
+    persistent_candidates: Sequence[bool] = (False,),
     repeats: int = 3,
-    cache: dict[Any, int] | None = None,
+    cache: dict[Any, Any] | None = None,
 ) -> int:
-    """Pick the fastest tile size for this rig's shape class, time each
-    candidate on the device (after calibrating its workspace) and leave
-    ``ragged`` set to the winner.  ``cache`` maps shape classes (resolution
-    multiset, scene sizes) to earlier choices."""
+    """Pick the fastest tile size (and, with ``persistent_candidates``, the
+    compositor launch: one CTA per tile or the resident work-queue grid) for
+    this rig's shape class: time each candidate on the device after
+    calibrating its workspace and leave ``ragged`` set to the winner.
+    ``cache`` maps shape classes (resolution multiset, scene sizes) to
+    earlier choices.  Returns the tile size."""
     key = (
         tuple(sorted(set(zip(ragged.heights, ragged.widths)))),
         ragged.batch,
         tuple(s.count for s in ragged.backend._scenes.values()),
+        tuple(candidates),
+        tuple(persistent_candidates),
     )
     if cache is not None and key in cache:
-        ragged._set_tiles(cache[key])
-        ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
-        return cache[key]
-    best, best_ms = None, float("inf")
-    stream = torch.cuda.current_stream(ragged.device)
-    for tile in candidates:
+        tile, persistent = cache[key]
+        ragged.persistent_compositor = persistent
         ragged._set_tiles(tile)
         ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
-        start = torch.cuda.Event(enable_timing=True)
-        stop = torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        for _ in range(repeats):
-            ragged.render(viewmats, intrinsics, scene_ids, outputs)
-        stop.record(stream)
-        stop.synchronize()
-        ms = start.elapsed_time(stop) / repeats
-        ragged.autotune_ms[tile] = ms
-        if ms < best_ms:
-            best, best_ms = tile, ms
+        return tile
+    best, best_ms = None, float("inf")
+    stream = torch.cuda.current_stream(ragged.device)
+    for persistent in persistent_candidates:
+        for tile in candidates:
+            ragged.persistent_compositor = persistent
+            ragged._set_tiles(tile)
+            ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
+            start = torch.cuda.Event(enable_timing=True)
+            stop = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            for _ in range(repeats):
+                ragged.render(viewmats, intrinsics, scene_ids, outputs)
+            stop.record(stream)
+            stop.synchronize()
+            ms = start.elapsed_time(stop) / repeats
+            ragged.autotune_ms[f"{tile}{'p' if persistent else ''}" if len(persistent_candidates) > 1 else tile] = ms
+            if ms < best_ms:
+                best, best_ms = (tile, persistent), ms
     assert best is not None
-    ragged._set_tiles(best)
+    ragged.persistent_compositor = best[1]
+    ragged._set_tiles(best[0])
     ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
     if cache is not None:
         cache[key] = best
-    return best
+    return best[0]
 
