@@ -675,7 +675,8 @@ def run_ragged(args, device, world: int) -> dict:
     plain = []
     for (h, w), cams in groups.items():
         idx = torch.tensor(cams, device=device)
-        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=tile)
+        # The backend keeps the reference's tile contract (<= 16 pixels).
+        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=min(tile, 16))
         svc = RendererService(b, height=h, width=w, max_views=len(cams))
         svc.initialize(stage=None, device=device)
         for sid, scene in work.scenes:
