@@ -292,7 +292,7 @@ def run_reference(args) -> None:
 
 
 def stage_bytes(counters: dict, scene, rig, tiles: int, sh_degree) -> dict[str, float]:
-    """Algorithmic bytes per launch of each stage (see DESIGN.md).
+    """Algorithmic bytes per launch of each stage.
 
     G Gaussians, B cameras, V visible records, I tile intersections, T tiles,
     P pixels.
@@ -616,7 +616,7 @@ RAGGED_METRIC = "Mpix/s, ragged batch (one submission, CUDA graph) vs plain form
 
 
 def run_ragged(args, device, world: int) -> dict:
-    """eight scenes (100k..3M Gaussians, SH3), 1,024 cameras
+    """Ragged batch: eight scenes (100k..3M Gaussians, SH3), 1,024 cameras
     of mixed resolutions, a pose sequence.  The ragged form renders each frame
     as one submission replayed from a CUDA graph; the plain form renders the
     same frame through RendererService, one call per resolution (the fewest

@@ -5,9 +5,9 @@ for tests).  Cameras and LiDAR sensors are independent units: a batch is
 split into contiguous per-rank shards and rendered against a replica of the
 scene with no exchange on the data path.  The differentiable form trains one
 scene data-parallel over cameras, so its only exchange is the sum of the
-scene-parameter gradients across ranks once per step (SURVEY's multi-GPU
-plan: one all-reduce of ~118 MB for 500k SH3 Gaussians), done here in a few
-large coalesced buckets.  Timings are taken on each rank with CUDA events and
+scene-parameter gradients across ranks once per step (one all-reduce of
+~118 MB for 500k SH3 Gaussians), done here in a few large coalesced
+buckets.  Timings are taken on each rank with CUDA events and
 reduced with a MAX over ranks.
 """
 
