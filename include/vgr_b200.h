@@ -138,6 +138,11 @@ typedef struct vgr_workspace {
   int64_t depth_tau_capacity;    /* elements */
   int32_t* tile_cutoff;          /* [T16] */
   int64_t tile_cutoff_capacity;  /* elements */
+  /* Exact-ray mode, optional mirrors in the reference workspace layout
+   * (renderer_cuda.cu:96-97): per visible record the camera-space precision
+   * [V,6] and (precision * mean, mean^T precision mean) [V,4]. */
+  float* visible_ray_precisions;
+  float* visible_ray_precision_means;
 } vgr_workspace;
 
 /* Depth buckets of dense mode's optical-thickness cutoff (16 per octave of

@@ -224,4 +224,10 @@ def test_exact_ray_through_native_module():
     counters = ws[13].cpu().tolist()
     assert counters[0] == cpu.visible and counters[1] == cpu.intersections
     assert_bitwise_equal((ws[12] - ws[11]).cpu().numpy().astype(np.int32), cpu.tile_counts, "tile counts")
+    # The precision terms are mirrored into the reference's workspace slots
+    # 22/23 (record order), equal to the extension records.
+    prec = ws[22][: counters[0]].cpu()
+    pm = ws[23][: counters[0]].cpu()
+    assert torch.isfinite(prec).all() and torch.isfinite(pm).all()
+    assert (prec[:, 0] > 0).all() and (prec[:, 3] > 0).all() and (prec[:, 5] > 0).all()  # P is positive definite
 

@@ -837,6 +837,13 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
             p.ray_ext[r * 3 + 0] = make_float4(t[0], t[1], t[2], t[3]);
             p.ray_ext[r * 3 + 1] = make_float4(t[4], t[5], t[6], t[7]);
             p.ray_ext[r * 3 + 2] = make_float4(t[8], t[9], 0.0f, 0.0f);
+            if (p.mirror_ray_precisions) {
+              // Reference workspace layout (renderer_cuda.cu:1056-1071).
+#pragma unroll
+              for (int k = 0; k < 6; ++k) p.mirror_ray_precisions[r * 6 + k] = t[k];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) p.mirror_ray_precision_means[r * 4 + k] = t[6 + k];
+            }
           }
         }
       }

@@ -482,6 +482,10 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     pp.mirror_camera_ids = ws->visible_camera_ids;
     pp.mirror_gaussian_ids = ws->visible_gaussian_ids;
     pp.mirror_radii = ws->visible_radii;
+    if (ray && ws->visible_ray_precisions && ws->visible_ray_precision_means) {
+      pp.mirror_ray_precisions = ws->visible_ray_precisions;
+      pp.mirror_ray_precision_means = ws->visible_ray_precision_means;
+    }
     pp.record_map = train ? train->record_map : nullptr;
     pp.record_map_stride = scene->max_scene_gaussians;
     pp.gaussian_ids = scene->gaussian_ids;

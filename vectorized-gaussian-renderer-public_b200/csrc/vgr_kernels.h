@@ -66,6 +66,8 @@ struct ProjectParams {
   int32_t* mirror_camera_ids;
   int32_t* mirror_gaussian_ids;
   int32_t* mirror_radii;
+  float* mirror_ray_precisions;       // exact-ray mode: [V,6] or null
+  float* mirror_ray_precision_means;  // exact-ray mode: [V,4] or null
   int32_t* record_map;         // training: [A, record_map_stride] record of (slot, local Gaussian)
   int64_t record_map_stride;
   const int32_t* gaussian_ids; // reported id of packed Gaussian g, or null (g itself)

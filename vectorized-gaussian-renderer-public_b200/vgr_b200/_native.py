@@ -97,6 +97,8 @@ class VgrWorkspace(ctypes.Structure):
         ("depth_tau_capacity", _c_i64),
         ("tile_cutoff", _c_p),
         ("tile_cutoff_capacity", _c_i64),
+        ("visible_ray_precisions", _c_p),
+        ("visible_ray_precision_means", _c_p),
     ]
 
 

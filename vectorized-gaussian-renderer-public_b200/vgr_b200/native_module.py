@@ -435,6 +435,8 @@ def render(
     if ray_gaussian_evaluation:
         # Workspace contract of the exact-ray path (renderer_cuda.cu:2721-2730);
         # this build keeps the precision terms in its own extension records.
+        _check_dtype(workspace[K_VISIBLE_RAY_PRECISIONS], torch.float32, "visible_ray_precisions")
+        _check_dtype(workspace[K_VISIBLE_RAY_PRECISION_MEANS], torch.float32, "visible_ray_precision_means")
         _check(workspace[K_VISIBLE_RAY_PRECISIONS].numel() >= visible_capacity * 6,
                "visible ray-precision workspace is too small")
         _check(workspace[K_VISIBLE_RAY_PRECISION_MEANS].numel() >= visible_capacity * 4,
@@ -521,6 +523,9 @@ def render(
         visible_camera_ids=_ptr(workspace[K_VISIBLE_CAMERA_IDS]) if mirror else None,
         visible_gaussian_ids=_ptr(workspace[K_VISIBLE_GAUSSIAN_IDS]) if mirror else None,
         visible_radii=_ptr(workspace[K_VISIBLE_RADII]) if mirror else None,
+        visible_ray_precisions=_ptr(workspace[K_VISIBLE_RAY_PRECISIONS]) if ray_gaussian_evaluation else None,
+        visible_ray_precision_means=(_ptr(workspace[K_VISIBLE_RAY_PRECISION_MEANS])
+                                     if ray_gaussian_evaluation else None),
         depth_tau=None if depth_tau is None else depth_tau.data_ptr(),
         depth_tau_capacity=0 if depth_tau is None else depth_tau.numel(),
         tile_cutoff=None if tile_cutoff is None else tile_cutoff.data_ptr(),
