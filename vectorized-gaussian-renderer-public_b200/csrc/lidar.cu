@@ -487,6 +487,16 @@ struct TraceStats {
 
 // Visits the leaves whose boxes the ray crosses inside [tmin, *tmax], nearest
 // box first; visit(leaf) may shrink *tmax, which prunes deferred entries.
+//
+// Warp-coherent: the lanes that reach this call with the same hierarchy walk
+// it together.  The stack of node codes is the same for all of them (every
+// push is decided by ballots), each lane keeps its own entry distances and a
+// bit per entry saying whether its own ray hit that box, and each lane still
+// tests, prunes and visits exactly the boxes its own ray crosses - so every
+// ray gets the leaves it would get alone, while the warp runs one loop
+// instead of up to 32 divergent ones (coherent rays of a scan share most of
+// their nodes).  Children hit by several lanes are ordered by the majority's
+// nearer child.
 template <typename Visit>
 __device__ __forceinline__ void traverse(const LidarDescriptor& sc, int leaves, const Ray& r,
                                          float tmin, float* tmax, TraceStats& st, Visit visit) {
@@ -496,44 +506,65 @@ __device__ __forceinline__ void traverse(const LidarDescriptor& sc, int leaves, 
     visit(0);
     return;
   }
+  const unsigned group =
+      __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(sc.nodes));
+  const int lane = threadIdx.x & 31;
   int stack[kMaxStack];
+  uint32_t lanes[kMaxStack];
   float entry[kMaxStack];
   int top = 0;
   stack[top] = 0;
+  lanes[top] = group;
   entry[top] = tmin;
   ++top;
-  while (top > 0) {
+  const float kInf = __int_as_float(0x7f800000);
+  while (top > 0) {  // top, stack[] and lanes[] are the same in every lane of the group
     --top;
     const int code = stack[top];
-    if (entry[top] > *tmax) continue;
+    const bool mine = ((lanes[top] >> lane) & 1u) != 0u && entry[top] <= *tmax;
     if (code < 0) {
-      visit(~code);
+      if (mine) visit(~code);
       continue;
     }
-    ++st.nodes;
-    const BvhNode n = sc.nodes[code];
-    float el = 0.0f, er = 0.0f;
-    const bool hl = hit_box(r, n.b0.x, n.b0.y, n.b0.z, n.b0.w, n.b1.x, n.b1.y, tmin, *tmax, &el);
-    const bool hr = hit_box(r, n.b1.z, n.b1.w, n.b2.x, n.b2.y, n.b2.z, n.b2.w, tmin, *tmax, &er);
-    const int needed = static_cast<int>(hl) + static_cast<int>(hr);
+    if (!__any_sync(group, mine)) continue;
+    float el = kInf, er = kInf;
+    bool hl = false, hr = false;
+    if (mine) {
+      ++st.nodes;
+      const BvhNode n = sc.nodes[code];
+      hl = hit_box(r, n.b0.x, n.b0.y, n.b0.z, n.b0.w, n.b1.x, n.b1.y, tmin, *tmax, &el);
+      hr = hit_box(r, n.b1.z, n.b1.w, n.b2.x, n.b2.y, n.b2.z, n.b2.w, tmin, *tmax, &er);
+      if (!hl) el = kInf;
+      if (!hr) er = kInf;
+    }
+    const unsigned ml = __ballot_sync(group, hl);
+    const unsigned mr = __ballot_sync(group, hr);
+    const unsigned left_first = __ballot_sync(group, hl && hr && el <= er);
+    const int needed = static_cast<int>(ml != 0u) + static_cast<int>(mr != 0u);
+    if (needed == 0) continue;
     if (top + needed > kMaxStack) {
       st.overflow = true;
       return;
     }
-    if (hl && hr) {
-      const bool left_near = el <= er;
-      stack[top] = left_near ? n.c.y : n.c.x;
+    const int4 kids = sc.nodes[code].c;  // the same node for every lane of the group
+    if (ml != 0u && mr != 0u) {
+      const bool left_near = 2 * __popc(left_first) >= __popc(ml & mr);
+      stack[top] = left_near ? kids.y : kids.x;
+      lanes[top] = left_near ? mr : ml;
       entry[top] = left_near ? er : el;
       ++top;
-      stack[top] = left_near ? n.c.x : n.c.y;
+      stack[top] = left_near ? kids.x : kids.y;
+      lanes[top] = left_near ? ml : mr;
       entry[top] = left_near ? el : er;
       ++top;
-    } else if (hl) {
-      stack[top] = n.c.x;
+    } else if (ml != 0u) {
+      stack[top] = kids.x;
+      lanes[top] = ml;
       entry[top] = el;
       ++top;
-    } else if (hr) {
-      stack[top] = n.c.y;
+    } else {
+      stack[top] = kids.y;
+      lanes[top] = mr;
       entry[top] = er;
       ++top;
     }
