@@ -580,7 +580,11 @@ __device__ __forceinline__ void add_counter(int64_t* counters, int index, uint32
   }
 }
 
-__global__ void __launch_bounds__(kLidarThreads) lidar_trace_kernel(TraceParams p) {
+// Five resident CTAs per SM (a 51-register cap, some spills to L1): the
+// traversal is latency-bound, and the extra warps beat the spills (4 / 5 / 6
+// / 8 CTAs per SM measured 24.5 / 22.3 / 23.2 / 24.9 ms per 16.8M-ray frame,
+// 28.4 ms uncapped at 80 registers).
+__global__ void __launch_bounds__(kLidarThreads, 5) lidar_trace_kernel(TraceParams p) {
   const int64_t work = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t total = p.active_count * p.rays;
   uint32_t traced = 0, bad_dir = 0, bad_scene = 0, bad_active = 0, returns_found = 0;
