@@ -194,9 +194,14 @@ __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t
 // the camera setup) until every (camera, tile) of the frame is done: no
 // CTA is launched for the grid's empty tail, and a CTA that finishes a cheap
 // tile immediately takes the next one.
+// Forward 16-pixel tiles keep three quarters of the SM's threads resident
+// (twelve 128-thread CTAs, a 40-register cap): the loop is latency- and
+// issue-bound, and the extra warps measured 2.6 % faster than half occupancy
+// at 64 registers.  Other shapes keep half occupancy.
 template <int kTile, bool kFull, bool kTrain, int kSplit>
 __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
-                                  2048 / CompositeGeometry<kTile>::kThreads / 2)
+                                  (kTile == 16 && !kTrain) ? 2048 / CompositeGeometry<kTile>::kThreads * 3 / 4
+                                                           : 2048 / CompositeGeometry<kTile>::kThreads / 2)
     composite_kernel(CompositeParams p) {
   __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
   __shared__ float4 s_cpo[kCompositeBatch];  // -conic_yy/2, lo, opacity, -
