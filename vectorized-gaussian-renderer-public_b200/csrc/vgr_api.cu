@@ -590,7 +590,9 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     if ((rc = check_launch("render: tile scan")) != VGR_OK) return rc;
     mark(3);
     int64_t sgrid = (ws->intersection_capacity + 2047) / 2048;
-    if (sgrid > static_cast<int64_t>(sms) * 8) sgrid = static_cast<int64_t>(sms) * 8;
+    // 16 CTAs per SM of grid-stride scatter (8: 1.09 ms, 16: 1.03 ms per
+    // 113.6M keys; 4: 1.18 ms).
+    if (sgrid > static_cast<int64_t>(sms) * 16) sgrid = static_cast<int64_t>(sms) * 16;
     if (sgrid < 1) sgrid = 1;
     bucket_scatter_kernel<<<static_cast<unsigned>(sgrid), 256, 0, stream>>>(bp);
     if ((rc = check_launch("render: bucket scatter")) != VGR_OK) return rc;
