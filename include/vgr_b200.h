@@ -198,9 +198,10 @@ const char* vgr_last_error(void);
 
 /* Scratch bytes vgr_render needs for a given intersection capacity, projection
  * task bound (active cameras * max scene Gaussians), global tile count and
- * active-camera bound.  The size depends on the active-camera bound (per-camera
- * plans and projection constants) and a constant part; the other bounds are
- * accepted for interface stability.  No counterpart in the reference: the
+ * active-camera bound.  The size depends only on the active-camera bound
+ * (per-camera plans and projection constants) and a constant part;
+ * max_projection_tasks and global_tiles are validated and otherwise ignored
+ * (accepted for interface stability).  No counterpart in the reference: the
  * reference sizes CUB temporary storage through the two functions below. */
 int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
                                  int64_t max_projection_tasks,
@@ -264,17 +265,25 @@ int vgr_render(const vgr_scene* scene, const vgr_cameras* cameras,
  * workspace exactly as for vgr_render; workspace->scratch and scratch_bytes
  * are ignored and a VGR_STATIC_SCRATCH_BYTES array inside the library is used
  * instead (every GPU that loads the library keeps it until exit).  The
- * scratch grows with the active cameras (160 bytes each, plus about 9 KB),
- * not with the scene or the intersections: a render of more than about
- * 104,000 active cameras fails with VGR_ERR_SCRATCH_TOO_SMALL.  Nothing is allocated.  All calls share
- * the array: calls ordered on one stream are fine, calls that overlap on the
- * GPU race.  The first call on a device looks the array's address up while
- * that device is current; make it before any stream capture. */
+ * scratch grows with the active cameras (176 bytes each, plus about 9 KB),
+ * not with the scene or the intersections: a render of more than
+ * vgr_static_scratch_max_cameras() active cameras (95,275) fails with
+ * VGR_ERR_SCRATCH_TOO_SMALL before anything is launched.  reuse_projection is
+ * refused (VGR_ERR_INVALID_ARGUMENT): the shared array may hold another
+ * call's camera plans.  Nothing is allocated.  All calls share the array:
+ * calls ordered on one stream are fine, calls that overlap on the GPU race.
+ * The first call on a device looks the array's address up while that device
+ * is current and caches it for the process; make it before any stream
+ * capture.  The address belongs to the device's primary context: do not call
+ * this after cudaDeviceReset, or from a driver-API context of one's own. */
 int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras,
                               const vgr_outputs* outputs,
                               const vgr_workspace* workspace,
                               const vgr_render_options* options, void* stream,
                               int64_t* sorted_buffer_selector);
+/* Largest active-camera count whose scratch fits in the static array of
+ * vgr_render_static_scratch (no counterpart in the reference). */
+int64_t vgr_static_scratch_max_cameras(void);
 
 /* Spatial layout of a scene (no counterpart in the reference).  Temp bytes
  * of vgr_scene_spatial_order for a scene of gaussian_count Gaussians. */

@@ -14,6 +14,9 @@ native_loader.py:15-20; LiDAR: -O3 -lineinfo, lidar_native_loader.py) plus
 travel to the GPU machine with the working tree, where
 tests/golden/make_reference_golden.py runs them to produce golden vectors.
 
+The checkout's location is the --reference argument, else the
+VGR_REFERENCE_ROOT environment variable; without either nothing is built.
+
 Usage: python oracle/build_ref.py [--reference /path/to/reference]
 """
 
@@ -25,7 +28,17 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REFERENCE = Path("/root/reference")
+
+
+def reference_root() -> Path | None:
+    """The reference checkout named by VGR_REFERENCE_ROOT, if it exists."""
+    value = os.environ.get("VGR_REFERENCE_ROOT")
+    if not value:
+        return None
+    path = Path(value)
+    return path if path.exists() else None
+
+
 NATIVE = Path("src/isaacsim_gaussian_renderer/native")
 TARGETS = {
     "vgr_reference_camera": (
@@ -39,7 +52,12 @@ TARGETS = {
 }
 
 
-def build(reference: Path = DEFAULT_REFERENCE, optional: bool = False) -> list[Path]:
+def build(reference: Path | None = None, optional: bool = False) -> list[Path]:
+    reference = reference or reference_root()
+    if reference is None:
+        if optional:
+            return []
+        raise FileNotFoundError("set VGR_REFERENCE_ROOT or pass --reference")
     native = reference / NATIVE
     if not native.exists():
         if optional:
@@ -90,7 +108,7 @@ def load_reference_module(name: str):
 
 if __name__ == "__main__":
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", type=Path, default=DEFAULT_REFERENCE)
+    parser.add_argument("--reference", type=Path, default=None)
     args = parser.parse_args()
     for path in build(args.reference):
         print(path)

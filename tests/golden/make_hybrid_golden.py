@@ -6,12 +6,13 @@ reference checkout (pure torch) and stores random Gaussian and mesh layers
 and near-equal depths) with the reference's composite in
 tests/golden/hybrid_composite.npz.
 
-Usage: python tests/golden/make_hybrid_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_hybrid_golden.py [--reference PATH]  (default: $VGR_REFERENCE_ROOT)
 """
 
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -47,7 +48,7 @@ def layers(seed: int):
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("VGR_REFERENCE_ROOT"), required="VGR_REFERENCE_ROOT" not in os.environ)
     args = parser.parse_args()
     # Load the module file alone: the package's __init__ imports optional
     # dependencies (plyfile) that this image lacks.

@@ -10,12 +10,13 @@ batch/active subsets with scene transforms) and add randomized scenes on the
 reference's randomized-oracle seeds (731, 2027, 99173, 104729) with a mix of
 planar and non-planar Gaussians.
 
-Usage: python tests/golden/make_lidar_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_lidar_golden.py [--reference PATH]  (default: $VGR_REFERENCE_ROOT)
 """
 
 from __future__ import annotations
 
 import argparse
+import os
 import math
 import sys
 from pathlib import Path
@@ -155,7 +156,7 @@ def save(name: str, case: dict, result: dict) -> None:
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    parser.add_argument("--reference", type=Path, default=os.environ.get("VGR_REFERENCE_ROOT"), required="VGR_REFERENCE_ROOT" not in os.environ)
     args = parser.parse_args()
     sys.path.insert(0, str(args.reference))
     from experiments.lidar_cpu_oracle import render_lidar_oracle

@@ -10,12 +10,13 @@ minimal stand-in module with the one call the loader makes
 (PlyData.read(path).elements[0][name] and .properties[i].name) is
 registered first; it reads the file written here with numpy.
 
-Usage: python tests/golden/make_ply_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_ply_golden.py [--reference PATH]  (default: $VGR_REFERENCE_ROOT)
 """
 
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import types
 from pathlib import Path
@@ -92,7 +93,7 @@ def plyfile_stand_in() -> types.ModuleType:
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("VGR_REFERENCE_ROOT"), required="VGR_REFERENCE_ROOT" not in os.environ)
     args = parser.parse_args()
     ply = HERE / "ply_sh3.ply"
     write_ply(ply)

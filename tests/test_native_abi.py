@@ -55,6 +55,17 @@ def test_version_and_scratch_queries_run_on_host():
     assert lib.vgr_radix_sort_double_buffer_temp_bytes(1000, 256) >= 1000 * _native.RECORD_BYTES
 
 
+def test_static_scratch_limit_is_the_largest_fitting_camera_count():
+    lib = _native.load_library()
+    limit = lib.vgr_static_scratch_max_cameras()
+    static_bytes = 16 << 20
+    # 176 bytes per active camera (plan, projection constants, tile prefix)
+    # plus a constant part of about 9 KB.
+    assert 95_000 < limit < 96_000
+    assert lib.vgr_render_scratch_bytes(1, 0, 1, limit) <= static_bytes
+    assert lib.vgr_render_scratch_bytes(1, 0, 1, limit + 1) > static_bytes
+
+
 @pytest.mark.parametrize(
     "items,segments,message",
     [

@@ -7,9 +7,11 @@ inputs, outputs and workspace buffers as vgr_render but keeps its scratch in
 a fixed array inside the library.  These tests call both entry points
 through the C ABI on the same inputs and require bit-identical outputs and
 counters, twice in a row (the shared array keeps the previous call's
-contents, so the second call checks that everything is cleared), and that a
-render needing more scratch than the array holds is refused with a clear
-error.  The file name sorts last so a run that stops at the first failure has
+contents, so the second call checks that everything is cleared), that a
+render of exactly vgr_static_scratch_max_cameras() cameras runs while one more
+camera is refused with a clear error before anything is launched, and that
+reuse_projection (which would read another call's plans from the shared
+array) is refused.  The file name sorts last so a run that stops at the first failure has
 already run every other test.
 """
 
@@ -162,19 +164,45 @@ def test_static_scratch_matches_vgr_render_twice_in_a_row():
                 assert torch.equal(got, want), name
 
 
-def test_static_scratch_refuses_oversized_render():
-    device, rig, backend = _setup()
-    lib = _native.load_library()
-    # The array holds the plans and projection constants of about 104,000
-    # active cameras (160 bytes each); 120,000 one-pixel cameras need more.
-    count = 120_000
+def _far_side_rig(count):
+    """``count`` one-pixel cameras whose scene lies behind them (nothing
+    visible): the render's cost is the per-camera setup, which is what the
+    static array's size limits."""
     view = torch.eye(4).repeat(count, 1, 1)
-    view[:, 2, 3] = 5.0
-    big_rig = CameraRig(view.contiguous(), pinhole(count, 1.0, 1.0, 0.5, 0.5), 1, 1)
-    structs = _structs(device, big_rig, backend, tiles=count)
-    structs[5]["counters"].fill_(-1)
+    view[:, 2, 3] = -5.0
+    return CameraRig(view.contiguous(), pinhole(count, 1.0, 1.0, 0.5, 0.5), 1, 1)
+
+
+def test_static_scratch_renders_at_its_camera_limit_and_refuses_one_more():
+    device, _, backend = _setup()
+    lib = _native.load_library()
+    limit = lib.vgr_static_scratch_max_cameras()
+    assert 95_000 < limit < 96_000
+    structs = _structs(device, _far_side_rig(limit), backend, tiles=limit)
+    structs[5]["alpha"].fill_(float("nan"))
     code, _ = _call(lib.vgr_render_static_scratch, device, structs)
+    assert code == 0, _native.last_error()
+    torch.cuda.synchronize()
+    assert int(structs[5]["counters"][0]) == 0 and int(structs[5]["counters"][1]) == 0
+    assert torch.all(structs[5]["alpha"] == 0.0)
+
+    over = _structs(device, _far_side_rig(limit + 1), backend, tiles=limit + 1)
+    over[5]["counters"].fill_(-1)
+    code, _ = _call(lib.vgr_render_static_scratch, device, over)
     assert code == _native.VGR_ERR_SCRATCH_TOO_SMALL
     assert "static array" in _native.last_error()
     torch.cuda.synchronize()
-    assert torch.all(structs[5]["counters"] == -1)  # nothing was launched
+    assert torch.all(over[5]["counters"] == -1)  # nothing was launched
+
+
+def test_static_scratch_refuses_reuse_projection():
+    device, rig, backend = _setup()
+    lib = _native.load_library()
+    structs = _structs(device, rig, backend)
+    structs[4].reuse_projection = 1
+    structs[5]["counters"].fill_(-1)
+    code, _ = _call(lib.vgr_render_static_scratch, device, structs)
+    assert code == _native.VGR_ERR_INVALID_ARGUMENT
+    assert "reuse_projection" in _native.last_error()
+    torch.cuda.synchronize()
+    assert torch.all(structs[5]["counters"] == -1)

@@ -99,9 +99,6 @@ extern "C" int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
     return fail(VGR_ERR_INVALID_ARGUMENT,
                 "scratch query needs positive capacity and tile count, non-negative bounds");
   }
-  const int64_t vblocks = (max_projection_tasks + kProjectChunk - 1) / kProjectChunk +
-                          max_active_cameras;
-  (void)vblocks;
   return make_scratch_layout(intersection_capacity, max_active_cameras, false).total;
 }
 

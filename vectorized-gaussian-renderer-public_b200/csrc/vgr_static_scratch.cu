@@ -15,9 +15,11 @@
 // Limits and rules:
 //  * The array is VGR_STATIC_SCRATCH_BYTES (16 MiB).  Every GPU on which the
 //    library is loaded holds it until the process exits.  The scratch grows
-//    with the active cameras (160 bytes each: plan, projection constants and
-//    tile prefix) plus about 9 KB, not with the scene or the intersections; a
-//    render of more than about 104,000 active cameras is rejected with
+//    with the active cameras (176 bytes each: a 56-byte plan, 112 bytes of
+//    projection constants and an 8-byte tile prefix entry) plus about 9 KB
+//    (header and sort histogram), not with the scene or the intersections.
+//    vgr_static_scratch_max_cameras() returns the exact limit (95,275
+//    active cameras); a larger render is rejected with
 //    VGR_ERR_SCRATCH_TOO_SMALL before anything is launched.
 //  * Every call on a device shares the one array, and it keeps the previous
 //    call's contents.  vgr_render clears everything that must start at zero
@@ -25,9 +27,15 @@
 //    stream, so back-to-back calls on one stream are correct; calls whose
 //    work overlaps on the GPU (different streams, or different host threads
 //    without ordering) race on the array and produce wrong results.
+//  * reuse_projection is refused: it would composite from the plans left in
+//    the array by whichever static-scratch call ran last on the device, which
+//    need not be the caller's previous render.
 //  * The first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress while that device is current, and caches it.  Make
-//    that first call before any stream capture begins.
+//    cudaGetSymbolAddress while that device is current, and caches it for the
+//    process.  Make that first call before any stream capture begins.  The
+//    cached address belongs to the device's primary context: after
+//    cudaDeviceReset (which unloads the library's module) or from a
+//    driver-API context of one's own, do not call this entry point.
 //  * Nothing here allocates: no cudaMalloc, cudaFree or allocating library
 //    routine is called on any path.
 #include <cuda_runtime.h>
@@ -37,6 +45,7 @@
 
 #include "../../include/vgr_b200.h"
 #include "vgr_api_internal.h"
+#include "vgr_camera.cuh"
 
 namespace {
 
@@ -69,12 +78,31 @@ int static_scratch_address(void** address) {
 
 }  // namespace
 
+extern "C" int64_t vgr_static_scratch_max_cameras(void) {
+  int64_t lo = 0;
+  int64_t hi = VGR_STATIC_SCRATCH_BYTES / 64;
+  while (lo < hi) {  // largest count whose layout fits in the array
+    const int64_t mid = (lo + hi + 1) / 2;
+    if (vgr::make_scratch_layout(1, mid, false).total <= VGR_STATIC_SCRATCH_BYTES) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
 extern "C" int vgr_render_static_scratch(const vgr_scene* scene, const vgr_cameras* cameras,
                                          const vgr_outputs* outputs,
                                          const vgr_workspace* workspace,
                                          const vgr_render_options* options, void* stream,
                                          int64_t* sorted_buffer_selector) {
   if (!workspace) return vgr::fail(VGR_ERR_INVALID_ARGUMENT, "render arguments must be non-null");
+  if (options && options->reuse_projection) {
+    return vgr::fail(VGR_ERR_INVALID_ARGUMENT,
+                     "vgr_render_static_scratch does not support reuse_projection: the shared "
+                     "static array may hold another call's camera plans; use vgr_render");
+  }
   void* address = nullptr;
   const int rc = static_scratch_address(&address);
   if (rc != VGR_OK) return rc;

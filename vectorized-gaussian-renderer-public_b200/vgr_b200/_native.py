@@ -214,6 +214,7 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
             ctypes.POINTER(_c_i64),
         ],
     ),
+    ("vgr_static_scratch_max_cameras", _c_i64, []),
     (
         "vgr_ply_canonicalize",
         ctypes.c_int,

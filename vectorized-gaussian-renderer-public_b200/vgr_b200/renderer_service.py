@@ -1,11 +1,20 @@
 """Public camera renderer service.
 
-Same lifecycle and call surface as the reference ``RendererService``
+Call surface of the reference ``RendererService``
 (src/isaacsim_gaussian_renderer/renderer_service.py:14-237): initialize,
 load_scene, update_scene_transforms, prepare_outputs, render (with optional
 caller-owned outputs and device-resident active camera ids), synchronize,
-shutdown, a render cadence (render_every_n) and service-owned outputs that
-start at the inactive contract (zeros, semantic -1).
+shutdown, a render cadence (``render_every_n``) and service-owned outputs
+that start at the inactive contract (zeros, semantic -1); same arguments,
+ValueError/RuntimeError texts and workspace identity.
+
+Structure: a ``ServiceLifecycle`` owns the device and the
+initialise-before-use guard, a ``SceneRegistry`` the packed offsets, an
+``OutputSetPool`` the service-owned outputs by batch size, and
+``RenderCadence`` decides which requests reach the backend.  ``render``
+validates the request (shapes, dtypes, residency; ids only for CPU tensors,
+never by reading device memory back), then either forwards one
+``RenderRequest`` or returns the previous outputs.
 """
 
 from __future__ import annotations
@@ -15,6 +24,7 @@ from typing import Any
 
 import torch
 
+from ._service_core import OutputSetPool, ServiceLifecycle
 from .backend import GaussianRendererBackend, RenderRequest
 from .contracts import (
     OUTPUT_SPECS,
@@ -24,6 +34,27 @@ from .contracts import (
     validate_outputs,
 )
 from .scene import GaussianScene, SceneRegistry
+
+
+class RenderCadence:
+    """Every n-th request renders, the first one included; the others return
+    the last rendered outputs."""
+
+    def __init__(self, every_n: int) -> None:
+        if every_n <= 0:
+            raise ValueError("render_every_n must be positive.")
+        self.every_n = every_n
+        self.requests = 0
+        self.last: dict[str, torch.Tensor] | None = None
+
+    def admit(self) -> bool:
+        self.requests += 1
+        return (self.requests - 1) % self.every_n == 0
+
+    def replay(self) -> dict[str, torch.Tensor]:
+        if self.last is None:
+            raise RuntimeError("Render cadence skipped before any output exists.")
+        return self.last
 
 
 class RendererService:
@@ -38,53 +69,55 @@ class RendererService:
         render_every_n: int = 1,
         allow_cpu_for_tests: bool = False,
     ) -> None:
-        if height <= 0 or width <= 0:
+        if min(height, width) <= 0:
             raise ValueError("height and width must be positive.")
-        if render_every_n <= 0:
-            raise ValueError("render_every_n must be positive.")
-        names = tuple(outputs)
-        unknown = sorted(set(names) - set(OUTPUT_SPECS))
-        if unknown:
-            raise ValueError(f"Unsupported output name(s): {', '.join(unknown)}.")
+        self._cadence = RenderCadence(render_every_n)
+        self.output_names = tuple(outputs)
+        unsupported = [name for name in sorted(set(self.output_names)) if name not in OUTPUT_SPECS]
+        if unsupported:
+            raise ValueError(f"Unsupported output name(s): {', '.join(unsupported)}.")
         self.backend = backend
         self.height = height
         self.width = width
-        self.output_names = names
         self.max_views = max_views
         self.render_every_n = render_every_n
         self.allow_cpu_for_tests = allow_cpu_for_tests
-        self.device: torch.device | None = None
         self.stage: Any | None = None
         self.registry = SceneRegistry()
         self.workspace: dict[str, torch.Tensor] = {}
-        self._owned_outputs: dict[int, dict[str, torch.Tensor]] = {}
-        self._last_outputs: dict[str, torch.Tensor] | None = None
-        self._render_request_count = 0
-        self._initialized = False
+        self._life = ServiceLifecycle("RendererService", allow_cpu_for_tests)
+        self._outputs = OutputSetPool(self._new_output_set,
+                                      still_valid=lambda found: tuple(found) == self.output_names)
 
     @property
-    def _require_cuda(self) -> bool:
-        return not self.allow_cpu_for_tests
+    def device(self) -> torch.device | None:
+        return self._life.device
 
+    # ------------------------------------------------------------ lifecycle
     def initialize(self, stage: Any, device: torch.device | str) -> None:
-        device = torch.device(device)
-        if device.type == "cuda" and device.index is None:
-            device = torch.device("cuda", torch.cuda.current_device())
-        if device.type != "cuda" and not self.allow_cpu_for_tests:
-            raise ValueError(f"RendererService requires a CUDA device; got {device}.")
+        resolved = self._life.start(device)
         self.stage = stage
-        self.device = device
-        self.backend.initialize(stage, device)
+        self.backend.initialize(stage, resolved)
         if self.max_views is not None:
             self.workspace = self.backend.allocate_workspace(
-                max_views=self.max_views,
-                height=self.height,
-                width=self.width,
-                device=device,
+                max_views=self.max_views, height=self.height, width=self.width, device=resolved,
                 dtype=torch.float32,
             )
-        self._initialized = True
+        self._life.ready = True
 
+    def synchronize(self) -> None:
+        self._life.check()
+        self.backend.synchronize()
+
+    def shutdown(self) -> None:
+        if self._life.ready:
+            self.backend.shutdown()
+        self._life.ready = False
+        self.workspace = {}
+        self._outputs.clear()
+        self._cadence.last = None
+
+    # ---------------------------------------------------------------- scenes
     def load_scene(
         self,
         scene_id: int,
@@ -96,45 +129,35 @@ class RendererService:
         features: torch.Tensor,
         semantic_ids: torch.Tensor,
     ) -> None:
-        self._require_initialized()
-        assert self.device is not None
-        scene = GaussianScene(
-            means=means,
-            scales=scales,
-            rotations=rotations,
-            opacities=opacities,
-            features=features,
-            semantic_ids=semantic_ids,
-        ).validate(device=self.device, require_cuda=self._require_cuda)
-        offset = self.registry.register(scene_id, scene)
-        self.backend.register_scene(scene_id, scene, offset)
-        # Materialise the packed offsets now so render() never allocates them.
-        self.registry.offsets_tensor(device=self.device, require_cuda=self._require_cuda)
+        device = self._life.check()
+        scene = GaussianScene(means, scales, rotations, opacities, features, semantic_ids)
+        scene.validate(device=device, require_cuda=self._life.require_cuda)
+        self.backend.register_scene(scene_id, scene, self.registry.register(scene_id, scene))
+        # The packed offsets are materialised here so render() never allocates them.
+        self.registry.offsets_tensor(device=device, require_cuda=self._life.require_cuda)
 
     def update_scene_transforms(self, scene_ids: torch.Tensor, transforms: torch.Tensor) -> None:
-        self._require_initialized()
-        assert self.device is not None
-        ensure_tensor(
-            transforms,
-            name="transforms",
-            shape=(None, 4, 4),
-            dtype=torch.float32,
-            device=self.device,
-            require_cuda=self._require_cuda,
-        )
-        if scene_ids.shape != (transforms.shape[0],):
+        device = self._life.check()
+        cuda = self._life.require_cuda
+        ensure_tensor(transforms, name="transforms", shape=(None, 4, 4), dtype=torch.float32, device=device,
+                      require_cuda=cuda)
+        count = transforms.shape[0]
+        if tuple(scene_ids.shape) != (count,):
             raise ValueError("scene_ids must have one entry per transform.")
-        ensure_tensor(
-            scene_ids,
-            name="scene_ids",
-            shape=(transforms.shape[0],),
-            dtype=torch.int64,
-            device=self.device,
-            require_cuda=self._require_cuda,
-        )
-        if not self._require_cuda:
+        ensure_tensor(scene_ids, name="scene_ids", shape=(count,), dtype=torch.int64, device=device,
+                      require_cuda=cuda)
+        if not cuda:
             self.registry.require_scene_ids(scene_ids)
         self.backend.update_scene_transforms(scene_ids, transforms)
+
+    # --------------------------------------------------------------- render
+    def prepare_outputs(self, batch: int) -> dict[str, torch.Tensor]:
+        """Allocate and retain one logical output set before steady state."""
+        self._life.check()
+        if batch <= 0:
+            raise ValueError("batch must be positive.")
+        self._check_batch(batch)
+        return self._outputs.get(batch)
 
     def render(
         self,
@@ -144,90 +167,44 @@ class RendererService:
         outputs: dict[str, torch.Tensor] | None = None,
         active_camera_ids: torch.Tensor | None = None,
     ) -> dict[str, torch.Tensor]:
-        self._require_initialized()
-        assert self.device is not None
-        require_cuda = self._require_cuda
-        batch = validate_camera_batch(
-            camera_transforms,
-            intrinsics,
-            scene_ids,
-            device=self.device,
-            require_cuda=require_cuda,
-        )
-        if self.max_views is not None and batch > self.max_views:
-            raise ValueError(f"Batch has {batch} cameras but service max_views is {self.max_views}.")
-        active_camera_ids = validate_active_camera_ids(
-            active_camera_ids,
-            batch=batch,
-            device=self.device,
-            require_cuda=require_cuda,
-        )
-        if not require_cuda:
+        device = self._life.check()
+        cuda = self._life.require_cuda
+        batch = validate_camera_batch(camera_transforms, intrinsics, scene_ids, device=device, require_cuda=cuda)
+        self._check_batch(batch)
+        active_camera_ids = validate_active_camera_ids(active_camera_ids, batch=batch, device=device,
+                                                       require_cuda=cuda)
+        if not cuda:
             self.registry.require_scene_ids(scene_ids)
-        target = outputs if outputs is not None else self._owned_output_set(batch)
-        validate_outputs(
-            target,
-            batch=batch,
-            height=self.height,
-            width=self.width,
-            device=self.device,
-            require_cuda=require_cuda,
+        target = self._outputs.get(batch) if outputs is None else outputs
+        validate_outputs(target, batch=batch, height=self.height, width=self.width, device=device,
+                         require_cuda=cuda)
+        if not self._cadence.admit():
+            return self._cadence.replay()
+        self.backend.render(
+            RenderRequest(
+                camera_transforms=camera_transforms,
+                intrinsics=intrinsics,
+                scene_ids=scene_ids,
+                scene_offsets=self.registry.offsets_tensor(device=device, require_cuda=cuda),
+                outputs=target,
+                active_camera_ids=active_camera_ids,
+                workspace=self.workspace,
+            )
         )
-        self._render_request_count += 1
-        if self.render_every_n > 1 and (self._render_request_count - 1) % self.render_every_n:
-            if self._last_outputs is None:
-                raise RuntimeError("Render cadence skipped before any output exists.")
-            return self._last_outputs
-        request = RenderRequest(
-            camera_transforms=camera_transforms,
-            intrinsics=intrinsics,
-            scene_ids=scene_ids,
-            scene_offsets=self.registry.offsets_tensor(device=self.device, require_cuda=require_cuda),
-            outputs=target,
-            active_camera_ids=active_camera_ids,
-            workspace=self.workspace,
-        )
-        self.backend.render(request)
-        self._last_outputs = target
+        self._cadence.last = target
         return target
 
-    def prepare_outputs(self, batch: int) -> dict[str, torch.Tensor]:
-        """Allocate and retain one logical output set before steady state."""
-        self._require_initialized()
-        if batch <= 0:
-            raise ValueError("batch must be positive.")
+    # -------------------------------------------------------------- helpers
+    def _check_batch(self, batch: int) -> None:
         if self.max_views is not None and batch > self.max_views:
             raise ValueError(f"Batch has {batch} cameras but service max_views is {self.max_views}.")
-        return self._owned_output_set(batch)
 
-    def synchronize(self) -> None:
-        self._require_initialized()
-        self.backend.synchronize()
-
-    def shutdown(self) -> None:
-        if self._initialized:
-            self.backend.shutdown()
-        self.workspace = {}
-        self._owned_outputs = {}
-        self._last_outputs = None
-        self._initialized = False
-
-    def _owned_output_set(self, batch: int) -> dict[str, torch.Tensor]:
-        assert self.device is not None
-        cached = self._owned_outputs.get(batch)
-        if cached is not None and tuple(cached) == self.output_names:
-            return cached
+    def _new_output_set(self, batch: int) -> dict[str, torch.Tensor]:
+        """One output set at the inactive contract: zeros, semantic -1."""
         owned: dict[str, torch.Tensor] = {}
         for name in self.output_names:
             channels, dtype = OUTPUT_SPECS[name]
-            owned[name] = torch.zeros(
-                (batch, self.height, self.width, channels), device=self.device, dtype=dtype
-            )
-            if name == "semantic_id":
-                owned[name].fill_(-1)
-        self._owned_outputs[batch] = owned
+            fill = -1 if name == "semantic_id" else 0
+            owned[name] = torch.full((batch, self.height, self.width, channels), fill, dtype=dtype,
+                                     device=self.device)
         return owned
-
-    def _require_initialized(self) -> None:
-        if not self._initialized:
-            raise RuntimeError("RendererService.initialize(stage, device) must be called first.")

@@ -1,20 +1,36 @@
 """Caller-owned Gaussian scenes and the packed-offset registry.
 
-Same canonical layout and validation as the reference
-(src/isaacsim_gaussian_renderer/scene.py:12-127): float32 means [G,3],
-activated scales [G,3], WXYZ rotations [G,4], activated opacities [G],
-features [G,F] whose first three channels are linear RGB (or, for the
-spherical-harmonics colour mode, [(d+1)^2, 3] coefficients per Gaussian),
-and int64 semantic ids [G].
+Public surface of src/isaacsim_gaussian_renderer/scene.py:12-127
+(``GaussianScene`` with ``count``/``validate``, ``SceneRegistry`` with
+``scene_ids``, ``total_gaussians``, ``register``, ``require_scene_ids`` and
+``offsets_tensor``, the same ValueError texts).  Layout: float32 means
+[G,3], activated scales [G,3], WXYZ rotations [G,4], activated opacities
+[G], features [G,F] (linear RGB in the first three channels, or the
+[(d+1)^2, 3] spherical-harmonics coefficients of the SH colour mode) and
+int64 semantic ids [G].
+
+The registry is one ``SceneTable`` of per-scene Gaussian counts; the packed
+offsets are their running sum, rebuilt as one int64 tensor per device the
+first time a device asks after a registration.
 """
 
 from __future__ import annotations
 
 from dataclasses import dataclass
+from itertools import accumulate
 
 import torch
 
-from .contracts import ensure_tensor
+from ._service_core import SceneTable, TensorField, check_fields
+
+SCENE_FIELDS: tuple[TensorField, ...] = (
+    TensorField("means", (3,), torch.float32, free_leading=True),
+    TensorField("scales", (3,), torch.float32),
+    TensorField("rotations", (4,), torch.float32),
+    TensorField("opacities", (), torch.float32),
+    TensorField("features", (None,), torch.float32),
+    TensorField("semantic_ids", (), torch.int64),
+)
 
 
 @dataclass(frozen=True)
@@ -31,64 +47,44 @@ class GaussianScene:
         return int(self.means.shape[0])
 
     def validate(self, *, device: torch.device, require_cuda: bool) -> "GaussianScene":
-        count = self.count
-        specs = (
-            ("means", self.means, (None, 3), torch.float32),
-            ("scales", self.scales, (count, 3), torch.float32),
-            ("rotations", self.rotations, (count, 4), torch.float32),
-            ("opacities", self.opacities, (count,), torch.float32),
-            ("features", self.features, (count, None), torch.float32),
-            ("semantic_ids", self.semantic_ids, (count,), torch.int64),
-        )
-        for name, tensor, shape, dtype in specs:
-            ensure_tensor(
-                tensor,
-                name=name,
-                shape=shape,
-                dtype=dtype,
-                device=device,
-                require_cuda=require_cuda,
-            )
+        check_fields(self, SCENE_FIELDS, self.count, device=device, require_cuda=require_cuda)
         return self
 
 
 class SceneRegistry:
-    """Scene id -> scene, with the packed offsets of the concatenated scenes."""
+    """Scene id -> scene, and the packed offsets of the concatenated scenes
+    in registration order (the order the backend packs them)."""
 
     def __init__(self) -> None:
-        self._scenes: dict[int, GaussianScene] = {}
-        self._offsets: list[int] = [0]
-        self._offset_tensors: dict[torch.device, torch.Tensor] = {}
+        self._table: SceneTable[GaussianScene] = SceneTable("scene")
+        self._per_device: dict[torch.device, torch.Tensor] = {}
 
     @property
     def scene_ids(self) -> tuple[int, ...]:
-        return tuple(self._scenes)
+        return self._table.ids
 
     @property
     def total_gaussians(self) -> int:
-        return self._offsets[-1]
+        return sum(scene.count for scene in self._table.values())
+
+    def offsets(self) -> list[int]:
+        """[S+1] running sum of the registered scenes' Gaussian counts."""
+        return list(accumulate((scene.count for scene in self._table.values()), initial=0))
 
     def register(self, scene_id: int, scene: GaussianScene) -> int:
-        if scene_id in self._scenes:
-            raise ValueError(f"Scene {scene_id} is already registered.")
-        offset = self._offsets[-1]
-        self._scenes[scene_id] = scene
-        self._offsets.append(offset + scene.count)
-        self._offset_tensors.clear()
-        return offset
+        """Add a scene after the ones already packed; returns its offset."""
+        start = self.total_gaussians
+        self._table.insert(scene_id, scene)
+        self._per_device = {}
+        return start
 
     def require_scene_ids(self, scene_ids: torch.Tensor) -> None:
-        if scene_ids.device.type != "cpu":
-            raise ValueError("Host scene-ID validation accepts CPU tensors only.")
-        missing = sorted({int(v) for v in scene_ids.tolist()} - set(self._scenes))
-        if missing:
-            raise ValueError(f"Unregistered scene ID(s): {missing}.")
+        self._table.check_host_ids(scene_ids)
 
     def offsets_tensor(self, *, device: torch.device, require_cuda: bool) -> torch.Tensor:
-        tensor = self._offset_tensors.get(device)
-        if tensor is None:
-            tensor = torch.tensor(self._offsets, dtype=torch.int64, device=device)
-            self._offset_tensors[device] = tensor
-        if require_cuda and tensor.device.type != "cuda":
+        if device not in self._per_device:
+            self._per_device[device] = torch.tensor(self.offsets(), dtype=torch.int64, device=device)
+        offsets = self._per_device[device]
+        if require_cuda and offsets.device.type != "cuda":
             raise ValueError("scene_offsets must be CUDA-resident.")
-        return tensor
+        return offsets
