@@ -1,26 +1,36 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 batched Gaussian-splat camera renderer.
+"""Benchmark of the B200 batched Gaussian-splat sensor renderer.
 
-python bench.py [--gpus N --steps K --warmup W] [--workload batched-1m-sh3|plain-10k-256]
-                [--impl b200|reference]
+python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
 
-One step renders the whole workload once (every camera, all four outputs).
-Default workload (batched-1m-sh3): 1,000,000 Gaussians with degree-3
-spherical harmonics, 64 pinhole cameras at 640x480 on a radius-8 orbit;
-seeded synthetic data of those shapes (no dataset).  Under torchrun each rank
-renders its own 64-camera rig against a replica of the scene (cameras are
-independent units; no collective on the data path), so scaling is weak.
+Headline workload (ragged-8scenes-1024cams): eight scenes of 100k..3M
+Gaussians (9.1M in all, degree-3 spherical harmonics), 1,024 cameras split
+32..256 per scene at mixed resolutions 128x128 / 160x120 / 320x240, a pose
+sequence with small per-frame deltas; seeded synthetic data of those laws (no
+dataset).  One step is one ragged frame: every camera, all four outputs, as
+one submission replayed from a CUDA graph.  ``value`` is Mpix/s with the
+inputs resident in HBM (scenes of 2.2 GB, far above L2); ``e2e`` is the same
+frame through the C-ABI ragged entry point with the poses copied from pinned
+host memory and every output copied back to pinned host memory inside the
+timed region.  Beside it, top-level keys give the plain form on the same
+frames (one render per resolution, the reference's drop-in form) and the
+ratio, the batched 1M-Gaussian 64-camera frame, the differentiable training
+step and the LiDAR frame.  ``roofline`` is for the ragged frame's kernel with
+the largest device time, timed live with CUDA events between its stages;
+``cpu_baseline`` times the CPU oracle on a bounded camera sample.
 
-The JSON line reports Mpix/s: ``value`` is device-timed with the inputs
-resident in HBM, ``e2e`` is the same metric through the public
-RendererService API with the camera batch copied from pinned host memory and
-all four outputs copied back to pinned host memory inside the timed region.
-``roofline`` is for the kernel stage with the largest device time, timed live
-with CUDA events recorded by the library between its stages.
-``cpu_baseline`` times the CPU oracle (the restatement of the reference
-equation, there being no CPU renderer in the reference) on a bounded camera
-sample of the same workload.  ``--impl reference`` times that CPU path as the
-reference arm.
+Under torchrun (N > 1) the ragged frame is split across ranks by estimated
+work (pixels and tile intersections per camera, from one calibration frame
+that every rank renders): each rank renders a contiguous run of cameras
+against its own replica of the scenes, with no collective on the data path;
+the frame time is the max over ranks, so the scaling is strong.
+
+``--impl reference`` times the reference's CPU path (the CPU oracle: the
+reference has no CPU renderer, so this is the restatement of its equation)
+on a camera sample of the same ragged frames, and beside it, when the
+reference's package and CUDA build are present, the reference's own CUDA
+path on the same box: the ragged frames, the batched frame and the LiDAR
+frame.
 """
 
 from __future__ import annotations
@@ -55,26 +65,34 @@ KERNEL_NAMES = {
     "composite": "composite_kernel",
 }
 FALLBACK_HBM_GBS = 6650.0
+RAGGED_WORKLOAD = "ragged-8scenes-1024cams"
 
 
 def parse_args() -> argparse.Namespace:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--steps", type=int, default=20, help="timed ragged frames")
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    parser.add_argument("--workload", choices=("batched-1m-sh3", "plain-10k-256"), default="batched-1m-sh3")
-    parser.add_argument("--cpu-sample-cameras", type=int, default=2)
-    parser.add_argument("--cameras", type=int, default=None,
-                        help="override the camera count (small profiling captures)")
+    parser.add_argument("--cpu-sample-cameras", type=int, default=16,
+                        help="ragged cameras the CPU oracle renders per step (two per scene)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--ragged-scale", type=float, default=1.0,
+                        help="scale scene sizes and camera counts of the ragged workload (small captures)")
+    parser.add_argument("--plain-steps", type=int, default=5, help="plain-form frames (0: skip)")
+    parser.add_argument("--rgb-steps", type=int, default=10,
+                        help="frames of the ragged workload on the linear-RGB equation (0: skip)")
+    parser.add_argument("--tile", type=int, default=None,
+                        help="fix the ragged tile size instead of autotuning (profiling captures)")
+    parser.add_argument("--batched-steps", type=int, default=10,
+                        help="frames of the batched 1M-Gaussian 64-camera workload (0: skip)")
+    parser.add_argument("--cameras", type=int, default=None,
+                        help="camera count of the batched workload (small profiling captures)")
     parser.add_argument("--lidar-steps", type=int, default=5,
-                        help="LiDAR frames timed after the camera workload (0: skip)")
+                        help="LiDAR frames (0: skip)")
     parser.add_argument("--lidar-sensors", type=int, default=None,
                         help="override the LiDAR sensor count (small profiling captures)")
-    parser.add_argument("--ragged-frames", type=int, default=20,
-                        help="frames of the ragged-batch workload (0: skip)")
     parser.add_argument("--aux-steps", type=int, default=10,
                         help="timed steps of PLY ingestion and the hybrid compositor (0: skip)")
     parser.add_argument("--mode-steps", type=int, default=5,
@@ -83,25 +101,11 @@ def parse_args() -> argparse.Namespace:
                         help="cameras of both mode workloads (default 32 deep-scene, 64 batched; small for ncu)")
     parser.add_argument("--diff-steps", type=int, default=10,
                         help="timed steps of the differentiable-form workload (0: skip)")
-    parser.add_argument("--ragged-scale", type=float, default=1.0,
-                        help="scale scene sizes and camera counts of the ragged workload")
+    parser.add_argument("--no-reference-cuda", action="store_true",
+                        help="reference arm: skip the reference's CUDA timings")
+    parser.add_argument("--detail", type=Path, default=None,
+                        help="also write every section's full record to this JSON file")
     return parser.parse_args()
-
-
-# --------------------------------------------------------------------------- workloads
-def make_workload(name: str, rank: int, cameras: int | None = None):
-    from vgr_b200 import workloads
-
-    if name == "plain-10k-256":
-        scene, rig = workloads.plain_workload()
-        return scene, rig, None, {"workload": name, "gaussians": 10_000, "cameras": 1,
-                                  "height": 256, "width": 256, "tile_size": 16, "color": "rgb"}
-    count = cameras or 64
-    scene, rig = workloads.batched_workload(cameras=count)
-    if rank:
-        rig = workloads.orbit_cameras(count, seed=2 + rank)
-    return scene, rig, 3, {"workload": name, "gaussians": 1_000_000, "cameras": count,
-                           "height": 480, "width": 640, "tile_size": 16, "color": "sh3"}
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -113,7 +117,7 @@ def measured_peaks() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def recorded_traffic(workload: str) -> dict[str, float]:
+def recorded_traffic(workload: str) -> dict:
     """Per-launch DRAM bytes from committed ncu summaries, if present."""
     path = ROOT / "profiles" / "traffic.json"
     try:
@@ -191,36 +195,6 @@ class ClockSampler:
         }
 
 
-# --------------------------------------------------------------------------- CPU path
-def oracle_inputs(scene, rig, cameras: list[int]):
-    from oracle import camera as oc
-
-    cov = oc.precompute_covariances(scene.scales.numpy(), scene.rotations.numpy())
-    return dict(
-        means=scene.means.numpy(), covariances=cov, opacities=scene.opacities.numpy(),
-        features=scene.features.numpy(), semantic_ids=scene.semantic_ids.numpy(),
-        registered_scene_ids=[0], scene_offsets=[0, scene.means.shape[0]],
-        viewmats=rig.viewmats.numpy()[cameras], intrinsics=rig.intrinsics.numpy()[cameras],
-        camera_scene_ids=[0] * len(cameras), height=rig.height, width=rig.width,
-    )
-
-
-def time_cpu(scene, rig, sh_degree, cameras: list[int], steps: int) -> tuple[float, float, int]:
-    """Mpix/s of the CPU oracle over ``steps`` renders of ``cameras``."""
-    from oracle import camera as oc
-
-    threads = os.cpu_count() or 1
-    kwargs = oracle_inputs(scene, rig, cameras)
-    kwargs["sh_degree"] = -1 if sh_degree is None else sh_degree
-    kwargs["threads"] = threads
-    start = time.perf_counter()
-    for _ in range(steps):
-        oc.render(**kwargs)
-    seconds = time.perf_counter() - start
-    pixels = len(cameras) * rig.height * rig.width * steps
-    return pixels / seconds / 1e6, seconds, threads
-
-
 # --------------------------------------------------------------------------- distributed
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -246,71 +220,513 @@ def barrier(world: int) -> None:
         dist.barrier()
 
 
-# --------------------------------------------------------------------------- arms
-def run_reference(args) -> None:
-    world, rank, _ = dist_setup()
-    if rank != 0:
-        return
-    scene, rig, sh_degree, config = make_workload(args.workload, 0, args.cameras)
-    sample = list(range(min(args.cpu_sample_cameras, rig.viewmats.shape[0])))
-    for _ in range(max(args.warmup, 0) and 1):
-        time_cpu(scene, rig, sh_degree, sample[:1], 1)
-    value, seconds, threads = time_cpu(scene, rig, sh_degree, sample, max(args.steps, 1))
-    sample_desc = (f"{len(sample)} of {rig.viewmats.shape[0]} cameras per step "
-                   f"({len(sample) * rig.height * rig.width} px, full scene), {args.steps} steps")
-    line = {
-        "impl": "reference",
-        "metric": METRIC,
-        "value": round(value, 3),
-        "unit": UNIT,
-        "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(seconds * 1e3 / max(args.steps, 1), 3),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic",
-        "config": config,
-        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": sample_desc},
-        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    if args.lidar_steps > 0:
-        from vgr_b200 import workloads
-
-        cfg = LIDAR_CONFIG
-        work = workloads.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
-        rays_per_s, lidar_threads, lidar_sample = lidar_cpu_sample(work)
-        line["lidar"] = {
-            "metric": LIDAR_METRIC, "value": round(rays_per_s, 1), "unit": "rays/s", "config": cfg,
-            "cpu_baseline": {"value": round(rays_per_s, 1), "unit": "rays/s", "cores": lidar_threads,
-                             "kind": "port", "sample": lidar_sample},
-        }
-    print(json.dumps(line), flush=True)
-
-
-def stage_bytes(counters: dict, scene, rig, tiles: int, sh_degree) -> dict[str, float]:
-    """Algorithmic bytes per launch of each stage.
-
-    G Gaussians, B cameras, V visible records, I tile intersections, T tiles,
-    P pixels.
-    """
-    g = scene.means.shape[0]
-    b = rig.viewmats.shape[0]
-    v = counters["visible_gaussians"]
-    i = counters["tile_intersections"]
-    p = b * rig.height * rig.width
-    color = 4 * scene.features.shape[1]
-    scene_read = g * (12 + 24 + 4)  # mean, covariance, opacity (once, L2 reuse across cameras)
+# --------------------------------------------------------------------------- workload description
+def ragged_config(work, frames: int) -> dict:
+    """The ragged workload's description, identical in both arms."""
+    groups: dict[str, int] = {}
+    for h, w in zip(work.heights, work.widths):
+        groups[f"{w}x{h}"] = groups.get(f"{w}x{h}", 0) + 1
     return {
-        "setup": b * (64 + 36 + 64 + 8) + b * 56,
-        "project_emit": scene_read + v * color + v * 48 + i * 12,
+        "workload": RAGGED_WORKLOAD,
+        "scene_gaussians": [s.means.shape[0] for _, s in work.scenes],
+        "cameras": len(work.heights),
+        "cameras_per_resolution": groups,
+        "pixels_per_frame": sum(h * w for h, w in zip(work.heights, work.widths)),
+        "sh_degree": 3,
+        "outputs": "rgb, depth, alpha, semantic_id",
+        "frames": frames,
+        "l2": "inputs larger than L2 (scenes 2.2 GB)",
+    }
+
+
+def ragged_frames(args) -> int:
+    """Pose frames generated: the workload's 100-frame sequence, or more
+    when warm-up and timed frames need them."""
+    return max(100, max(args.warmup, 0) + max(args.steps, 1))
+
+
+def group_by_resolution(work, cams=None) -> dict[tuple[int, int], list[int]]:
+    groups: dict[tuple[int, int], list[int]] = {}
+    for c in (range(len(work.heights)) if cams is None else cams):
+        groups.setdefault((work.heights[c], work.widths[c]), []).append(c)
+    return groups
+
+
+def cpu_sample_cameras(work, count: int) -> list[int]:
+    """``count`` cameras spread over the scenes: the first cameras of each
+    scene in turn (cameras are grouped by scene)."""
+    ids = work.scene_ids.tolist()
+    firsts = {}
+    for c, sid in enumerate(ids):
+        firsts.setdefault(sid, []).append(c)
+    picked: list[int] = []
+    k = 0
+    while len(picked) < count and any(k < len(v) for v in firsts.values()):
+        for sid in sorted(firsts):
+            if k < len(firsts[sid]) and len(picked) < count:
+                picked.append(firsts[sid][k])
+        k += 1
+    return sorted(picked)
+
+
+# --------------------------------------------------------------------------- CPU path
+class RaggedOracle:
+    """The CPU oracle over the ragged scenes (all registered, covariances
+    precomputed once), rendering camera subsets of the ragged frames."""
+
+    def __init__(self, work) -> None:
+        from oracle import camera as oc
+
+        self.oc = oc
+        self.work = work
+        scenes = [s for _, s in work.scenes]
+        self.kwargs = dict(
+            means=np.concatenate([s.means.numpy() for s in scenes]),
+            covariances=oc.precompute_covariances(np.concatenate([s.scales.numpy() for s in scenes]),
+                                                  np.concatenate([s.rotations.numpy() for s in scenes])),
+            opacities=np.concatenate([s.opacities.numpy() for s in scenes]),
+            features=np.concatenate([s.features.numpy() for s in scenes]),
+            semantic_ids=np.concatenate([s.semantic_ids.numpy() for s in scenes]),
+            registered_scene_ids=np.array([sid for sid, _ in work.scenes], dtype=np.int64),
+            scene_offsets=np.cumsum([0] + [s.means.shape[0] for s in scenes]).astype(np.int64),
+        )
+
+    def render(self, cams: list[int], frame: int, threads: int):
+        w = self.work
+        heights = [w.heights[c] for c in cams]
+        widths = [w.widths[c] for c in cams]
+        ragged = dict(
+            widths=widths, heights=heights,
+            tile_offsets=np.cumsum([0] + [-(-h // 16) * -(-x // 16) for h, x in zip(heights, widths)]),
+            pixel_offsets=np.cumsum([0] + [h * x for h, x in zip(heights, widths)]),
+        )
+        result = self.oc.render(
+            **self.kwargs, viewmats=w.viewmats[frame % w.viewmats.shape[0]].numpy()[cams],
+            intrinsics=w.intrinsics.numpy()[cams], camera_scene_ids=w.scene_ids.numpy()[cams],
+            height=max(heights), width=max(widths), sh_degree=3, threads=threads, ragged=ragged,
+        )
+        return result, int(ragged["pixel_offsets"][-1])
+
+
+def time_ragged_cpu(work, cams: list[int], steps: int, warmup: int) -> tuple[float, float, int, str]:
+    """Mpix/s of the CPU oracle rendering ``cams`` of the ragged frames,
+    one frame per step, on every host core."""
+    threads = os.cpu_count() or 1
+    oracle = RaggedOracle(work)
+    for k in range(min(warmup, 1)):
+        oracle.render(cams[:1], k, threads)
+    pixels = 0
+    start = time.perf_counter()
+    for k in range(steps):
+        _, px = oracle.render(cams, k, threads)
+        pixels += px
+    seconds = time.perf_counter() - start
+    sample = (f"{len(cams)} of {len(work.heights)} cameras per frame (two per scene, all three resolutions, "
+              f"{pixels // max(steps, 1)} px), full scenes, {steps} frames")
+    return pixels / seconds / 1e6, seconds, threads, sample
+
+
+# --------------------------------------------------------------------------- algorithmic bytes
+def camera_stage_bytes(g_total: int, feature_floats: int, visible: int, isects: int, tiles: int,
+                       pixels: int, cameras: int) -> dict[str, float]:
+    """Algorithmic bytes per launch of each camera stage, per unit as the
+    survey's camera formula counts them: the scene read once per frame
+    (G x (12 mean + 16 quaternion + 12 scale + 4 opacity + 8 semantic + 4F)),
+    a 48-byte record written once by the projection and read once by the
+    compositor, 12 bytes of key + value per intersection at emission, the
+    sort's own passes over the intersections (scatter: key + value read,
+    8-byte bucket entry written; tile sort: entry read, key + value
+    written), the compositor's 4-byte value per intersection and 28 bytes of
+    outputs per pixel."""
+    scene = g_total * (12 + 16 + 12 + 4 + 8 + 4 * feature_floats)
+    return {
+        "setup": cameras * (64 + 36 + 64 + 8 + 176),
+        "project_emit": scene + visible * 48 + isects * 12,
         "tile_scan": tiles * (4 + 8),
-        "bucket_scatter": i * (12 + 8),
-        "tile_sort": i * (8 + 12),
-        "composite": i * (4 + 48 + 8) + p * 28,
+        "bucket_scatter": isects * (12 + 8),
+        "tile_sort": isects * (8 + 12),
+        "composite": isects * 4 + visible * 48 + pixels * 28,
+    }
+
+
+def roofline_of(stage_avg: dict[str, float], stage_bytes: dict[str, float], workload: str) -> dict:
+    dominant = max(stage_avg, key=stage_avg.get)
+    peak, peak_kind = measured_peaks()
+    traffic = recorded_traffic(workload)
+    achieved = stage_bytes[dominant] / (stage_avg[dominant] / 1e3) / 1e9
+    kernel = KERNEL_NAMES[dominant]
+    return {
+        "bound": "hbm",
+        "kernel": kernel,
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "peak_source": f"hbm_gbs of {peak_kind}",
+        "traffic": traffic.get(kernel),
+        "algorithmic_bytes": int(stage_bytes[dominant]),
+        "ms": round(stage_avg[dominant], 4),
+        "issue_active_ncu": traffic.get("_issue_active", {}).get(kernel),
+    }
+
+
+# --------------------------------------------------------------------------- ragged headline
+def ragged_backend(work, device, sh_degree):
+    from vgr_b200 import CustomCudaBackend, RendererService
+
+    backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False)
+    holder = RendererService(backend, height=16, width=16, max_views=1)
+    holder.initialize(stage=None, device=device)
+    for sid, scene in work.scenes:
+        kw = scene.to(device).as_kwargs()
+        if sh_degree is None:
+            kw["features"] = kw["features"][:, :3].contiguous()
+        holder.load_scene(sid, **kw)
+    return backend, holder
+
+
+def run_ragged(args, device, world: int, rank: int, work) -> dict:
+    """The headline: the ragged frame as one CUDA-graph submission per frame
+    (the rank's share of the cameras under torchrun)."""
+    from vgr_b200 import _native
+    from vgr_b200.distributed import camera_costs, weighted_camera_shards
+    from vgr_b200.ragged import RaggedBatch, autotune_tile_size
+
+    lib = _native.load_library()
+    frames = ragged_frames(args)
+    stream = torch.cuda.current_stream(device)
+    scene_ids = work.scene_ids.to(device)
+    intr = work.intrinsics.to(device)
+    poses = work.viewmats.to(device)
+    backend, holder = ragged_backend(work, device, 3)
+
+    cams = list(range(len(work.heights)))
+    split = None
+    if world > 1:
+        # Every rank renders the whole first frame once, derives the same
+        # per-camera costs and cuts the same contiguous shards.
+        full = RaggedBatch(backend, work.heights, work.widths)
+        out_full = full.outputs()
+        full.calibrate(poses[0].contiguous(), intr, scene_ids, out_full)
+        ws = full.workspace
+        tile_offsets = [0]
+        for h, w in zip(work.heights, work.widths):
+            tile_offsets.append(tile_offsets[-1] + math.ceil(h / full.tile_size) * math.ceil(w / full.tile_size))
+        costs = camera_costs(ws["tile_starts"], ws["tile_ends"], tile_offsets,
+                             [h * w for h, w in zip(work.heights, work.widths)])
+        shards = weighted_camera_shards(costs, world)
+        cams = list(range(len(work.heights)))[shards[rank]]
+        split = {"shard_cameras": [s.stop - s.start for s in shards],
+                 "shard_cost_share": [round(sum(costs[s]) / max(sum(costs), 1e-9), 4) for s in shards]}
+        del full, out_full, ws
+        torch.cuda.empty_cache()
+    idx = torch.tensor(cams, device=device)
+    heights = [work.heights[c] for c in cams]
+    widths = [work.widths[c] for c in cams]
+    r_ids = scene_ids[idx].contiguous()
+    r_intr = intr[idx].contiguous()
+    r_poses = poses[:, idx].contiguous()
+    pixels = sum(h * w for h, w in zip(heights, widths))
+
+    ragged = RaggedBatch(backend, heights, widths)
+    outputs = ragged.outputs()
+    view = r_poses[0].clone()
+    if args.tile:
+        ragged._set_tiles(args.tile)
+        tile = args.tile
+    else:
+        tile = autotune_tile_size(ragged, view, r_intr, r_ids, outputs, candidates=(8, 16, 32),
+                                  persistent_candidates=(False, True))
+    counters = ragged.calibrate(view, r_intr, r_ids, outputs)
+    launches0 = lib.vgr_kernel_launch_count()
+    ragged.render(view, r_intr, r_ids, outputs)
+    launches_per_frame = lib.vgr_kernel_launch_count() - launches0
+    graph = ragged.capture(view, r_intr, r_ids, outputs)
+    for k in range(max(args.warmup, 3)):
+        view.copy_(r_poses[k % frames])
+        graph.replay()
+    torch.cuda.synchronize(device)
+
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    sampler.start()
+    time.sleep(0.3)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(args.steps):
+        view.copy_(r_poses[(args.warmup + k) % frames])
+        graph.replay()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    clocks = sampler.stop()
+    elapsed = max_over_ranks(start.elapsed_time(stop), world, device)
+    ms = elapsed / args.steps
+    check = ragged.check()
+    total_pixels = sum(h * w for h, w in zip(work.heights, work.widths))
+    value = total_pixels / (ms / 1e3) / 1e6
+
+    # Live stage times (eager frames with CUDA events at the stage boundaries).
+    stage_runs = []
+    for k in range(3):
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(_native.STAGE_EVENTS)]
+        ragged.set_stage_events(marks)
+        view.copy_(r_poses[k % frames])
+        ragged.render(view, r_intr, r_ids, outputs)
+        ragged.set_stage_events(None)
+        stage_runs.append(marks)
+    torch.cuda.synchronize(device)
+    stage_avg = {name: statistics.fmean(m[i].elapsed_time(m[i + 1]) for m in stage_runs)
+                 for i, name in enumerate(STAGES)}
+    g_total = sum(s.means.shape[0] for _, s in work.scenes)
+    sbytes = camera_stage_bytes(g_total, 48, counters["visible_gaussians"], counters["tile_intersections"],
+                                ragged.total_tiles, pixels, len(cams))
+    roofline = roofline_of(stage_avg, sbytes, RAGGED_WORKLOAD)
+    roofline["stage_ms"] = {k: round(v, 3) for k, v in stage_avg.items()}
+    roofline["stage_frac_of_hbm"] = {
+        k: round(sbytes[k] / (stage_avg[k] / 1e3) / 1e9 / roofline["peak"], 4) for k in STAGES if stage_avg[k] > 0
+    }
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = ragged_e2e(args, device, world, ragged, r_poses, r_intr, r_ids, outputs, total_pixels)
+    last = {name: t.clone() for name, t in outputs.items()}
+    result = {
+        "value": value, "ms": ms, "clocks": clocks, "roofline": roofline, "e2e": e2e,
+        "launches": launches_per_frame * args.steps, "tile": tile,
+        "persistent": bool(ragged.persistent_compositor),
+        "autotune_ms": {str(k): round(v, 3) for k, v in ragged.autotune_ms.items()},
+        "counters": counters, "overflow": bool(check["visible_overflow"] or check["intersection_overflow"]),
+        "split": split, "cams": cams, "last": last, "ragged": ragged, "backend": backend, "holder": holder,
+        "poses": r_poses, "intr": r_intr, "ids": r_ids,
+    }
+    return result
+
+
+def ragged_e2e(args, device, world, ragged, poses, intr, ids, outputs, total_pixels) -> dict:
+    """End to end through the C-ABI ragged entry point: per frame, poses from
+    pinned host memory, the render, and every output back to pinned host
+    memory, pipelined over two output sets (frame k's download on a copy
+    stream overlaps frame k+1's render)."""
+    stream = torch.cuda.current_stream(device)
+    host_poses = poses.cpu().pin_memory()
+    view = poses[0].clone()
+    sets = [outputs, {name: torch.empty_like(t) for name, t in outputs.items()}]
+    host_sets = [{name: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for name, t in outputs.items()}
+                 for _ in range(2)]
+    h2d = view.numel() * 4
+    d2h = sum(t.numel() * t.element_size() for t in host_sets[0].values())
+    steps = max(2, min(args.steps, 10))
+    copy_stream = torch.cuda.Stream(device)
+
+    def run(count: int) -> float:
+        done = [None, None]
+        torch.cuda.synchronize(device)
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(count):
+            b = k % 2
+            if done[b] is not None:
+                stream.wait_event(done[b])
+            view.copy_(host_poses[k % host_poses.shape[0]], non_blocking=True)
+            ragged.render(view, intr, ids, sets[b])
+            rendered = torch.cuda.Event()
+            rendered.record(stream)
+            copy_stream.wait_event(rendered)
+            with torch.cuda.stream(copy_stream):
+                for name, t in sets[b].items():
+                    host_sets[b][name].copy_(t, non_blocking=True)
+            done[b] = torch.cuda.Event()
+            done[b].record(copy_stream)
+        for ev in done:
+            if ev is not None:
+                stream.wait_event(ev)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return max_over_ranks(e0.elapsed_time(e1), world, device)
+
+    run(2)
+    e_ms = run(steps)
+    for b in range(2):
+        for name in outputs:
+            if not torch.equal(host_sets[b][name].to(device), sets[b][name]):
+                raise RuntimeError(f"e2e: downloaded {name} differs from the device output")
+    return {
+        "value": round(total_pixels * steps / (e_ms / 1e3) / 1e6, 3),
+        "unit": UNIT,
+        "h2d_bytes_per_step": h2d,
+        "d2h_bytes_per_step": d2h,
+        "steps": steps,
+        "pipelined": "two output sets; frame k's download overlaps frame k+1's render",
+    }
+
+
+def run_plain(args, device, work, head: dict) -> dict:
+    """The plain form on the same frames: one RendererService per
+    resolution, every scene registered, one render call per resolution per
+    frame (the fewest calls the plain form allows).  Its images must equal
+    the ragged form's."""
+    from vgr_b200 import CustomCudaBackend, RendererService
+
+    frames = ragged_frames(args)
+    stream = torch.cuda.current_stream(device)
+    poses, intr, ids = head["poses"], head["intr"], head["ids"]
+    cams = head["cams"]
+    groups: dict[tuple[int, int], list[int]] = {}
+    for j, c in enumerate(cams):
+        groups.setdefault((work.heights[c], work.widths[c]), []).append(j)
+    plain = []
+    for (h, w), members in groups.items():
+        idx = torch.tensor(members, device=device)
+        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=min(head["tile"], 16))
+        svc = RendererService(b, height=h, width=w, max_views=len(members))
+        svc.initialize(stage=None, device=device)
+        for sid, scene in work.scenes:
+            svc.load_scene(sid, **scene.to(device).as_kwargs())
+        gp, gi, gs = poses[:, idx].contiguous(), intr[idx].contiguous(), ids[idx].contiguous()
+        out = svc.prepare_outputs(len(members))
+        svc.render(gp[0], gi, gs, outputs=out)
+        b.adaptive_capacity = False
+        plain.append((svc, b, gp, gi, gs, out, members))
+
+    def frame(k: int) -> None:
+        for svc, _, gp, gi, gs, out, _ in plain:
+            svc.render(gp[k % frames], gi, gs, outputs=out)
+
+    for k in range(3):
+        frame(k)
+    torch.cuda.synchronize(device)
+    steps = max(args.plain_steps, 1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(steps):
+        frame(args.warmup + k)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(stop) / steps
+    # Same frame both ways: re-render the ragged form's last frame eagerly.
+    ragged, outputs = head["ragged"], head["last"]
+    last = (args.warmup + args.steps - 1) % frames
+    view = poses[last].contiguous()
+    ragged.render(view, intr, ids, outputs)
+    frame(last)
+    torch.cuda.synchronize(device)
+    max_abs = 0.0
+    for *_, out, members in plain:
+        for j, cam in enumerate(members):
+            diff = (ragged.view(outputs, "rgb", cam) - out["rgb"][j]).abs().max().item()
+            max_abs = max(max_abs, diff)
+    overflow = any(b.check_capacity()["intersection_overflow"] or b.check_capacity()["visible_overflow"]
+                   for _, b, *_ in plain)
+    for svc, *_ in plain:
+        svc.shutdown()
+    pixels = sum(work.heights[c] * work.widths[c] for c in cams)
+    return {"value": round(pixels / (ms / 1e3) / 1e6, 3), "ms_per_frame": round(ms, 3),
+            "calls_per_frame": len(plain), "rgb_max_abs_vs_ragged": max_abs, "overflow": overflow}
+
+
+def run_ragged_rgb(args, device, work) -> dict:
+    """The ragged frames with features[0..2] as linear RGB (the reference's
+    equation), for the same-box comparison with the reference's CUDA path."""
+    from vgr_b200.ragged import RaggedBatch, autotune_tile_size
+
+    backend, holder = ragged_backend(work, device, None)
+    ids = work.scene_ids.to(device)
+    intr = work.intrinsics.to(device)
+    poses = work.viewmats.to(device)
+    ragged = RaggedBatch(backend, work.heights, work.widths)
+    outputs = ragged.outputs()
+    view = poses[0].clone()
+    autotune_tile_size(ragged, view, intr, ids, outputs, candidates=(16, 32))
+    ragged.calibrate(view, intr, ids, outputs)
+    graph = ragged.capture(view, intr, ids, outputs)
+    stream = torch.cuda.current_stream(device)
+    for k in range(3):
+        view.copy_(poses[k])
+        graph.replay()
+    torch.cuda.synchronize(device)
+    steps = max(args.rgb_steps, 2)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(steps):
+        view.copy_(poses[k % poses.shape[0]])
+        graph.replay()
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(stop) / steps
+    ragged.check()
+    holder.shutdown()
+    pixels = sum(h * w for h, w in zip(work.heights, work.widths))
+    return {"value": round(pixels / (ms / 1e3) / 1e6, 1), "ms_per_frame": round(ms, 3), "tile": ragged.tile_size}
+
+
+# --------------------------------------------------------------------------- batched 1M frame
+def run_batched(args, device) -> dict:
+    """Batched frame: 1M Gaussians SH3, 64 cameras 640x480, through
+    RendererService (one call per frame); per-stage times and the
+    compositor's roofline."""
+    from vgr_b200 import CustomCudaBackend, RendererService, _native
+    from vgr_b200.workloads import batched_workload
+
+    count = args.cameras or 64
+    scene, rig = batched_workload(cameras=count)
+
+    def frame_ms(sh_degree, with_stages: bool):
+        backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=16)
+        service = RendererService(backend, height=rig.height, width=rig.width, max_views=count)
+        service.initialize(stage=None, device=device)
+        kw = scene.to(device).as_kwargs()
+        if sh_degree is None:
+            kw["features"] = kw["features"][:, :3].contiguous()
+        service.load_scene(0, **kw)
+        view, intr = rig.viewmats.to(device), rig.intrinsics.to(device)
+        ids = torch.zeros((count,), dtype=torch.int64, device=device)
+        out = service.prepare_outputs(count)
+        service.render(view, intr, ids, outputs=out)
+        counters = backend.read_counters()
+        backend.adaptive_capacity = False
+        for _ in range(3):
+            service.render(view, intr, ids, outputs=out)
+        torch.cuda.synchronize(device)
+        steps = max(args.batched_steps, 1)
+        events = [[torch.cuda.Event(enable_timing=True) for _ in range(_native.STAGE_EVENTS)] for _ in range(steps)]
+        stream = torch.cuda.current_stream(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for k in range(steps):
+            if with_stages:
+                backend.set_stage_events(events[k])
+            service.render(view, intr, ids, outputs=out)
+        stop.record(stream)
+        torch.cuda.synchronize(device)
+        backend.set_stage_events(None)
+        ms = start.elapsed_time(stop) / steps
+        overflow = backend.check_capacity()
+        stages = None
+        if with_stages:
+            stages = {name: statistics.fmean(ev[i].elapsed_time(ev[i + 1]) for ev in events)
+                      for i, name in enumerate(STAGES)}
+        service.shutdown()
+        return ms, counters, stages, bool(overflow["visible_overflow"] or overflow["intersection_overflow"])
+
+    ms, counters, stages, overflow = frame_ms(3, True)
+    pixels = count * rig.height * rig.width
+    tiles = count * math.ceil(rig.height / 16) * math.ceil(rig.width / 16)
+    sbytes = camera_stage_bytes(scene.means.shape[0], 48, counters["visible_gaussians"],
+                                counters["tile_intersections"], tiles, pixels, count)
+    peak, _ = measured_peaks()
+    comp = sbytes["composite"] / (stages["composite"] / 1e3) / 1e9
+    rgb_ms, _, _, _ = frame_ms(None, False)
+    return {
+        "workload": f"batched-1m-sh3 (1M Gaussians SH3, {count} cameras 640x480)",
+        "value": round(pixels / (ms / 1e3) / 1e6, 1), "ms_per_frame": round(ms, 3),
+        "stage_ms": {k: round(v, 3) for k, v in stages.items()},
+        "composite_frac_of_hbm": round(comp / peak, 4),
+        "visible_records": counters["visible_gaussians"], "tile_intersections": counters["tile_intersections"],
+        "overflow": overflow,
+        "rgb_equation": {"value": round(pixels / (rgb_ms / 1e3) / 1e6, 1), "ms_per_frame": round(rgb_ms, 3)},
     }
 
 
@@ -611,133 +1027,6 @@ def run_lidar(args, device, world: int, with_cpu: bool) -> dict:
     return result
 
 
-# --------------------------------------------------------------------------- ragged batch
-RAGGED_METRIC = "Mpix/s, ragged batch (one submission, CUDA graph) vs plain form (one render per resolution)"
-
-
-def run_ragged(args, device, world: int) -> dict:
-    """Ragged batch: eight scenes (100k..3M Gaussians, SH3), 1,024 cameras
-    of mixed resolutions, a pose sequence.  The ragged form renders each frame
-    as one submission replayed from a CUDA graph; the plain form renders the
-    same frame through RendererService, one call per resolution (the fewest
-    calls the plain form allows: every scene can share a call)."""
-    from vgr_b200 import CustomCudaBackend, RendererService, workloads
-    from vgr_b200.ragged import RaggedBatch, autotune_tile_size
-
-    frames = max(args.ragged_frames, 2)
-    work = workloads.ragged_workload(frames=frames, scale=args.ragged_scale)
-    batch = len(work.heights)
-    pixels = sum(h * w for h, w in zip(work.heights, work.widths))
-    scene_ids = work.scene_ids.to(device)
-    intr = work.intrinsics.to(device)
-    poses = work.viewmats.to(device)
-
-    backend = CustomCudaBackend(sh_degree=3, output_srgb=False)
-    holder = RendererService(backend, height=16, width=16, max_views=1)
-    holder.initialize(stage=None, device=device)
-    for sid, scene in work.scenes:
-        holder.load_scene(sid, **scene.to(device).as_kwargs())
-    ragged = RaggedBatch(backend, work.heights, work.widths)
-    outputs = ragged.outputs()
-    view = poses[0].clone()
-    tile = autotune_tile_size(ragged, view, intr, scene_ids, outputs, candidates=(8, 16, 32),
-                              persistent_candidates=(False, True))
-    counters = ragged.calibrate(view, intr, scene_ids, outputs)
-    graph = ragged.capture(view, intr, scene_ids, outputs)
-    stream = torch.cuda.current_stream(device)
-    for k in range(min(3, frames)):
-        view.copy_(poses[k])
-        graph.replay()
-    torch.cuda.synchronize(device)
-    barrier(world)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for k in range(frames):
-        view.copy_(poses[k])
-        graph.replay()
-    stop.record(stream)
-    torch.cuda.synchronize(device)
-    ragged_ms = max_over_ranks(start.elapsed_time(stop), world, device) / frames
-    check = ragged.check()
-    # Stage breakdown of one frame outside the graph (live CUDA events).
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(STAGES) + 1)]
-    ragged.set_stage_events(marks)
-    ragged.render(view, intr, scene_ids, outputs)
-    ragged.set_stage_events(None)
-    torch.cuda.synchronize(device)
-    ragged_stages = {name: round(marks[k].elapsed_time(marks[k + 1]), 3) for k, name in enumerate(STAGES)}
-    last = {name: t.clone() for name, t in outputs.items()}
-
-    # Plain form: one RendererService per resolution, all scenes registered.
-    groups: dict[tuple[int, int], list[int]] = {}
-    for c, hw in enumerate(zip(work.heights, work.widths)):
-        groups.setdefault(hw, []).append(c)
-    plain = []
-    for (h, w), cams in groups.items():
-        idx = torch.tensor(cams, device=device)
-        # The backend keeps the reference's tile contract (<= 16 pixels).
-        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=min(tile, 16))
-        svc = RendererService(b, height=h, width=w, max_views=len(cams))
-        svc.initialize(stage=None, device=device)
-        for sid, scene in work.scenes:
-            svc.load_scene(sid, **scene.to(device).as_kwargs())
-        group_poses = poses[:, idx].contiguous()
-        group_intr = intr[idx].contiguous()
-        group_ids = scene_ids[idx].contiguous()
-        out = svc.prepare_outputs(len(cams))
-        svc.render(group_poses[0], group_intr, group_ids, outputs=out)
-        b.adaptive_capacity = False
-        plain.append((svc, b, group_poses, group_intr, group_ids, out, cams))
-    for k in range(min(3, frames)):
-        for svc, _, gp, gi, gs, out, _ in plain:
-            svc.render(gp[k], gi, gs, outputs=out)
-    torch.cuda.synchronize(device)
-    barrier(world)
-    start.record(stream)
-    for k in range(frames):
-        for svc, _, gp, gi, gs, out, _ in plain:
-            svc.render(gp[k], gi, gs, outputs=out)
-    stop.record(stream)
-    torch.cuda.synchronize(device)
-    plain_ms = max_over_ranks(start.elapsed_time(stop), world, device) / frames
-    overflow = any(b.check_capacity()["intersection_overflow"] or b.check_capacity()["visible_overflow"]
-                   for _, b, *_ in plain)
-    # Same last frame both ways: the per-camera images must agree.
-    max_abs = 0.0
-    for *_, out, cams in plain:
-        for j, c in enumerate(cams):
-            diff = (ragged.view(last, "rgb", c) - out["rgb"][j]).abs().max().item()
-            max_abs = max(max_abs, diff)
-    ragged_value = world * pixels / (ragged_ms / 1e3) / 1e6
-    plain_value = world * pixels / (plain_ms / 1e3) / 1e6
-    result = {
-        "metric": RAGGED_METRIC,
-        "value": round(ragged_value, 3),
-        "unit": "Mpix/s",
-        "frames": frames,
-        "ms_per_frame": round(ragged_ms, 3),
-        "plain_form_value": round(plain_value, 3),
-        "plain_form_ms_per_frame": round(plain_ms, 3),
-        "plain_form_calls_per_frame": len(plain),
-        "speedup_vs_plain": round(ragged_value / plain_value, 3),
-        "rgb_max_abs_vs_plain": max_abs,
-        "tile_size": tile,
-        "persistent_compositor": bool(ragged.persistent_compositor),
-        "autotune_ms": {str(k): round(v, 3) for k, v in ragged.autotune_ms.items()},
-        "stage_ms": ragged_stages,
-        "cuda_graph": True,
-        "config": {"workload": "ragged-8scenes-1024cams", "scene_gaussians": [s.means.shape[0] for _, s in work.scenes],
-                   "cameras": batch, "pixels_per_frame": pixels, "resolutions": sorted(groups),
-                   "visible_records": counters["visible_gaussians"],
-                   "tile_intersections": counters["tile_intersections"],
-                   "capacity_overflow": bool(check["visible_overflow"] or check["intersection_overflow"] or overflow)},
-    }
-    for svc, *_ in plain:
-        svc.shutdown()
-    holder.shutdown()
-    return result
-
-
 # --------------------------------------------------------------------------- differentiable form
 DIFF_METRIC = "fwd+bwd ms/iter, loss L2(RGB) + 0.1 L1(depth) vs a perturbed-scene target"
 
@@ -876,219 +1165,203 @@ def run_b200(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
 
-    from vgr_b200 import CustomCudaBackend, RendererService, _native
+    from vgr_b200 import workloads
 
-    scene, rig, sh_degree, config = make_workload(args.workload, rank, args.cameras)
-    batch = rig.viewmats.shape[0]
-    backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=config["tile_size"])
-    service = RendererService(backend, height=rig.height, width=rig.width, max_views=batch)
-    service.initialize(stage=None, device=device)
-    service.load_scene(0, **scene.to(device).as_kwargs())
-    viewmats = rig.viewmats.to(device)
-    intrinsics = rig.intrinsics.to(device)
-    scene_ids = torch.zeros((batch,), dtype=torch.int64, device=device)
-    outputs = service.prepare_outputs(batch)
+    frames = ragged_frames(args)
+    work = workloads.ragged_workload(frames=frames, scale=args.ragged_scale)
+    config = ragged_config(work, frames)
+    head = run_ragged(args, device, world, rank, work)
+    detail: dict = {"ragged": {k: v for k, v in head.items() if k in (
+        "value", "ms", "tile", "persistent", "autotune_ms", "counters", "overflow", "split", "launches")}}
+    detail["ragged"]["stage_ms"] = head["roofline"]["stage_ms"]
+    detail["ragged"]["stage_frac_of_hbm"] = head["roofline"]["stage_frac_of_hbm"]
 
-    # Calibrate capacity with the adaptive policy, then time in explicit mode
-    # (the capacity is checked again after the timed region).
-    service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
-    counters = backend.read_counters()
-    backend.adaptive_capacity = False
-
-    for _ in range(args.warmup):
-        service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
-    torch.cuda.synchronize(device)
-
-    stream = torch.cuda.current_stream(device)
-    events = [[torch.cuda.Event(enable_timing=True) for _ in range(_native.STAGE_EVENTS)]
-              for _ in range(args.steps)]
-    for ev in events:
-        backend.set_stage_events(ev)
-    backend.set_stage_events(None)
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
-    lib = _native.load_library()
-    sampler = ClockSampler(device.index if device.index is not None else 0)
-    barrier(world)
-    torch.cuda.synchronize(device)
-    sampler.start()
-    time.sleep(0.3)
-    launches0 = lib.vgr_kernel_launch_count()
-    start.record(stream)
-    for step in range(args.steps):
-        backend.set_stage_events(events[step])
-        service.render(viewmats, intrinsics, scene_ids, outputs=outputs)
-    stop.record(stream)
-    torch.cuda.synchronize(device)
-    launches = lib.vgr_kernel_launch_count() - launches0
-    barrier(world)
-    clocks = sampler.stop()
-    backend.set_stage_events(None)
-    elapsed_ms = max_over_ranks(start.elapsed_time(stop), world, device)
-    check = backend.check_capacity()
-    stage_ms = {name: [] for name in STAGES}
-    for ev in events:
-        for k, name in enumerate(STAGES):
-            stage_ms[name].append(ev[k].elapsed_time(ev[k + 1]))
-    stage_avg = {name: statistics.fmean(vals) for name, vals in stage_ms.items()}
-
-    pixels_per_step = batch * rig.height * rig.width
-    value = world * pixels_per_step * args.steps / (elapsed_ms / 1e3) / 1e6
-
-    # End to end through the public API with host buffers: every step uploads
-    # its cameras from pinned host memory and downloads all four outputs.
-    # Pipelined the way a serving loop runs it: two output sets, frame i's
-    # download on a copy stream overlapping frame i+1's render (a set is
-    # reused only after its download finished).  The sequential form (render,
-    # then download, in one stream) is reported beside it.
-    e2e = None
-    if not args.no_e2e:
-        host_view = rig.viewmats.pin_memory()
-        host_intr = rig.intrinsics.pin_memory()
-        sets = [outputs, {name: torch.empty_like(t) for name, t in outputs.items()}]
-        host_sets = [{name: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for name, t in outputs.items()}
-                     for _ in range(2)]
-        h2d = host_view.numel() * 4 + host_intr.numel() * 4
-        d2h = sum(t.numel() * t.element_size() for t in host_sets[0].values())
-        e2e_steps = max(2, min(args.steps, 10))
-        copy_stream = torch.cuda.Stream(device)
-
-        def e2e_run(pipelined: bool) -> float:
-            done = [None, None]
-            torch.cuda.synchronize(device)
-            barrier(world)
-            e_start = torch.cuda.Event(enable_timing=True)
-            e_stop = torch.cuda.Event(enable_timing=True)
-            e_start.record(stream)
-            for i in range(e2e_steps):
-                k = i % 2 if pipelined else 0
-                if done[k] is not None:
-                    stream.wait_event(done[k])
-                viewmats.copy_(host_view, non_blocking=True)
-                intrinsics.copy_(host_intr, non_blocking=True)
-                service.render(viewmats, intrinsics, scene_ids, outputs=sets[k])
-                rendered = torch.cuda.Event()
-                rendered.record(stream)
-                copy_stream.wait_event(rendered)
-                with torch.cuda.stream(copy_stream):
-                    for name, t in sets[k].items():
-                        host_sets[k][name].copy_(t, non_blocking=True)
-                done[k] = torch.cuda.Event()
-                done[k].record(copy_stream)
-                if not pipelined:
-                    stream.wait_event(done[k])
-            for ev in done:
-                if ev is not None:
-                    stream.wait_event(ev)
-            e_stop.record(stream)
-            torch.cuda.synchronize(device)
-            return max_over_ranks(e_start.elapsed_time(e_stop), world, device)
-
-        for pipelined in (False, True):  # warm-up of both forms
-            e2e_run(pipelined)
-        seq_ms = e2e_run(False)
-        e_ms = e2e_run(True)
-        for k in range(2):
-            for name in outputs:
-                if not torch.equal(host_sets[k][name].to(device), sets[k][name]):
-                    raise RuntimeError(f"e2e: downloaded {name} differs from the device output")
-        e2e = {
-            "value": round(world * pixels_per_step * e2e_steps / (e_ms / 1e3) / 1e6, 3),
-            "unit": UNIT,
-            "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h,
-            "steps": e2e_steps,
-            "pipelined": "two output sets; step i's download overlaps step i+1's render",
-            "sequential_value": round(world * pixels_per_step * e2e_steps / (seq_ms / 1e3) / 1e6, 3),
-        }
-
-    # Roofline of the dominant stage.
-    tiles = batch * math.ceil(rig.height / config["tile_size"]) * math.ceil(rig.width / config["tile_size"])
-    bytes_per_stage = stage_bytes(counters, scene, rig, tiles, sh_degree)
-    dominant = max(stage_avg, key=stage_avg.get)
-    peak, peak_kind = measured_peaks()
-    traffic_table = recorded_traffic(config["workload"])
-    achieved = bytes_per_stage[dominant] / (stage_avg[dominant] / 1e3) / 1e9
-    roofline = {
-        "bound": "hbm",
-        "kernel": KERNEL_NAMES[dominant],
-        "achieved": round(achieved, 1),
-        "peak": peak,
-        "unit": "GB/s",
-        "frac": round(achieved / peak, 4),
-        "peak_source": f"hbm_gbs of {peak_kind}",
-        "traffic": traffic_table.get(KERNEL_NAMES[dominant]),
-        "traffic_source": traffic_table.get("_source"),
-        # Fraction of peak instruction issue from the committed ncu capture: the compositor
-        # is issue-bound, so this, not the HBM fraction, is its binding roofline.
-        "issue_active_ncu": traffic_table.get("_issue_active", {}).get(KERNEL_NAMES[dominant]),
-        "algorithmic_bytes": int(bytes_per_stage[dominant]),
-        "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
-        "stage_frac_of_measured_hbm": {
-            k: round(bytes_per_stage[k] / (stage_avg[k] / 1e3) / 1e9 / peak, 4)
-            for k in STAGES if stage_avg[k] > 0
-        },
-    }
+    plain = rgb = batched = diff = lidar = aux = modes = None
+    if world == 1:
+        if args.plain_steps > 0:
+            plain = run_plain(args, device, work, head)
+        for key in ("ragged", "holder", "backend", "last"):
+            head.pop(key, None)
+        torch.cuda.empty_cache()
+        if args.rgb_steps > 0:
+            rgb = run_ragged_rgb(args, device, work)
+            torch.cuda.empty_cache()
+        if args.batched_steps > 0:
+            batched = run_batched(args, device)
+            torch.cuda.empty_cache()
+        if args.diff_steps > 0:
+            diff = run_differentiable(args, device, world)
+            torch.cuda.empty_cache()
+        if args.lidar_steps > 0:
+            lidar = run_lidar(args, device, world, with_cpu=not args.no_cpu_baseline)
+            torch.cuda.empty_cache()
+        if args.aux_steps > 0:
+            aux = run_aux(args, device, world)
+        if args.mode_steps > 0:
+            modes = run_modes(args, device)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = list(range(min(args.cpu_sample_cameras, batch)))
-        cpu_value, _, threads = time_cpu(scene, rig, sh_degree, sample, 1)
-        cpu_baseline = {
-            "value": round(cpu_value, 3), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(sample)} of {batch} cameras ({len(sample) * rig.height * rig.width} px), full scene, 1 render",
-        }
-
-    ragged = None
-    if args.ragged_frames > 0:
-        ragged = run_ragged(args, device, world)
-
-    differentiable = None
-    if args.diff_steps > 0:
-        differentiable = run_differentiable(args, device, world)
-
-    lidar = None
-    if args.lidar_steps > 0:
-        lidar = run_lidar(args, device, world, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
-
-    aux = run_aux(args, device, world) if args.aux_steps > 0 else None
-    modes = run_modes(args, device) if args.mode_steps > 0 and world == 1 else None
+        cams = cpu_sample_cameras(work, args.cpu_sample_cameras)
+        value, _, threads, sample = time_ragged_cpu(work, cams, 1, 1)
+        cpu_baseline = {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                        "sample": sample}
 
     if rank == 0:
+        detail.update({"plain_form": plain, "rgb_equation": rgb, "batched": batched, "differentiable": diff,
+                       "lidar": lidar, "ingest_and_hybrid": aux, "modes": modes})
         line = {
             "metric": METRIC,
-            "value": round(value, 3),
+            "value": round(head["value"], 3),
             "unit": UNIT,
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": round(elapsed_ms / args.steps, 4),
+            "ms_per_step": round(head["ms"], 4),
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {**config, "parallelism": f"camera-shard x{world}" if world > 1 else "single-gpu",
-                       "l2": "inputs larger than L2 (scene 240 MB, keys/values > 126 MB)",
-                       "visible_records": counters["visible_gaussians"],
-                       "tile_intersections": counters["tile_intersections"]},
-            "e2e": e2e,
-            "gpu_launches": int(launches),
-            "roofline": roofline,
+            "config": config,
+            "parallelism": ("single-gpu, one CUDA-graph submission per frame" if world == 1 else
+                            f"ragged frame split over {world} ranks by estimated work, no data-path collective"),
+            "e2e": head["e2e"],
+            "gpu_launches": int(head["launches"]),
+            "roofline": {k: v for k, v in head["roofline"].items() if k != "stage_frac_of_hbm"},
             "cpu_baseline": cpu_baseline,
-            "clocks": clocks,
-            "capacity_check": {k: check[k] for k in ("visible_overflow", "intersection_overflow")},
-            "ragged": ragged,
-            "differentiable": differentiable,
-            "lidar": lidar,
-            "ingest_and_hybrid": aux,
-            "modes": modes,
+            "clocks": head["clocks"],
+            "capacity_overflow": head["overflow"],
+            "autotune": {"tile": head["tile"], "persistent_compositor": head["persistent"]},
         }
+        if plain is not None:
+            line["plain_form"] = {k: plain[k] for k in ("value", "ms_per_frame", "calls_per_frame",
+                                                        "rgb_max_abs_vs_ragged")}
+            line["speedup_vs_plain"] = round(head["value"] / plain["value"], 3)
+            line["target_speedup_vs_plain"] = 3.0
+        if diff is not None:
+            line["fwd_bwd"] = {"ms_per_iter": diff["value"], "forward_ms": diff["forward_ms"],
+                               "ratio": diff["fwd_bwd_over_fwd"], "target_ratio": 2.5,
+                               "workload": diff["config"]["workload"]}
+        if batched is not None:
+            line["batched"] = {"value": batched["value"], "ms_per_frame": batched["ms_per_frame"],
+                               "composite_frac_of_hbm": batched["composite_frac_of_hbm"],
+                               "workload": "batched-1m-sh3"}
+        if rgb is not None:
+            line["rgb_equation"] = {"ragged": rgb["value"],
+                                    "batched": None if batched is None else batched["rgb_equation"]["value"],
+                                    "note": "features[0..2] as linear RGB, the reference's equation"}
+        if lidar is not None:
+            line["lidar"] = {"value": lidar["value"], "unit": "rays/s", "ms_per_frame": lidar["ms_per_frame"],
+                             "build_ms": lidar["build_ms"], "trace_ms": lidar["trace_ms"],
+                             "e2e": lidar["e2e"]["value"], "workload": lidar["config"]["workload"]}
+        text = json.dumps(detail, default=str)
+        if args.detail:
+            args.detail.parent.mkdir(parents=True, exist_ok=True)
+            args.detail.write_text(text + "\n")
+        print(text, file=sys.stderr, flush=True)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def reference_cuda_section(args, work) -> dict:
+    """The reference's own CUDA path on this box (its Python classes on its
+    CUDA build): the ragged frames (one call per resolution, features[0..2]
+    as linear RGB), the batched frame, and the LiDAR frame."""
+    from oracle import reference_cuda
+
+    reason = reference_cuda.unavailable_reason()
+    if reason is not None:
+        return {"unavailable": reason}
+    from vgr_b200 import workloads
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    sampler = ClockSampler(0)
+    sampler.start()
+    out: dict = {"equation": "features[0..2] as linear RGB (the reference's camera equation)"}
+    frames = max(min(args.steps, 10), 2)
+    ids = work.scene_ids.to(device)
+    intr = work.intrinsics.to(device)
+    poses = work.viewmats.to(device)
+    ms, totals, _ = reference_cuda.camera_groups(work.scenes, group_by_resolution(work), intr, ids, poses,
+                                                 device, frames)
+    pixels = sum(h * w for h, w in zip(work.heights, work.widths))
+    out["ragged"] = {"value": round(pixels / (ms / 1e3) / 1e6, 1), "ms_per_frame": round(ms, 3),
+                     "calls_per_frame": 3, **totals}
+    del poses
+    torch.cuda.empty_cache()
+    scene, rig = workloads.batched_workload()
+    count = rig.viewmats.shape[0]
+    ms, totals, _ = reference_cuda.camera_groups(
+        [(0, scene)], {(rig.height, rig.width): list(range(count))}, rig.intrinsics.to(device),
+        torch.zeros((count,), dtype=torch.int64, device=device), rig.viewmats.to(device)[None], device, frames)
+    out["batched"] = {"value": round(count * rig.height * rig.width / (ms / 1e3) / 1e6, 1),
+                      "ms_per_frame": round(ms, 3), **totals}
+    del scene, rig
+    torch.cuda.empty_cache()
+    if args.lidar_steps > 0:
+        cfg = LIDAR_CONFIG
+        lw = workloads.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
+        moved = [lidar_moved_means(lw.means, 100 + k).to(device) for k in range(2)]
+        ms, found = reference_cuda.lidar_frames(lw, device, max(args.lidar_steps, 1), moved,
+                                                cfg["far_plane_m"], cfg["packet"])
+        rays = lw.ray_directions.shape[0] * cfg["sensors"]
+        out["lidar"] = {"value": round(rays / (ms / 1e3), 1), "unit": "rays/s", "ms_per_frame": round(ms, 3),
+                        "returns_found": found}
+    out["clocks"] = sampler.stop()
+    return out
+
+
+def run_reference(args) -> None:
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from vgr_b200 import workloads
+
+    frames = ragged_frames(args)
+    work = workloads.ragged_workload(frames=frames, scale=args.ragged_scale)
+    config = ragged_config(work, frames)
+    cams = cpu_sample_cameras(work, args.cpu_sample_cameras)
+    steps = max(args.steps, 1)
+    value, seconds, threads, sample = time_ragged_cpu(work, cams, steps, args.warmup)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(seconds * 1e3 / steps, 3),
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": config,
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU renderer; its CPU path is the oracle's restatement of its equation",
+    }
+    if args.lidar_steps > 0:
+        from vgr_b200 import workloads as wl
+
+        cfg = LIDAR_CONFIG
+        lw = wl.lidar_workload(cfg["gaussians"], cfg["sensors"], cfg["beams"], cfg["azimuths"])
+        rays_per_s, lidar_threads, lidar_sample = lidar_cpu_sample(lw)
+        line["lidar"] = {"value": round(rays_per_s, 1), "unit": "rays/s", "cores": lidar_threads,
+                         "kind": "port", "sample": lidar_sample}
+    if not args.no_reference_cuda:
+        try:
+            line["reference_cuda"] = reference_cuda_section(args, work)
+        except Exception as error:  # report, do not fail the CPU arm
+            line["reference_cuda"] = {"unavailable": f"{type(error).__name__}: {error}"[:300]}
+    print(json.dumps(line), flush=True)
 
 
 def main() -> None:

@@ -99,6 +99,8 @@ def load() -> ctypes.CDLL:
         ]
         lib.vo_precompute_covariances.restype = None
         lib.vo_precompute_covariances.argtypes = [_p, _p, _i64, _p]
+        lib.vo_set_margin_output.restype = None
+        lib.vo_set_margin_output.argtypes = [_p]
         for name in ("vo_exp_public", "vo_log_public", "vo_srgb_public"):
             getattr(lib, name).restype = ctypes.c_float
             getattr(lib, name).argtypes = [ctypes.c_float]
@@ -133,6 +135,7 @@ class OracleResult:
     active_tiles: int
     tile_counts: np.ndarray | None
     sorted_gaussian_ids: np.ndarray | None
+    margins: np.ndarray | None = None  # [..., 3] decision margins (with_margins)
 
 
 def render(
@@ -164,10 +167,14 @@ def render(
     with_tiles: bool = False,
     ragged: dict | None = None,
     ray_gaussian_evaluation: bool = False,
+    with_margins: bool = False,
 ) -> OracleResult:
     """Render every active camera on the CPU.  ``ragged`` may carry per-camera
     ``widths``, ``heights``, ``tile_offsets``, ``pixel_offsets`` and
-    ``total_pixels``/``total_tiles`` for the mixed-resolution form."""
+    ``total_pixels``/``total_tiles`` for the mixed-resolution form.
+    ``with_margins`` also returns each pixel's decision margins (relative
+    distance of the closest alpha / power-cut, transmittance-stop and
+    depth-order decision; see vo_set_margin_output in camera_oracle.c)."""
     means = _arr(means, np.float32)
     covariances = _arr(covariances, np.float32)
     opacities = _arr(opacities, np.float32)
@@ -219,6 +226,7 @@ def render(
     tile_counts = np.zeros((tiles,), dtype=np.int32) if with_tiles else None
     stats = _Stats()
     lib = load()
+    margins = np.full((total_pixels, 3), np.inf, dtype=np.float32) if with_margins else None
     # First pass sizes the sorted-id list when requested.
     sorted_ids = None
     if with_tiles:
@@ -228,9 +236,13 @@ def render(
             raise RuntimeError("oracle render failed")
         sorted_ids = np.zeros((max(stats.intersections, 1),), dtype=np.int32)
         tile_counts[:] = 0
-    code = lib.vo_render(scene, cams, opts, _ptr(rgb), _ptr(depth), _ptr(alpha), _ptr(semantic),
-                         _ptr(tile_counts), tiles if with_tiles else 0, _ptr(sorted_ids),
-                         0 if sorted_ids is None else sorted_ids.shape[0], ctypes.byref(stats))
+    lib.vo_set_margin_output(_ptr(margins))
+    try:
+        code = lib.vo_render(scene, cams, opts, _ptr(rgb), _ptr(depth), _ptr(alpha), _ptr(semantic),
+                             _ptr(tile_counts), tiles if with_tiles else 0, _ptr(sorted_ids),
+                             0 if sorted_ids is None else sorted_ids.shape[0], ctypes.byref(stats))
+    finally:
+        lib.vo_set_margin_output(None)
     if code != 0:
         raise RuntimeError("oracle render failed")
     del keep
@@ -240,10 +252,13 @@ def render(
         depth = depth.reshape(*shape, 1)
         alpha = alpha.reshape(*shape, 1)
         semantic = semantic.reshape(*shape, 1)
+        if margins is not None:
+            margins = margins.reshape(*shape, 3)
     return OracleResult(
         rgb, depth, alpha, semantic, int(stats.visible), int(stats.intersections),
         int(stats.active_tiles), tile_counts,
         None if sorted_ids is None else sorted_ids[: stats.intersections],
+        margins,
     )
 
 

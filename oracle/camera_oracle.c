@@ -459,6 +459,27 @@ static int entry_cmp(const void* pa, const void* pb) {
   return 0;
 }
 
+/* Optional per-pixel decision margins of the screen-space compositor, three
+ * floats per pixel (NULL: not written).  For each pixel: the smallest
+ * relative distance of an evaluated record's unclamped alpha o exp(power)
+ * from the 1/255 floor, and of its power from the -20 cut; the smallest
+ * relative distance of a running transmittance T (1 - alpha) from the 1e-4
+ * stop; and the smallest relative depth gap between two consecutive blended
+ * records.  A pixel whose margins are all large cannot change when an
+ * implementation evaluates the same equation with a few ulp of different
+ * rounding (fast-math exp or division, contracted products); a small margin
+ * marks a decision that can go the other way, or two records whose order
+ * can swap.  Test instrumentation only; set with vo_set_margin_output and
+ * reset to NULL after the render. */
+static float* g_margins = NULL;
+void vo_set_margin_output(float* margins) { g_margins = margins; }
+
+static float rel_gap(float a, float b) {
+  const float d = fabsf(a - b);
+  const float m = fmaxf(fabsf(a), fabsf(b));
+  return m > 0.0f ? d / m : 0.0f;
+}
+
 typedef struct slot_info {
   int valid, slot_scene, width, height, tiles_x, tiles_y;
   int64_t camera, g_begin, g_count, tile_base, pixel_base;
@@ -677,6 +698,7 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
               if (next_t <= TRANSMITTANCE_THRESHOLD) break;
             }
           }
+          float m_alpha = INFINITY, m_trans = INFINITY, m_depth = INFINITY, last_depth = NAN;
           for (int64_t i = start; i < end && !opt->ray_eval; ++i) {
             const vo_record* rec = &records[entries[i].record];
             const float dx = cx - rec->mean_x;
@@ -684,10 +706,18 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
             const float q = fmaf(rec->conic2 * dy, dy,
                                  fmaf((2.0f * rec->conic1) * dx, dy, (rec->conic0 * dx) * dx));
             const float power = -0.5f * q;
+            if (g_margins && power <= 0.0f) m_alpha = fminf(m_alpha, rel_gap(power, -20.0f));
             if (power > 0.0f || power < -20.0f) continue;
-            const float al = fminf(MAX_ALPHA, rec->opacity * vo_exp(power));
+            const float raw = rec->opacity * vo_exp(power);
+            if (g_margins) m_alpha = fminf(m_alpha, rel_gap(raw, ALPHA_THRESHOLD));
+            const float al = fminf(MAX_ALPHA, raw);
             if (al < ALPHA_THRESHOLD) continue;
             const float next_t = tr * (1.0f - al);
+            if (g_margins) {
+              m_trans = fminf(m_trans, rel_gap(next_t, TRANSMITTANCE_THRESHOLD));
+              if (last_depth == last_depth) m_depth = fminf(m_depth, rel_gap(rec->depth, last_depth));
+              last_depth = rec->depth;
+            }
             if (next_t <= TRANSMITTANCE_THRESHOLD) break;
             const float w = tr * al;
             r = fmaf(w, rec->rgb[0], r);
@@ -701,6 +731,11 @@ int vo_render(const vo_scene* s, const vo_cameras* cams, const vo_options* opt, 
             tr = next_t;
           }
           const int64_t pix = si->pixel_base + (int64_t)y * si->width + x;
+          if (g_margins) {
+            g_margins[pix * 3 + 0] = m_alpha;
+            g_margins[pix * 3 + 1] = m_trans;
+            g_margins[pix * 3 + 2] = m_depth;
+          }
           const float out_alpha = 1.0f - tr;
           if (opt->output_srgb) {
             r = vo_srgb(r);

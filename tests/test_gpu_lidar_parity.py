@@ -24,12 +24,12 @@ def _f32(a):
     return torch.as_tensor(np.asarray(a), dtype=torch.float32).contiguous()
 
 
-def _gpu_render(case, packet=8):
+def _gpu_render(case, packet=8, **backend_kwargs):
     device = torch.device("cuda")
     sensors = case["sensors"]
     batch = sensors.shape[0]
     rays = case["rays"].shape[0]
-    backend = CudaLidarBackend(packet_size=packet)
+    backend = CudaLidarBackend(packet_size=packet, **backend_kwargs)
     service = GaussianLidarService(backend, max_sensors=batch, max_rays=rays, returns=case["kwargs"]["returns"])
     service.initialize(stage=None, device=device)
     for sid, scene in case["scenes"].items():
