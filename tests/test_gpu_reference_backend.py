@@ -146,7 +146,11 @@ def test_reference_service_chunked_logical_batch():
     physical chunks of two (cuda_backend.py:759-967)."""
     scene = synthetic_scene(7_000, seed=41, mean_half_extent=1.5, log_scale_mean=-3.5)
     rig = orbit_cameras(6, seed=4, radius=4.0, height_offset=0.6, width=64, height=48, focal=60.0)
-    service, backend = _reference_camera_service(rig, [(3, scene)], max_physical_views=2)
+    # The reference's chunked form runs with explicit capacity and a
+    # fixed-capacity sort (cuda_backend.py:192-206).
+    service, backend = _reference_camera_service(rig, [(3, scene)], max_physical_views=2, fixed_capacity_sort=True,
+                                                 adaptive_capacity=False, max_visible_records=60_000,
+                                                 max_intersections=400_000)
     device = torch.device("cuda")
     out = service.render(rig.viewmats.to(device), rig.intrinsics.to(device),
                          torch.full((6,), 3, dtype=torch.int64, device=device))

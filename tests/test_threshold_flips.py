@@ -23,7 +23,10 @@ decision (camera_oracle.c, vo_set_margin_output).  This test re-renders the
 case with the oracle and checks that every pixel the reference moved by
 more than 1e-4 has a decision within 1e-4 (relative) of its threshold, or a
 pair of blended depths within 1e-6, while such near-threshold pixels are
-rare in the frame as a whole (so the explanation is not vacuous).
+rare in the frame as a whole (so the explanation is not vacuous).  On the
+recorded case 181 of 1,228,800 pixels differ by more than 1e-4 (at most
+0.0082), every one of them near a threshold, against about 4 % of all
+pixels near one.
 """
 
 from __future__ import annotations
@@ -73,9 +76,11 @@ def test_near_threshold_pixels_are_rare(frame):
     margins = got.margins.reshape(-1, 3)
     near = (np.minimum(margins[:, 0], margins[:, 1]) < DECISION_MARGIN) | (margins[:, 2] < DEPTH_MARGIN)
     fraction = float(near.mean())
-    flagged = golden["flagged"].size / float(golden["pixels"])
-    # Every flagged pixel is near a threshold, but most near-threshold pixels
-    # do not flip; the flagged share is far below the near share, which is
-    # itself a small part of the frame.
-    assert fraction < 0.05, fraction
-    assert flagged <= fraction
+    flagged = int(golden["flagged"].size)
+    # About one pixel in twenty-five sits this close to a decision (most of
+    # them do not flip), so if the flipped pixels were unrelated to the
+    # thresholds, all of them landing among the near ones would have
+    # probability fraction ** flagged.
+    assert 0.0 < fraction < 0.1, fraction
+    assert flagged >= 50
+    assert flagged * np.log10(fraction) < -50.0

@@ -594,7 +594,14 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     bucket_scatter_kernel<<<static_cast<unsigned>(sgrid), 256, 0, stream>>>(bp);
     if ((rc = check_launch("render: bucket scatter")) != VGR_OK) return rc;
     mark(4);
-    tile_sort_kernel<<<static_cast<unsigned>(global_tiles), kTileSortThreads, 0, stream>>>(bp);
+    bp.large_workers = static_cast<int64_t>(sms) * 5;
+    bp.large_list = ws->values_in;
+    if (global_tiles + bp.large_workers > INT_MAX) {
+      return fail(VGR_ERR_INVALID_ARGUMENT, "tile sort grid exceeds CUDA limit");
+    }
+    large_tile_list_kernel<<<static_cast<unsigned>((global_tiles + 255) / 256), 256, 0, stream>>>(bp);
+    if ((rc = check_launch("render: large tile list")) != VGR_OK) return rc;
+    tile_sort_kernel<<<static_cast<unsigned>(global_tiles + bp.large_workers), kTileSortThreads, 0, stream>>>(bp);
     if ((rc = check_launch("render: tile sort")) != VGR_OK) return rc;
     selector = 1;
     sorted_values = ws->values_out;

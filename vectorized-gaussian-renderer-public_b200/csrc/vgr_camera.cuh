@@ -150,7 +150,9 @@ struct ScratchHeader {
   uint32_t pad1;
   unsigned long long visible_total;  // records reserved by the projection blocks
   unsigned long long isect_total;    // keys reserved by the projection blocks
-  uint32_t pad2[12];
+  uint32_t large_tile_queue;         // tile ticket of the tile sort's large-bucket workers
+  uint32_t large_tile_count;         // tiles listed for the large-bucket workers
+  uint32_t pad2[10];
 };
 static_assert(sizeof(ScratchHeader) == 128, "ScratchHeader layout");
 
@@ -174,6 +176,7 @@ constexpr int kMaxSortPasses = 8;
 constexpr int kTileSortThreads = 256;
 constexpr int kTileSortItems = 12;
 constexpr int kTileSortCap = kTileSortThreads * kTileSortItems;
+constexpr int kTileSortSplitBits = 11;  // depth-range splits of one bucket
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanItems = 16;
 

@@ -143,6 +143,8 @@ struct BucketParams {
   int32_t* tile_ends;
   const Record* records;       // projected records (Gaussian ids break depth ties)
   int64_t visible_capacity;
+  int64_t large_workers;       // tile sort: leading CTAs that sort the buckets above kTileSortCap
+  int32_t* large_list;         // tiles above kTileSortCap (in the consumed values_in buffer)
 };
 
 struct CompositeParams {
@@ -319,6 +321,7 @@ __global__ void sort_histogram_kernel(SortParams p);
 __global__ void sort_onesweep_kernel(SortParams p);
 __global__ void tile_scan_kernel(BucketParams p);
 __global__ void bucket_scatter_kernel(BucketParams p);
+__global__ void large_tile_list_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
 template <int kTile, bool kFull, bool kTrain, int kSplit>
 __global__ void composite_kernel(CompositeParams p);

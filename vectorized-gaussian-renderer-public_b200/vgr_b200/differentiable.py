@@ -86,6 +86,8 @@ class DifferentiableRenderer:
         self.covariance_epsilon = float(covariance_epsilon)
         self.headroom = float(headroom)
         self.device = torch.device(device) if device is not None else None
+        if self.device is not None and self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self._lib = _native.load_library()
         self._ws: dict[str, torch.Tensor] = {}
         self._visible_capacity = 0
