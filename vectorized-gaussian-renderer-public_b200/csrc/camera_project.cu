@@ -536,6 +536,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   __shared__ uint32_t s_rect_min[kProjectChunk];   // min_tx | min_ty << 16
   __shared__ uint32_t s_rect_size[kProjectChunk];  // ntx | nty << 16
   __shared__ uint32_t s_prefix[kProjectChunk + 1]; // exclusive isect prefix
+  __shared__ uint16_t s_owner[kOwnerKeys];         // key -> record rank (blocks of <= kOwnerKeys keys)
   __shared__ int32_t s_radii[kProjectChunk * 2];
   __shared__ uint32_t s_warp_vis[kProjectRounds][kProjectThreads / 32];
   __shared__ uint64_t s_warp_isect[kProjectRounds][kProjectThreads / 32];
@@ -791,6 +792,11 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         s_radii[rank * 2 + 0] = radius_x[round];
         s_radii[rank * 2 + 1] = radius_y[round];
         if (kRay) ray_rank[kRay ? round : 0] = rank;
+        // Owner of each of the record's keys, for blocks whose keys fit
+        // (the emission below falls back to a search of s_prefix otherwise).
+        for (uint64_t k = excl; k < excl + ntiles[round] && k < static_cast<uint64_t>(kOwnerKeys); ++k) {
+          s_owner[k] = static_cast<uint16_t>(rank);
+        }
       }
       block_vis += rv;
       block_isect += rt;
@@ -916,17 +922,23 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           }
         }
       }
+      const bool owner_table = nisect <= static_cast<uint32_t>(kOwnerKeys);
       for (uint32_t j = tid; j < limit && kMode != kProjectDenseCull; j += kProjectThreads) {
         // Owner record: last i with s_prefix[i] <= j.
-        uint32_t lo = 0, hi = nvis;  // invariant s_prefix[lo] <= j < s_prefix[hi]
-        while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (s_prefix[mid] <= j) lo = mid; else hi = mid;
+        uint32_t i;
+        if (owner_table) {
+          i = s_owner[j];
+        } else {
+          uint32_t lo = 0, hi = nvis;  // invariant s_prefix[lo] <= j < s_prefix[hi]
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_prefix[mid] <= j) lo = mid; else hi = mid;
+          }
+          i = lo;
         }
-        const uint32_t i = lo;
         const uint32_t local = j - s_prefix[i];
         const uint32_t ntx = s_rect_size[i] & 0xffffu;
-        const uint32_t ty = local / ntx;
+        const uint32_t ty = ntx == 1u ? local : local / ntx;  // most records span one tile column
         const uint32_t tx = local - ty * ntx;
         const uint32_t min_tx = s_rect_min[i] & 0xffffu;
         const uint32_t min_ty = s_rect_min[i] >> 16;

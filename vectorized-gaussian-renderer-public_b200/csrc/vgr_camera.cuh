@@ -160,6 +160,7 @@ constexpr int kProjectThreads = 256;
 constexpr int kProjectRounds = 2;
 constexpr int kProjectChunk = kProjectThreads * kProjectRounds;  // tasks per virtual block
 constexpr int kTicketBatch = 32;  // virtual blocks taken per queue ticket (one per lane)
+constexpr int kOwnerKeys = 2048;  // keys per block whose owners the projection tabulates
 
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
