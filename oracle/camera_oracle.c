@@ -22,7 +22,7 @@
  *     :203-245, 2190-2270  exact-ray alpha and blend-then-stop compositing
  * with every floating-point operation written in a fixed order with
  * contraction disabled (built with -ffp-contract=off; fmaf only where a fused
- * multiply-add is intended), and exp/log evaluated by the Cody-Waite/Taylor
+ * multiply-add is intended), and exp/log evaluated by the Cody-Waite/minimax
  * and atanh-series methods spelled out below.  The CUDA kernels perform the
  * identical operation sequence, so outputs agree bit for bit.  Against the
  * reference's own CUDA build (compiled with --use_fast_math, __expf/__logf)
@@ -109,8 +109,9 @@ static uint32_t float_to_bits(float f) {
 }
 
 /* exp(x): x log2 e = n + f, n = rint, f by two fma steps against a split
- * log2 e, 2^f by the degree-7 Taylor polynomial in f with c_k = (ln 2)^k/k!,
- * times 2^n built in the exponent field. */
+ * log2 e, 2^f by the degree-5 minimax polynomial on |f| <= 1/2 (relative
+ * error 7.5e-8, coefficients rounded to float; the same method and constants
+ * as the CUDA kernels' vexp), times 2^n built in the exponent field. */
 static float vo_exp(float x) {
   const float log2e_hi = 1.44269502162933349609375f;
   const float log2e_lo = 1.925963033500011079e-8f;
@@ -118,14 +119,12 @@ static float vo_exp(float x) {
   const float n = rintf(t);
   float f = fmaf(x, log2e_hi, -n);
   f = fmaf(x, log2e_lo, f);
-  float p = 1.525273380405984e-05f;
-  p = fmaf(p, f, 1.540353039338161e-04f);
-  p = fmaf(p, f, 1.333355814642844e-03f);
-  p = fmaf(p, f, 9.618129107628477e-03f);
-  p = fmaf(p, f, 5.550410866482158e-02f);
-  p = fmaf(p, f, 2.402265069591007e-01f);
-  p = fmaf(p, f, 6.931471805599453e-01f);
-  p = fmaf(p, f, 1.0f);
+  float p = 1.327647245e-03f; /* degree-5 minimax of 2^f on |f| <= 1/2 */
+  p = fmaf(p, f, 9.675540961e-03f);
+  p = fmaf(p, f, 5.550713092e-02f);
+  p = fmaf(p, f, 2.402212024e-01f);
+  p = fmaf(p, f, 6.931469440e-01f);
+  p = fmaf(p, f, 1.000000119e+00f);
   const int e = (int)n;
   return p * bits_to_float((uint32_t)(e + 127) << 23);
 }

@@ -34,12 +34,14 @@ __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a,
 __device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
 
 // exp(x) for finite x in [-87, 88]: Cody-Waite reduction x = n ln2 + r with
-// n = rint(x log2 e), r carried as f = x log2(e) - n in two fma steps, and the
-// degree-7 Taylor polynomial of 2^f = e^(f ln 2) on |f| <= 0.5 (truncation
-// error < 5e-9 relative), scaled by 2^n through the exponent field.  The
-// rounding to an integer adds and subtracts 1.5 * 2^23 (round-to-nearest-even,
-// exact for |t| < 2^22, so identical to rint), and n's integer value is read
-// from the bits of the sum: all on the FMA and integer pipes.
+// n = rint(x log2 e), r carried as f = x log2(e) - n in two fma steps, and a
+// degree-5 minimax polynomial of 2^f on |f| <= 0.5 (Remez exchange for the
+// relative error, 7.5e-8; coefficients from exp2_minimax.py, rounded to
+// float), scaled by 2^n through the exponent field: within 2.3e-7 of exp
+// over the range.  The rounding to an integer adds and subtracts 1.5 * 2^23
+// (round-to-nearest-even, exact for |t| < 2^22, so identical to rint), and
+// n's integer value is read from the bits of the sum: all on the FMA and
+// integer pipes.
 __device__ __forceinline__ float vexp(float x) {
   const float kLog2eHi = 1.44269502162933349609375f;
   const float kLog2eLo = 1.925963033500011079e-8f;
@@ -49,15 +51,12 @@ __device__ __forceinline__ float vexp(float x) {
   const float n = fsub(tm, kRoundMagic);
   float f = ffma(x, kLog2eHi, -n);
   f = ffma(x, kLog2eLo, f);
-  // c_k = (ln 2)^k / k!
-  float p = 1.525273380405984e-05f;            // k = 7
-  p = ffma(p, f, 1.540353039338161e-04f);      // k = 6
-  p = ffma(p, f, 1.333355814642844e-03f);      // k = 5
-  p = ffma(p, f, 9.618129107628477e-03f);      // k = 4
-  p = ffma(p, f, 5.550410866482158e-02f);      // k = 3
-  p = ffma(p, f, 2.402265069591007e-01f);      // k = 2
-  p = ffma(p, f, 6.931471805599453e-01f);      // k = 1
-  p = ffma(p, f, 1.0f);                        // k = 0
+  float p = 1.327647245e-03f;        // c5
+  p = ffma(p, f, 9.675540961e-03f);  // c4
+  p = ffma(p, f, 5.550713092e-02f);  // c3
+  p = ffma(p, f, 2.402212024e-01f);  // c2
+  p = ffma(p, f, 6.931469440e-01f);  // c1
+  p = ffma(p, f, 1.000000119e+00f);  // c0
   const int e = __float_as_int(tm) - 0x4b400000;  // bits of 1.5 * 2^23
   return fmul(p, __int_as_float((e + 127) << 23));
 }
