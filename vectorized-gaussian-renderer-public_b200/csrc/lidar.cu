@@ -41,6 +41,7 @@ namespace vgr {
 namespace {
 
 constexpr int kLidarThreads = 256;
+constexpr int kTraceThreads = 64;
 constexpr int kMaxStack = 64;
 constexpr int kMaxSemanticSlots = 32;
 constexpr int kMaxCluster = 16;  // candidates kept per cluster window in one traversal
@@ -580,11 +581,15 @@ __device__ __forceinline__ void add_counter(int64_t* counters, int index, uint32
   }
 }
 
-// Five resident CTAs per SM (a 51-register cap, some spills to L1): the
-// traversal is latency-bound, and the extra warps beat the spills (4 / 5 / 6
-// / 8 CTAs per SM measured 24.5 / 22.3 / 23.2 / 24.9 ms per 16.8M-ray frame,
-// 28.4 ms uncapped at 80 registers).
-__global__ void __launch_bounds__(kLidarThreads, 5) lidar_trace_kernel(TraceParams p) {
+// Two-warp CTAs, twenty resident per SM (1,280 threads and a 51-register
+// cap, some spills to L1): the traversal is latency-bound, and the extra
+// warps beat the spills (at 256 threads, 4 / 5 / 6 / 8 CTAs per SM measured
+// 24.5 / 22.3 / 23.2 / 24.9 ms per 16.8M-ray frame, 28.4 ms uncapped at 80
+// registers).  Ray costs vary a lot (hits, misses, grazing rays), and a CTA
+// keeps its slot until its slowest warp is done: small CTAs free their
+// slots at a finer grain, while the hardware scheduler still hands out
+// consecutive rays, which share most of their nodes.
+__global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TraceParams p) {
   const int64_t work = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t total = p.active_count * p.rays;
   uint32_t traced = 0, bad_dir = 0, bad_scene = 0, bad_active = 0, returns_found = 0;
@@ -1037,7 +1042,7 @@ extern "C" int vgr_render_lidar(const void* descriptors, int64_t scene_count,
   if (rc != VGR_OK) return rc;
   const int64_t work = tp.active_count * in->rays;
   if (work > 0) {
-    lidar_trace_kernel<<<grid_for(work, kLidarThreads), kLidarThreads, 0, stream>>>(tp);
+    lidar_trace_kernel<<<grid_for(work, kTraceThreads), kTraceThreads, 0, stream>>>(tp);
     if ((rc = check_launch("render_lidar: trace")) != VGR_OK) return rc;
   }
   lidar_end_kernel<<<1, 1, 0, stream>>>(counters);
