@@ -436,7 +436,7 @@ def run_ragged(args, device, world: int, rank: int, work) -> dict:
         tile = args.tile
     else:
         tile = autotune_tile_size(ragged, view, r_intr, r_ids, outputs, candidates=(8, 16, 32),
-                                  persistent_candidates=(False, True))
+                                  persistent_candidates=(False, True), shape_candidates=(0, 1, 2))
     counters = ragged.calibrate(view, r_intr, r_ids, outputs)
     launches0 = lib.vgr_kernel_launch_count()
     ragged.render(view, r_intr, r_ids, outputs)
@@ -495,7 +495,7 @@ def run_ragged(args, device, world: int, rank: int, work) -> dict:
     result = {
         "value": value, "ms": ms, "clocks": clocks, "roofline": roofline, "e2e": e2e,
         "launches": launches_per_frame * args.steps, "tile": tile,
-        "persistent": bool(ragged.persistent_compositor),
+        "persistent": bool(ragged.persistent_compositor), "shape": int(ragged.composite_shape),
         "autotune_ms": {str(k): round(v, 3) for k, v in ragged.autotune_ms.items()},
         "counters": counters, "overflow": bool(check["visible_overflow"] or check["intersection_overflow"]),
         "split": split, "cams": cams, "last": last, "ragged": ragged, "backend": backend, "holder": holder,
@@ -580,7 +580,8 @@ def run_plain(args, device, work, head: dict) -> dict:
     plain = []
     for (h, w), members in groups.items():
         idx = torch.tensor(members, device=device)
-        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=min(head["tile"], 16))
+        b = CustomCudaBackend(sh_degree=3, output_srgb=False, tile_size=min(head["tile"], 16),
+                              composite_shape=head["shape"])
         svc = RendererService(b, height=h, width=w, max_views=len(members))
         svc.initialize(stage=None, device=device)
         for sid, scene in work.scenes:
@@ -1172,7 +1173,7 @@ def run_b200(args) -> None:
     config = ragged_config(work, frames)
     head = run_ragged(args, device, world, rank, work)
     detail: dict = {"ragged": {k: v for k, v in head.items() if k in (
-        "value", "ms", "tile", "persistent", "autotune_ms", "counters", "overflow", "split", "launches")}}
+        "value", "ms", "tile", "persistent", "shape", "autotune_ms", "counters", "overflow", "split", "launches")}}
     detail["ragged"]["stage_ms"] = head["roofline"]["stage_ms"]
     detail["ragged"]["stage_frac_of_hbm"] = head["roofline"]["stage_frac_of_hbm"]
 
@@ -1232,7 +1233,8 @@ def run_b200(args) -> None:
             "cpu_baseline": cpu_baseline,
             "clocks": head["clocks"],
             "capacity_overflow": head["overflow"],
-            "autotune": {"tile": head["tile"], "persistent_compositor": head["persistent"]},
+            "autotune": {"tile": head["tile"], "persistent_compositor": head["persistent"],
+                         "composite_shape": head["shape"]},
         }
         if plain is not None:
             line["plain_form"] = {k: plain[k] for k in ("value", "ms_per_frame", "calls_per_frame",

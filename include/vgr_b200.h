@@ -184,6 +184,12 @@ typedef struct vgr_render_options {
    * (camera, tile); 1 = a resident grid taking (camera, tile) work items from
    * a device queue. */
   int32_t persistent_compositor;
+  /* Compositor CTA shape (no counterpart in the reference; 8-, 16- and
+   * 32-pixel tiles of the screen-space forward path): 0 = two pixels per
+   * thread at the tuned occupancy; 1 = one pixel per thread (8x4-pixel warp
+   * blocks, twice the threads); 2 = two pixels per thread at half
+   * occupancy.  Every shape renders the same bits. */
+  int32_t composite_shape;
 } vgr_render_options;
 
 #define VGR_STAGE_EVENTS 7

@@ -60,11 +60,11 @@ def test_plain_config_bitwise():
     assert_bitwise_equal((ends - starts).astype(np.int32), cpu.tile_counts, "per-tile counts")
 
 
-@pytest.mark.parametrize("tile_size", [4, 8, 16])
-def test_batched_tile_sizes_bitwise(tile_size):
+@pytest.mark.parametrize("tile_size,shape", [(4, 0), (8, 0), (8, 1), (16, 0), (16, 1), (16, 2)])
+def test_batched_tile_sizes_bitwise(tile_size, shape):
     scene = synthetic_scene(20_000, seed=5, mean_half_extent=1.5, log_scale_mean=-3.5)
     rig = _small_rig()
-    gpu = render_gpu([(7, scene)], rig, [7] * 4, tile_size=tile_size)
+    gpu = render_gpu([(7, scene)], rig, [7] * 4, tile_size=tile_size, composite_shape=shape)
     cpu = render_oracle([(7, scene)], rig, [7] * 4, tile_size=tile_size, with_tiles=True)
     _compare(gpu, cpu)
     assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")

@@ -45,7 +45,7 @@ def _poses(seed: int):
     return view, intr
 
 
-def _setup(tile_size, persistent_compositor=False):
+def _setup(tile_size, persistent_compositor=False, composite_shape=0):
     device = torch.device("cuda")
     # The backend keeps the reference's tile contract (<= 16); the ragged
     # form takes its own tile size (32-pixel tiles included).
@@ -57,7 +57,7 @@ def _setup(tile_size, persistent_compositor=False):
     heights = [h for h, _ in RESOLUTIONS]
     widths = [w for _, w in RESOLUTIONS]
     return RaggedBatch(backend, heights, widths, tile_size=tile_size,
-                       persistent_compositor=persistent_compositor), device
+                       persistent_compositor=persistent_compositor, composite_shape=composite_shape), device
 
 
 def _check_against_oracle(ragged, outputs, view, intr, tile_size):
@@ -87,9 +87,16 @@ def _check_against_oracle(ragged, outputs, view, intr, tile_size):
     assert counters["tile_intersections"] == intersections
 
 
-@pytest.mark.parametrize("tile_size,persistent", [(8, False), (16, False), (16, True), (32, False), (32, True)])
-def test_ragged_batch_matches_oracle_per_camera(tile_size, persistent):
-    ragged, device = _setup(tile_size, persistent)
+# Every autotuner candidate: tile size x compositor launch x CTA shape
+# (composite_shape 0 two pixels per thread, 1 one pixel per thread, 2 two
+# pixels per thread at half occupancy) renders the oracle's bits.
+@pytest.mark.parametrize(
+    "tile_size,persistent,shape",
+    [(8, False, 0), (8, False, 1), (8, True, 1), (16, False, 0), (16, True, 0), (16, False, 1), (16, True, 1),
+     (16, False, 2), (16, True, 2), (32, False, 0), (32, True, 0), (32, False, 1), (32, False, 2), (32, True, 2)],
+)
+def test_ragged_batch_matches_oracle_per_camera(tile_size, persistent, shape):
+    ragged, device = _setup(tile_size, persistent, shape)
     view, intr = _poses(1)
     vm, km = view.to(device), intr.to(device)
     ids = torch.tensor(SCENE_IDS, dtype=torch.int64, device=device)
@@ -130,12 +137,14 @@ def test_autotuner_picks_a_candidate_and_caches_it():
     ids = torch.tensor(SCENE_IDS, dtype=torch.int64, device=device)
     outputs = ragged.outputs()
     cache = {}
-    kw = {"candidates": (8, 16, 32), "persistent_candidates": (False, True), "cache": cache}
+    kw = {"candidates": (8, 16, 32), "persistent_candidates": (False, True), "shape_candidates": (0, 1, 2),
+          "cache": cache}
     tile = autotune_tile_size(ragged, vm, km, ids, outputs, **kw)
-    persistent = ragged.persistent_compositor
+    persistent, shape = ragged.persistent_compositor, ragged.composite_shape
     assert tile in (8, 16, 32) and ragged.tile_size == tile and len(cache) == 1
-    assert len(ragged.autotune_ms) == 6
+    # Tiles 8 (shapes 0, 1), 16 and 32 (shapes 0, 1, 2), each with both launches.
+    assert len(ragged.autotune_ms) == 16
     assert autotune_tile_size(ragged, vm, km, ids, outputs, **kw) == tile
-    assert ragged.persistent_compositor == persistent and len(cache) == 1
+    assert (ragged.persistent_compositor, ragged.composite_shape) == (persistent, shape) and len(cache) == 1
     ragged.render(vm, km, ids, outputs)
     _check_against_oracle(ragged, outputs, view, intr, tile)

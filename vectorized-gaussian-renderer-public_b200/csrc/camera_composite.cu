@@ -97,12 +97,13 @@ __device__ __forceinline__ void write_pixel(const CompositeParams& p, const CamP
 
 // One work item (one (camera, tile), or with kSplit > 1 one kTile-pixel
 // quadrant of a (kSplit * kTile)-pixel tile whose sorted list the quadrants
-// share); every exit is CTA-uniform.
-template <int kTile, bool kFull, bool kTrain, int kSplit>
+// share); every exit is CTA-uniform.  kPix pixels per thread: rows y and
+// y + kLaneRows of the warp block when two.
+template <int kTile, bool kFull, bool kTrain, int kSplit, int kPix>
 __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t work,
                                                float4* s_geo, float4* s_cpo, float4* s_col,
                                                uint32_t* s_mask) {
-  using Geo = CompositeGeometry<kTile>;
+  using Geo = CompositeGeometry<kTile, kPix>;
   CamPlan plan;
   int64_t local_tile;
   const int64_t item = work / (kSplit * kSplit);
@@ -128,17 +129,21 @@ __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t
   const bool lane_used = ly < Geo::kLaneRows;
   const int pixel_x = tile_x * kTile + warp_x * Geo::kBlockW + lx;
   const int pixel_y0 = tile_y * kTile + warp_y * Geo::kBlockH + ly;
-  const int pixel_y1 = pixel_y0 + Geo::kLaneRows;
-  const bool valid0 = lane_used && pixel_x < plan.width && pixel_y0 < plan.height;
-  const bool valid1 = lane_used && pixel_x < plan.width && pixel_y1 < plan.height;
   const float kNaN = __int_as_float(0x7fc00000);
   const float cx = fadd(static_cast<float>(pixel_x), 0.5f);
-  float cy0 = valid0 ? fadd(static_cast<float>(pixel_y0), 0.5f) : kNaN;
-  float cy1 = valid1 ? fadd(static_cast<float>(pixel_y1), 0.5f) : kNaN;
-
-  PixelState s0{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid0};
-  PixelState s1{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid1};
-  bool warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
+  bool valid[kPix];
+  float cy[kPix];
+  PixelState s[kPix];
+  bool all_done = true;
+#pragma unroll
+  for (int q = 0; q < kPix; ++q) {
+    const int pixel_y = pixel_y0 + q * Geo::kLaneRows;
+    valid[q] = lane_used && pixel_x < plan.width && pixel_y < plan.height;
+    cy[q] = valid[q] ? fadd(static_cast<float>(pixel_y), 0.5f) : kNaN;
+    s[q] = PixelState{1.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f, 0, 0, !valid[q]};
+    all_done = all_done && s[q].done;
+  }
+  bool warp_done = __all_sync(0xffffffffu, all_done);
 
   const int64_t range_start = p.tile_starts[global_tile];
   const int64_t range_end = p.tile_ends[global_tile];
@@ -149,8 +154,8 @@ __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t
     for (int64_t chunk = range_start; chunk < range_end; chunk += kCompositeBatch) {
       const int n = static_cast<int>(min(static_cast<int64_t>(kCompositeBatch), range_end - chunk));
       for (int j = tid; j < n; j += Geo::kThreads) {
-        stage_composite_record<kTile>(p.records[p.values[chunk + j]], tile_x0, tile_y0, s_geo[j],
-                                      s_cpo[j], s_col[j], s_mask[j]);
+        stage_composite_record<kTile, kPix>(p.records[p.values[chunk + j]], tile_x0, tile_y0, s_geo[j],
+                                            s_cpo[j], s_col[j], s_mask[j]);
       }
       __syncthreads();
       if (!warp_done) {
@@ -166,50 +171,70 @@ __device__ __forceinline__ void composite_item(const CompositeParams& p, int64_t
             const float dx = fsub(cx, geo.x);
             const float adx = fmul(fmul(geo.z, dx), dx);
             const float bdx = fmul(geo.w, dx);
-            const float dy0 = fsub(cy0, geo.y);
-            const float dy1 = fsub(cy1, geo.y);
-            const float p0 = ffma(fmul(cpo.x, dy0), dy0, ffma(bdx, dy0, adx));
-            const float p1 = ffma(fmul(cpo.x, dy1), dy1, ffma(bdx, dy1, adx));
-            const bool in0 = p0 >= cpo.y && p0 <= 0.0f;
-            const bool in1 = p1 >= cpo.y && p1 <= 0.0f;
-            if (in0 || in1) {
+            float pw[kPix];
+            bool in_range = false;
+#pragma unroll
+            for (int q = 0; q < kPix; ++q) {
+              const float dy = fsub(cy[q], geo.y);
+              pw[q] = ffma(fmul(cpo.x, dy), dy, ffma(bdx, dy, adx));
+              in_range = in_range || (pw[q] >= cpo.y && pw[q] <= 0.0f);
+            }
+            if (in_range) {
               const float4 col = s_col[j];
-              blend<kFull, kTrain>(s0, cy0, p0, cpo.y, cpo.z, chunk_pos + j, col);
-              blend<kFull, kTrain>(s1, cy1, p1, cpo.y, cpo.z, chunk_pos + j, col);
+#pragma unroll
+              for (int q = 0; q < kPix; ++q) {
+                blend<kFull, kTrain>(s[q], cy[q], pw[q], cpo.y, cpo.z, chunk_pos + j, col);
+              }
             }
           }
-          warp_done = __all_sync(0xffffffffu, s0.done && s1.done);
+          all_done = true;
+#pragma unroll
+          for (int q = 0; q < kPix; ++q) all_done = all_done && s[q].done;
+          warp_done = __all_sync(0xffffffffu, all_done);
         }
       }
-      if (__syncthreads_count(!(s0.done && s1.done)) == 0) break;
+      bool live = false;
+#pragma unroll
+      for (int q = 0; q < kPix; ++q) live = live || !s[q].done;
+      if (__syncthreads_count(live) == 0) break;
     }
   }
 
-  if (valid0) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y0, s0);
-  if (valid1) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y1, s1);
+#pragma unroll
+  for (int q = 0; q < kPix; ++q) {
+    if (valid[q]) write_pixel<kFull, kTrain>(p, plan, pixel_x, pixel_y0 + q * Geo::kLaneRows, s[q]);
+  }
 }
+
+// Resident CTAs per SM of each compositor shape: forward 16-pixel tiles in
+// the default shape keep three quarters of the SM's threads resident (a
+// 40-register cap: the loop is latency- and issue-bound, and the extra warps
+// measured 2.6 % faster than half occupancy at 64 registers); the
+// half-occupancy shape keeps half, and so do the other tile sizes.
+template <int kTile, bool kTrain, int kShape>
+struct CompositeOccupancy {
+  static constexpr int kThreads = CompositeGeometry<kTile, CompositeShape<kShape>::kPix>::kThreads;
+  static constexpr bool kThreeQuarters = kTile == 16 && !kTrain && kShape != kShapeHalfOccupancy;
+  static constexpr int kBlocks = kThreeQuarters ? 2048 / kThreads * 3 / 4 : 2048 / kThreads / 2;
+};
 
 // One CTA per work item, or (p.persistent) a resident grid whose CTAs take
 // work items from a device queue (ScratchHeader::composite_queue, zeroed by
 // the camera setup) until every (camera, tile) of the frame is done: no
 // CTA is launched for the grid's empty tail, and a CTA that finishes a cheap
 // tile immediately takes the next one.
-// Forward 16-pixel tiles keep three quarters of the SM's threads resident
-// (twelve 128-thread CTAs, a 40-register cap): the loop is latency- and
-// issue-bound, and the extra warps measured 2.6 % faster than half occupancy
-// at 64 registers.  Other shapes keep half occupancy.
-template <int kTile, bool kFull, bool kTrain, int kSplit>
-__global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
-                                  (kTile == 16 && !kTrain) ? 2048 / CompositeGeometry<kTile>::kThreads * 3 / 4
-                                                           : 2048 / CompositeGeometry<kTile>::kThreads / 2)
+template <int kTile, bool kFull, bool kTrain, int kSplit, int kShape>
+__global__ void __launch_bounds__(CompositeOccupancy<kTile, kTrain, kShape>::kThreads,
+                                  CompositeOccupancy<kTile, kTrain, kShape>::kBlocks)
     composite_kernel(CompositeParams p) {
+  constexpr int kPix = CompositeShape<kShape>::kPix;
   __shared__ float4 s_geo[kCompositeBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
   __shared__ float4 s_cpo[kCompositeBatch];  // -conic_yy/2, lo, opacity, -
   __shared__ float4 s_col[kCompositeBatch];  // r, g, b, depth
   __shared__ uint32_t s_mask[kCompositeBatch];
   __shared__ uint32_t s_item;
   if (!p.persistent) {
-    composite_item<kTile, kFull, kTrain, kSplit>(p, blockIdx.x, s_geo, s_cpo, s_col, s_mask);
+    composite_item<kTile, kFull, kTrain, kSplit, kPix>(p, blockIdx.x, s_geo, s_cpo, s_col, s_mask);
     return;
   }
   ScratchHeader* header = reinterpret_cast<ScratchHeader*>(p.scratch + p.layout.header);
@@ -220,7 +245,7 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads,
     __syncthreads();
     const int64_t item = s_item;
     if (item >= total) break;
-    composite_item<kTile, kFull, kTrain, kSplit>(p, item, s_geo, s_cpo, s_col, s_mask);
+    composite_item<kTile, kFull, kTrain, kSplit, kPix>(p, item, s_geo, s_cpo, s_col, s_mask);
     __syncthreads();  // shared staging and s_item are reused by the next item
   }
 }
@@ -427,16 +452,21 @@ template __global__ void composite_ray_kernel<16, true, 1>(CompositeParams);
 template __global__ void composite_ray_kernel<16, false, 2>(CompositeParams);
 template __global__ void composite_ray_kernel<16, true, 2>(CompositeParams);
 
-template __global__ void composite_kernel<4, false, false, 1>(CompositeParams);
-template __global__ void composite_kernel<4, true, false, 1>(CompositeParams);
-template __global__ void composite_kernel<8, false, false, 1>(CompositeParams);
-template __global__ void composite_kernel<8, true, false, 1>(CompositeParams);
-template __global__ void composite_kernel<16, false, false, 1>(CompositeParams);
-template __global__ void composite_kernel<16, true, false, 1>(CompositeParams);
-template __global__ void composite_kernel<16, false, false, 2>(CompositeParams);
-template __global__ void composite_kernel<16, true, false, 2>(CompositeParams);
-template __global__ void composite_kernel<4, true, true, 1>(CompositeParams);
-template __global__ void composite_kernel<8, true, true, 1>(CompositeParams);
-template __global__ void composite_kernel<16, true, true, 1>(CompositeParams);
+#define VGR_COMPOSITE_SHAPES(TILE, FULL, SPLIT)                                      \
+  template __global__ void composite_kernel<TILE, FULL, false, SPLIT, kShapeDefault>(CompositeParams); \
+  template __global__ void composite_kernel<TILE, FULL, false, SPLIT, kShapeOnePixel>(CompositeParams); \
+  template __global__ void composite_kernel<TILE, FULL, false, SPLIT, kShapeHalfOccupancy>(CompositeParams);
+template __global__ void composite_kernel<4, false, false, 1, kShapeDefault>(CompositeParams);
+template __global__ void composite_kernel<4, true, false, 1, kShapeDefault>(CompositeParams);
+VGR_COMPOSITE_SHAPES(8, false, 1)
+VGR_COMPOSITE_SHAPES(8, true, 1)
+VGR_COMPOSITE_SHAPES(16, false, 1)
+VGR_COMPOSITE_SHAPES(16, true, 1)
+VGR_COMPOSITE_SHAPES(16, false, 2)
+VGR_COMPOSITE_SHAPES(16, true, 2)
+#undef VGR_COMPOSITE_SHAPES
+template __global__ void composite_kernel<4, true, true, 1, kShapeDefault>(CompositeParams);
+template __global__ void composite_kernel<8, true, true, 1, kShapeDefault>(CompositeParams);
+template __global__ void composite_kernel<16, true, true, 1, kShapeDefault>(CompositeParams);
 
 }  // namespace vgr

@@ -200,14 +200,14 @@ namespace vgr {
 // over the device work queue.
 // kSplit > 1: each (kSplit * kTile)-pixel tile is composited as kSplit^2
 // kTile-pixel quadrants (one work item each).
-template <int kTile, bool kFull, bool kTrain, int kSplit = 1>
+template <int kTile, bool kFull, bool kTrain, int kSplit = 1, int kShape = kShapeDefault>
 void launch_composite(const CompositeParams& cp, int64_t max_items, int sms, cudaStream_t stream) {
-  const int threads = composite_threads(kTile);
+  const int threads = CompositeGeometry<kTile, CompositeShape<kShape>::kPix>::kThreads;
   max_items *= kSplit * kSplit;
   unsigned grid = static_cast<unsigned>(max_items);
   if (cp.persistent) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, composite_kernel<kTile, kFull, kTrain, kSplit>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, composite_kernel<kTile, kFull, kTrain, kSplit, kShape>,
                                                       threads, 0) != cudaSuccess ||
         per_sm < 1) {
       cudaGetLastError();
@@ -216,7 +216,24 @@ void launch_composite(const CompositeParams& cp, int64_t max_items, int sms, cud
     const int64_t resident = static_cast<int64_t>(sms) * per_sm;
     if (resident < max_items) grid = static_cast<unsigned>(resident);
   }
-  composite_kernel<kTile, kFull, kTrain, kSplit><<<grid, threads, 0, stream>>>(cp);
+  composite_kernel<kTile, kFull, kTrain, kSplit, kShape><<<grid, threads, 0, stream>>>(cp);
+}
+
+// Forward screen-space compositor of one tile size in the requested CTA
+// shape (vgr_render_options.composite_shape; 4-pixel tiles have one shape).
+template <int kTile, int kSplit = 1>
+void launch_forward_composite(const CompositeParams& cp, bool full, int shape, int64_t max_items, int sms,
+                              cudaStream_t stream) {
+  if (kTile == 4 || shape == kShapeDefault) {
+    if (full) launch_composite<kTile, true, false, kSplit>(cp, max_items, sms, stream);
+    else launch_composite<kTile, false, false, kSplit>(cp, max_items, sms, stream);
+  } else if (shape == kShapeOnePixel) {
+    if (full) launch_composite<kTile, true, false, kSplit, kShapeOnePixel>(cp, max_items, sms, stream);
+    else launch_composite<kTile, false, false, kSplit, kShapeOnePixel>(cp, max_items, sms, stream);
+  } else {
+    if (full) launch_composite<kTile, true, false, kSplit, kShapeHalfOccupancy>(cp, max_items, sms, stream);
+    else launch_composite<kTile, false, false, kSplit, kShapeHalfOccupancy>(cp, max_items, sms, stream);
+  }
 }
 
 int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_outputs* out,
@@ -256,6 +273,9 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
   if (!std::isfinite(opt->semantic_min_alpha) || opt->semantic_min_alpha < 0.0 ||
       opt->semantic_min_alpha > 1.0) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "semantic_min_alpha must be finite and in [0, 1]");
+  }
+  if (opt->composite_shape < kShapeDefault || opt->composite_shape > kShapeHalfOccupancy) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "composite_shape must be 0, 1 or 2");
   }
   const int ts = opt->tile_size;
   if (ts <= 0 || ts > 32 || (ts & (ts - 1)) != 0) {
@@ -662,17 +682,13 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
       else launch_composite<4, true, true>(cp, max_items, sms, stream);
     } else if (bin == 32) {
       if (max_items * 4 > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "raster grid exceeds CUDA limit");
-      if (full) launch_composite<16, true, false, 2>(cp, max_items, sms, stream);
-      else launch_composite<16, false, false, 2>(cp, max_items, sms, stream);
+      launch_forward_composite<16, 2>(cp, full, opt->composite_shape, max_items, sms, stream);
     } else if (bin == 16) {
-      if (full) launch_composite<16, true, false>(cp, max_items, sms, stream);
-      else launch_composite<16, false, false>(cp, max_items, sms, stream);
+      launch_forward_composite<16>(cp, full, opt->composite_shape, max_items, sms, stream);
     } else if (bin == 8) {
-      if (full) launch_composite<8, true, false>(cp, max_items, sms, stream);
-      else launch_composite<8, false, false>(cp, max_items, sms, stream);
+      launch_forward_composite<8>(cp, full, opt->composite_shape, max_items, sms, stream);
     } else {
-      if (full) launch_composite<4, true, false>(cp, max_items, sms, stream);
-      else launch_composite<4, false, false>(cp, max_items, sms, stream);
+      launch_forward_composite<4>(cp, full, opt->composite_shape, max_items, sms, stream);
     }
     if ((rc = check_launch("render: compositor")) != VGR_OK) return rc;
   }

@@ -172,16 +172,29 @@ struct CompositeParams {
   float support_sigma;
 };
 
-template <int kTile>
+template <int kTile, int kPix = 2>
 struct CompositeGeometry {
+  static_assert(kPix == 1 || kPix == 2, "one or two pixels per thread");
   static constexpr int kBlockW = kTile < 8 ? kTile : 8;  // warp block width (px)
   static constexpr int kLaneRows =
-      (32 / kBlockW) < (kTile / 2) ? (32 / kBlockW) : (kTile / 2);  // lane rows
-  static constexpr int kBlockH = 2 * kLaneRows;  // warp block height (px)
+      (32 / kBlockW) < (kTile / kPix) ? (32 / kBlockW) : (kTile / kPix);  // lane rows
+  static constexpr int kBlockH = kPix * kLaneRows;  // warp block height (px)
   static constexpr int kWarpsX = kTile / kBlockW;
   static constexpr int kWarpsY = kTile / kBlockH;
   static constexpr int kWarps = kWarpsX * kWarpsY;
   static constexpr int kThreads = kWarps * 32;
+};
+
+// Compositor CTA shapes (vgr_render_options.composite_shape): the default
+// two pixels per thread at the tuned occupancy; one pixel per thread (8x4
+// warp blocks, twice the threads, finer warp masks); two pixels per thread
+// at half occupancy (no register spills).
+constexpr int kShapeDefault = 0;
+constexpr int kShapeOnePixel = 1;
+constexpr int kShapeHalfOccupancy = 2;
+template <int kShape>
+struct CompositeShape {
+  static constexpr int kPix = kShape == kShapeOnePixel ? 1 : 2;
 };
 
 constexpr int kCompositeBatch = 256;
@@ -192,11 +205,11 @@ constexpr int kCompositeBatch = 256;
 // opacity, -), col = (r, g, b, depth), and the mask of the warp blocks the
 // record's conservative alpha footprint touches.  lo = max(-qmax/2, -20)
 // merges the footprint bound with the reference's power >= -20 cut.
-template <int kTile>
+template <int kTile, int kPix = 2>
 __device__ __forceinline__ void stage_composite_record(const Record& rec, float tile_x0,
                                                        float tile_y0, float4& geo, float4& cpo,
                                                        float4& col, uint32_t& mask_out) {
-  using Geo = CompositeGeometry<kTile>;
+  using Geo = CompositeGeometry<kTile, kPix>;
   geo = make_float4(rec.a.x, rec.a.y, fmul(-0.5f, rec.a.z), -rec.a.w);
   const float o = rec.b.y;
   const float qmax = fminf(40.0f, 2.0f * __logf(255.0f * o)) * 1.001f + 1.0e-3f;
@@ -323,7 +336,7 @@ __global__ void tile_scan_kernel(BucketParams p);
 __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void large_tile_list_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
-template <int kTile, bool kFull, bool kTrain, int kSplit>
+template <int kTile, bool kFull, bool kTrain, int kSplit, int kShape>
 __global__ void composite_kernel(CompositeParams p);
 template <int kTile, bool kFull, int kSplit>
 __global__ void composite_ray_kernel(CompositeParams p);

@@ -125,6 +125,7 @@ class VgrRenderOptions(ctypes.Structure):
         ("stage_events", ctypes.POINTER(_c_p)),
         ("stage_event_count", _c_i32),
         ("persistent_compositor", _c_i32),
+        ("composite_shape", _c_i32),
     ]
 
 

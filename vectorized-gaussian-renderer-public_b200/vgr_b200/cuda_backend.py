@@ -125,6 +125,7 @@ class CustomCudaBackend:
         mirror_reference_workspace: bool = False,
         spatial_layout: bool = True,
         persistent_compositor: bool = False,
+        composite_shape: int = 0,
     ) -> None:
         if max_visible_records is not None and max_visible_records <= 0:
             raise ValueError("max_visible_records must be positive.")
@@ -231,6 +232,10 @@ class CustomCudaBackend:
         # Compositor as a resident grid over a device work queue (see
         # vgr_render_options.persistent_compositor).
         self.persistent_compositor = persistent_compositor
+        # Compositor CTA shape (see vgr_render_options.composite_shape).
+        if composite_shape not in (0, 1, 2):
+            raise ValueError("composite_shape must be 0, 1 or 2.")
+        self.composite_shape = composite_shape
         self._native = native_module
         self._native_loader = native_loader
         self.allow_cpu_for_tests = allow_cpu_for_tests
@@ -673,6 +678,7 @@ class CustomCudaBackend:
             sh_degree=-1 if self.sh_degree is None else self.sh_degree,
             sorted_buffer_hint=1,
             persistent_compositor=int(self.persistent_compositor),
+            composite_shape=int(self.composite_shape),
         )
         if self._stage_event_handles is not None:
             options.stage_events = self._stage_event_handles

@@ -49,6 +49,7 @@ class RaggedBatch:
         full_sensor_output: bool = True,
         headroom: float = 1.25,
         persistent_compositor: bool = False,
+        composite_shape: int = 0,
     ) -> None:
         if backend.device is None or not backend._packed_scene:
             raise RuntimeError("RaggedBatch needs an initialized backend with registered scenes.")
@@ -69,6 +70,10 @@ class RaggedBatch:
         # on the 1,024-camera frame both take 11.0 ms (the empty slots exit at
         # once and the hardware scheduler balances the rest).
         self.persistent_compositor = bool(persistent_compositor)
+        # Compositor CTA shape (vgr_render_options.composite_shape): 0 two
+        # pixels per thread, 1 one pixel per thread, 2 two pixels per thread
+        # at half occupancy; every shape renders the same bits.
+        self.composite_shape = int(composite_shape)
         self.tile_size = int(tile_size or backend.tile_size)
         self._visible_capacity = 0
         self._intersection_capacity = 0
@@ -241,6 +246,7 @@ class RaggedBatch:
             sh_degree=-1 if b.sh_degree is None else b.sh_degree,
             sorted_buffer_hint=1,
             persistent_compositor=int(self.persistent_compositor),
+            composite_shape=self.composite_shape,
         )
         if self._stage_events is not None:
             options.stage_events = self._stage_events
@@ -336,51 +342,66 @@ def autotune_tile_size(
     *,
     candidates: Sequence[int] = (8, 16, 32),
     persistent_candidates: Sequence[bool] = (False,),
+    shape_candidates: Sequence[int] = (0,),
     repeats: int = 3,
     cache: dict[Any, Any] | None = None,
 ) -> int:
-    """Pick the fastest tile size (and, with ``persistent_candidates``, the
-    compositor launch: one CTA per tile or the resident work-queue grid) for
-    this rig's shape class: time each candidate on the device after
-    calibrating its workspace and leave ``ragged`` set to the winner.
-    ``cache`` maps shape classes (resolution multiset, scene sizes) to
-    earlier choices.  Returns the tile size."""
+    """Pick the fastest tile size and compositor launch for this rig's shape
+    class: tile size x (with ``persistent_candidates``) one CTA per tile or
+    the resident work-queue grid x (with ``shape_candidates``) the
+    compositor's CTA shape (composite_shape: pixels per thread and
+    occupancy; 4-pixel tiles have one shape, and on 8-pixel tiles shapes 0
+    and 2 coincide).  Each candidate is timed on the device after
+    calibrating its workspace; ``ragged`` is left set to the winner.
+    ``cache`` maps shape classes (resolution multiset, camera count, scene
+    sizes) to earlier choices.  Returns the tile size; the launch choices are
+    on ``ragged`` (``persistent_compositor``, ``composite_shape``) and every
+    timing in ``ragged.autotune_ms``."""
     key = (
         tuple(sorted(set(zip(ragged.heights, ragged.widths)))),
         ragged.batch,
         tuple(s.count for s in ragged.backend._scenes.values()),
         tuple(candidates),
         tuple(persistent_candidates),
+        tuple(shape_candidates),
     )
-    if cache is not None and key in cache:
-        tile, persistent = cache[key]
+
+    def apply(choice) -> None:
+        tile, persistent, shape = choice
         ragged.persistent_compositor = persistent
+        ragged.composite_shape = shape
         ragged._set_tiles(tile)
         ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
-        return tile
+
+    if cache is not None and key in cache:
+        apply(cache[key])
+        return cache[key][0]
     best, best_ms = None, float("inf")
     stream = torch.cuda.current_stream(ragged.device)
     for persistent in persistent_candidates:
         for tile in candidates:
-            ragged.persistent_compositor = persistent
-            ragged._set_tiles(tile)
-            ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
-            start = torch.cuda.Event(enable_timing=True)
-            stop = torch.cuda.Event(enable_timing=True)
-            start.record(stream)
-            for _ in range(repeats):
-                ragged.render(viewmats, intrinsics, scene_ids, outputs)
-            stop.record(stream)
-            stop.synchronize()
-            ms = start.elapsed_time(stop) / repeats
-            ragged.autotune_ms[f"{tile}{'p' if persistent else ''}" if len(persistent_candidates) > 1 else tile] = ms
-            if ms < best_ms:
-                best, best_ms = (tile, persistent), ms
+            for shape in shape_candidates:
+                if (tile == 4 and shape != 0) or (tile == 8 and shape == 2):
+                    continue  # the same kernel as shape 0
+                apply((tile, persistent, shape))
+                start = torch.cuda.Event(enable_timing=True)
+                stop = torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                for _ in range(repeats):
+                    ragged.render(viewmats, intrinsics, scene_ids, outputs)
+                stop.record(stream)
+                stop.synchronize()
+                ms = start.elapsed_time(stop) / repeats
+                label = str(tile)
+                if len(persistent_candidates) > 1 and persistent:
+                    label += "p"
+                if len(shape_candidates) > 1:
+                    label += f"s{shape}"
+                ragged.autotune_ms[label if label != str(tile) else tile] = ms
+                if ms < best_ms:
+                    best, best_ms = (tile, persistent, shape), ms
     assert best is not None
-    ragged.persistent_compositor = best[1]
-    ragged._set_tiles(best[0])
-    ragged.calibrate(viewmats, intrinsics, scene_ids, outputs)
+    apply(best)
     if cache is not None:
         cache[key] = best
     return best[0]
-
