@@ -364,6 +364,7 @@ def roofline_of(stage_avg: dict[str, float], stage_bytes: dict[str, float], work
         "frac": round(achieved / peak, 4),
         "peak_source": f"hbm_gbs of {peak_kind}",
         "traffic": traffic.get(kernel),
+        "traffic_source": traffic.get("_source"),
         "algorithmic_bytes": int(stage_bytes[dominant]),
         "ms": round(stage_avg[dominant], 4),
         "issue_active_ncu": traffic.get("_issue_active", {}).get(kernel),
