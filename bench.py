@@ -85,6 +85,8 @@ def parse_args() -> argparse.Namespace:
                         help="frames of the ragged workload on the linear-RGB equation (0: skip)")
     parser.add_argument("--tile", type=int, default=None,
                         help="fix the ragged tile size instead of autotuning (profiling captures)")
+    parser.add_argument("--composite-shape", type=int, default=None, choices=(0, 1, 2),
+                        help="compositor CTA shape with --tile, and for the batched workload")
     parser.add_argument("--batched-steps", type=int, default=10,
                         help="frames of the batched 1M-Gaussian 64-camera workload (0: skip)")
     parser.add_argument("--cameras", type=int, default=None,
@@ -433,6 +435,8 @@ def run_ragged(args, device, world: int, rank: int, work) -> dict:
     outputs = ragged.outputs()
     view = r_poses[0].clone()
     if args.tile:
+        if args.composite_shape is not None:
+            ragged.composite_shape = args.composite_shape
         ragged._set_tiles(args.tile)
         tile = args.tile
     else:
@@ -676,7 +680,8 @@ def run_batched(args, device) -> dict:
     scene, rig = batched_workload(cameras=count)
 
     def frame_ms(sh_degree, with_stages: bool):
-        backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=16)
+        backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=16,
+                                    composite_shape=args.composite_shape or 0)
         service = RendererService(backend, height=rig.height, width=rig.width, max_views=count)
         service.initialize(stage=None, device=device)
         kw = scene.to(device).as_kwargs()

@@ -533,6 +533,8 @@ template <int kShDegree, bool kRay, int kMode>
 __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(ProjectParams p) {
   __shared__ Record s_rec[kProjectChunk];          // by task slot
   __shared__ uint16_t s_slot[kProjectChunk];       // rank -> task slot
+  // By task slot, like s_rec (held in shared memory rather than registers
+  // across the two projection rounds).
   __shared__ uint32_t s_rect_min[kProjectChunk];   // min_tx | min_ty << 16
   __shared__ uint32_t s_rect_size[kProjectChunk];  // ntx | nty << 16
   __shared__ uint32_t s_prefix[kProjectChunk + 1]; // exclusive isect prefix
@@ -613,7 +615,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       }
     }
     const int64_t b = s_vbs[cursor];
-    const CamPlan plan = s_plans[cursor];
+    const CamPlan& plan = s_plans[cursor];
     const CamConst& s_cam = s_cams[cursor];
     ++cursor;
     const int64_t chunk = b / p.active_count;
@@ -623,8 +625,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
     // Project both rounds first (no barrier), then one block scan of
     // (visible, tiles) over the kProjectChunk tasks in task order.
     bool vis[kProjectRounds];
-    uint32_t ntiles[kProjectRounds], rect_min[kProjectRounds], rect_size[kProjectRounds];
-    int32_t radius_x[kProjectRounds], radius_y[kProjectRounds];
+    uint32_t ntiles[kProjectRounds];
     float ray_terms[kRay ? kProjectRounds : 1][10];
     uint32_t ray_rank[kRay ? kProjectRounds : 1];
     const float its = 1.0f / static_cast<float>(p.tile_size);
@@ -633,10 +634,6 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       const int64_t local = local_begin + round * kProjectThreads + tid;
       vis[round] = false;
       ntiles[round] = 0;
-      rect_min[round] = 0;
-      rect_size[round] = 0;
-      radius_x[round] = 0;
-      radius_y[round] = 0;
       Projected pr;
       if (live && local < plan.g_count) {
         const int64_t g = plan.g_begin + local;
@@ -706,11 +703,12 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           const int min_ty = max(0, floor_clamped(fsub(fmul(pr.mean_y, its), fmul(fry, its))));
           const int ntx = max(0, min(plan.tiles_x, ceil_clamped(fadd(fmul(pr.mean_x, its), fmul(frx, its)))) - min_tx);
           const int nty = max(0, min(plan.tiles_y, ceil_clamped(fadd(fmul(pr.mean_y, its), fmul(fry, its)))) - min_ty);
-          rect_min[round] = static_cast<uint32_t>(min(min_tx, 65535)) |
-                            (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
-          rect_size[round] = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
-          radius_x[round] = pr.radius_x;
-          radius_y[round] = pr.radius_y;
+          const int slot = round * kProjectThreads + tid;
+          s_rect_min[slot] = static_cast<uint32_t>(min(min_tx, 65535)) |
+                             (static_cast<uint32_t>(min(min_ty, 65535)) << 16);
+          s_rect_size[slot] = static_cast<uint32_t>(ntx) | (static_cast<uint32_t>(nty) << 16);
+          s_radii[slot * 2 + 0] = pr.radius_x;
+          s_radii[slot * 2 + 1] = pr.radius_y;
           if (kRay) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) ray_terms[kRay ? round : 0][k] = pr.prec[k];
@@ -718,17 +716,10 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
             for (int k = 0; k < 3; ++k) ray_terms[kRay ? round : 0][6 + k] = pr.prec_mean[k];
             ray_terms[kRay ? round : 0][9] = pr.mean_prec_mean;
           }
-          float rgb[3];
-          if (kShDegree < 0) {
-            rgb[0] = p.features[g * p.feature_width + 0];
-            rgb[1] = p.features[g * p.feature_width + 1];
-            rgb[2] = p.features[g * p.feature_width + 2];
-          } else {
-            eval_sh<kShDegree < 0 ? 0 : kShDegree>(p.features + g * p.feature_width,
-                                                   p.vector_feature_loads, s_cam, pr.px, pr.py,
-                                                   pr.pz, rgb);
-          }
-          // Staged by task slot; the scan below maps ranks to slots.
+          // Staged by task slot; the scan below maps ranks to slots.  The
+          // colour is evaluated after the scan, over the compacted visible
+          // records (full warps), from the camera-space position kept in
+          // c.x / c.y (c.z unused until then; z is the depth b.z).
           Record& staged = s_rec[round * kProjectThreads + tid];
           staged.a = make_float4(pr.mean_x, pr.mean_y, pr.conic0, pr.conic1);
           const int32_t id = p.gaussian_ids ? p.gaussian_ids[g] : static_cast<int32_t>(g);
@@ -740,7 +731,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
               kRay ? static_cast<uint32_t>(min(pr.radius_x, 32766) + 1) |
                          (static_cast<uint32_t>(min(pr.radius_y, 32766) + 1) << 16)
                    : footprint_box(pr.opacity, pr.cov_a, pr.cov_b, pr.cov_c);
-          staged.c = make_float4(rgb[0], rgb[1], rgb[2], __uint_as_float(box));
+          staged.c = make_float4(pr.px, pr.py, 0.0f, __uint_as_float(box));
         }
       }
     }
@@ -786,11 +777,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         const uint32_t rank = block_vis + wv + v_incl[round] - 1;
         const uint64_t excl = block_isect + wt + t_incl[round] - ntiles[round];
         s_slot[rank] = static_cast<uint16_t>(round * kProjectThreads + tid);
-        s_rect_min[rank] = rect_min[round];
-        s_rect_size[rank] = rect_size[round];
         s_prefix[rank] = static_cast<uint32_t>(excl > 0x7fffffffull ? 0x7fffffffull : excl);
-        s_radii[rank * 2 + 0] = radius_x[round];
-        s_radii[rank * 2 + 1] = radius_y[round];
         if (kRay) ray_rank[kRay ? round : 0] = rank;
         // Owner of each of the record's keys, for blocks whose keys fit
         // (the emission below falls back to a search of s_prefix otherwise).
@@ -825,13 +812,28 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       const uint64_t base_isect = s_base_isect;
       const uint64_t vcap = static_cast<uint64_t>(p.visible_capacity);
       const uint64_t icap = static_cast<uint64_t>(p.intersection_capacity);
-      // Records: coalesced float4 stream of the compacted block.
+      // Records in rank order, one thread per record: the colour (SH or
+      // linear RGB) of the record's Gaussian, then the three float4s.
       float4* dst = reinterpret_cast<float4*>(p.records);
-      const float4* src = reinterpret_cast<const float4*>(s_rec);
-      for (uint32_t i = tid; i < nvis * 3; i += kProjectThreads) {
-        const uint32_t rank = i / 3;
-        const uint64_t r = base_vis + rank;
-        if (r < vcap) dst[r * 3 + (i - rank * 3)] = src[s_slot[rank] * 3 + (i - rank * 3)];
+      for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
+        const uint32_t slot = s_slot[i];
+        const Record& st = s_rec[slot];
+        const int64_t g = plan.g_begin + local_begin + slot;
+        float rgb[3];
+        if (kShDegree < 0) {
+          rgb[0] = p.features[g * p.feature_width + 0];
+          rgb[1] = p.features[g * p.feature_width + 1];
+          rgb[2] = p.features[g * p.feature_width + 2];
+        } else {
+          eval_sh<kShDegree < 0 ? 0 : kShDegree>(p.features + g * p.feature_width, p.vector_feature_loads,
+                                                 s_cam, st.c.x, st.c.y, st.b.z, rgb);
+        }
+        const uint64_t r = base_vis + i;
+        if (r < vcap) {
+          dst[r * 3 + 0] = st.a;
+          dst[r * 3 + 1] = st.b;
+          dst[r * 3 + 2] = make_float4(rgb[0], rgb[1], rgb[2], st.c.w);
+        }
       }
       if (kRay) {
         // Extension records: each thread writes its own visible Gaussians'.
@@ -877,8 +879,8 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           p.mirror_opacities[r] = rec.b.y;
           p.mirror_camera_ids[r] = plan.camera;
           p.mirror_gaussian_ids[r] = __float_as_int(rec.b.w);
-          p.mirror_radii[r * 2 + 0] = s_radii[i * 2 + 0];
-          p.mirror_radii[r * 2 + 1] = s_radii[i * 2 + 1];
+          p.mirror_radii[r * 2 + 0] = s_radii[s_slot[i] * 2 + 0];
+          p.mirror_radii[r * 2 + 1] = s_radii[s_slot[i] * 2 + 1];
         }
       }
       // Tile intersections: one key per covered tile, cooperative over the
@@ -895,12 +897,13 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         // record (the kept tiles are not a dense range of the rect).
         for (uint32_t i = tid; i < nvis; i += kProjectThreads) {
           const uint64_t r = base_vis + i;
-          const float depth = s_rec[s_slot[i]].b.z;
+          const uint32_t slot = s_slot[i];
+          const float depth = s_rec[slot].b.z;
           const int bucket = dense_bucket(depth, p.near_bits);
-          const uint32_t ntx = s_rect_size[i] & 0xffffu;
-          const uint32_t nty = s_rect_size[i] >> 16;
-          const uint32_t min_tx = s_rect_min[i] & 0xffffu;
-          const uint32_t min_ty = s_rect_min[i] >> 16;
+          const uint32_t ntx = s_rect_size[slot] & 0xffffu;
+          const uint32_t nty = s_rect_size[slot] >> 16;
+          const uint32_t min_tx = s_rect_min[slot] & 0xffffu;
+          const uint32_t min_ty = s_rect_min[slot] >> 16;
           uint32_t j = s_prefix[i];
           for (uint32_t ty = min_ty; ty < min_ty + nty; ++ty) {
             for (uint32_t tx = min_tx; tx < min_tx + ntx; ++tx) {
@@ -937,18 +940,19 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           i = lo;
         }
         const uint32_t local = j - s_prefix[i];
-        const uint32_t ntx = s_rect_size[i] & 0xffffu;
+        const uint32_t slot = s_slot[i];
+        const uint32_t ntx = s_rect_size[slot] & 0xffffu;
         const uint32_t ty = ntx == 1u ? local : local / ntx;  // most records span one tile column
         const uint32_t tx = local - ty * ntx;
-        const uint32_t min_tx = s_rect_min[i] & 0xffffu;
-        const uint32_t min_ty = s_rect_min[i] >> 16;
+        const uint32_t min_tx = s_rect_min[slot] & 0xffffu;
+        const uint32_t min_ty = s_rect_min[slot] >> 16;
         const uint64_t r = base_vis + i;
         uint64_t key = ~0ull;
         int32_t value = 0;
         if (r < vcap) {
           const uint64_t tile = static_cast<uint64_t>(plan.tile_base) +
                                 static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
-          key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[s_slot[i]].b.z));
+          key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[slot].b.z));
           value = static_cast<int32_t>(r);
           // Bucket size for the tile sort (a tile past the batch's range - a
           // caller's inconsistent ragged offsets - is left to the scatter's
