@@ -164,27 +164,6 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
 
   const float* s = covariances + g * 6;
   const float s00 = s[0], s01 = s[1], s02 = s[2], s11 = s[3], s12 = s[4], s22 = s[5];
-  if (!kRay) {
-    // Early off-screen cull, conservative so that it never drops a record
-    // the full test below keeps.  The x-row of the Jacobian has squared norm
-    // (fx/z)^2 (1 + clamp(x/z)^2) <= (fx/z)^2 (1 + L^2), the camera-space
-    // covariance R S R^T has largest eigenvalue at most trace(S) times the
-    // bound of R^T R's largest eigenvalue (r_scale2), and the extent
-    // factor is at most support_sigma, so the pixel radius is below
-    // R = support_sigma * sqrt((fx/z)^2 (1 + L^2) trace + eps) (+ margins
-    // for rounding and the ceiling).  Rounding is monotone, so
-    // u + R <= 0 implies u + radius <= 0 as computed below, and likewise
-    // for the other three sides.
-    const float trace = (s00 + s11 + s22) * c.r_scale2;
-    const float lx = fmaxf(c.lim_xp, c.lim_xn), ly = fmaxf(c.lim_yp, c.lim_yn);
-    const float gx = c.fx * iz, gy = c.fy * iz;
-    const float bx = support_sigma * sqrtf(gx * gx * (1.0f + lx * lx) * trace + cov_eps) * 1.01f + 2.0f;
-    const float by = support_sigma * sqrtf(gy * gy * (1.0f + ly * ly) * trace + cov_eps) * 1.01f + 2.0f;
-    if (fadd(u, bx) <= 0.0f || fadd(v, by) <= 0.0f || fsub(u, bx) >= c.width ||
-        fsub(v, by) >= c.height) {
-      return false;
-    }
-  }
   float tm[9];
 #pragma unroll
   for (int row = 0; row < 3; ++row) {
@@ -333,16 +312,18 @@ __device__ __forceinline__ bool project_gaussian(const float* __restrict__ means
 // Real spherical harmonics through degree 3 (the basis and constants of the
 // 3D Gaussian Splatting reference implementation, as used by gsplat), view
 // direction from the camera centre to the mean in object space, +0.5 offset,
-// clamped at zero.  coeffs is [(d+1)^2, 3], coefficient-major.  With
-// vector_loads the row is fetched as float4s (rows 16-byte aligned and padded
-// to a multiple of four floats), otherwise as scalars.
+// clamped at zero.  coeffs is [(d+1)^2, 3], coefficient-major.  The row is
+// fetched in 256-bit loads with wide_loads (rows 32-byte aligned and padded
+// to a multiple of eight floats), else as float4s with vector_loads (16 bytes
+// and four floats), otherwise as scalars; the sums are the same.
 template <int kDegree>
-__device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vector_loads,
+__device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool wide_loads, bool vector_loads,
                                         const CamConst& c, float px, float py, float pz,
                                         float* rgb) {
   constexpr int kCount = (kDegree + 1) * (kDegree + 1);
   constexpr int kFloats = kCount * 3;
   constexpr int kVectors = (kFloats + 3) / 4;
+  constexpr int kOctets = (kFloats + 7) / 8;
   float dx = ffma(c.r[6], pz, ffma(c.r[3], py, fmul(c.r[0], px)));
   float dy = ffma(c.r[7], pz, ffma(c.r[4], py, fmul(c.r[1], px)));
   float dz = ffma(c.r[8], pz, ffma(c.r[5], py, fmul(c.r[2], px)));
@@ -384,7 +365,15 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ row, bool vect
     if (k >= kCount) return;
     acc[ch] = k == 0 ? fmul(basis[0], v) : ffma(basis[k], v, acc[ch]);
   };
-  if (vector_loads) {
+  if (wide_loads) {
+#pragma unroll
+    for (int i = 0; i < kOctets; ++i) {
+      float v[8];
+      ldg8(row + 8 * i, v);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) take(8 * i + k, v[k]);
+    }
+  } else if (vector_loads) {
     const float4* row4 = reinterpret_cast<const float4*>(row);
 #pragma unroll
     for (int i = 0; i < kVectors; ++i) {
@@ -420,12 +409,17 @@ __device__ __forceinline__ uint32_t footprint_box(float opacity, float a, float 
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// True when no Gaussian of a chunk can pass the early off-screen cull of
+// True when no Gaussian of a chunk can pass the screen cull of
 // project_gaussian for this camera, so the chunk need not be projected.
-// With p = R m + t (camera space), the early cull rejects a Gaussian when
-// pz is outside [near, far] or u + bx <= 0 (and likewise for the other three
-// image sides), bx = 1.01 sigma sqrt((fx/pz)^2 (1 + L^2) tr + eps) + 2 with
-// tr <= T (the chunk's largest trace times r_scale2).  Since
+// With p = R m + t (camera space), u = fx px / pz + cx: the x-row of the
+// Jacobian has squared norm (fx/pz)^2 (1 + clamp(px/pz)^2) <= (fx/pz)^2
+// (1 + L^2), the camera-space covariance R S R^T has largest eigenvalue at
+// most trace(S) times the bound of R^T R's largest eigenvalue (r_scale2),
+// and the extent factor is at most sigma, so the pixel radius is below
+// bx = 1.01 sigma sqrt((fx/pz)^2 (1 + L^2) tr + eps) + 2 (margins for
+// rounding and the ceiling) with tr <= T (the chunk's largest trace times
+// r_scale2).  A Gaussian is therefore culled when pz is outside [near, far]
+// or u + bx <= 0 (and likewise for the other three image sides).  Since
 // sqrt(a + b) <= sqrt(a) + sqrt(b), pz bx / fx <= K + pz m with
 // K = 1.01 sigma sqrt((1 + L^2) T) and m = (1.01 sigma sqrt(eps) + 2) / fx,
 // and u + bx = (fx / pz)(px + pz cx / fx + pz bx / fx), a Gaussian with
@@ -825,8 +819,8 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
           rgb[1] = p.features[g * p.feature_width + 1];
           rgb[2] = p.features[g * p.feature_width + 2];
         } else {
-          eval_sh<kShDegree < 0 ? 0 : kShDegree>(p.features + g * p.feature_width, p.vector_feature_loads,
-                                                 s_cam, st.c.x, st.c.y, st.b.z, rgb);
+          eval_sh<kShDegree < 0 ? 0 : kShDegree>(p.features + g * p.feature_width, p.wide_feature_loads,
+                                                 p.vector_feature_loads, s_cam, st.c.x, st.c.y, st.b.z, rgb);
         }
         const uint64_t r = base_vis + i;
         if (r < vcap) {

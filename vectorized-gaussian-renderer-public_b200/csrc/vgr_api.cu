@@ -473,6 +473,8 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     pp.feature_width = scene->feature_width;
     pp.vector_feature_loads = (reinterpret_cast<uintptr_t>(scene->features) & 15) == 0 &&
                               (scene->feature_width & 3) == 0;
+    pp.wide_feature_loads = (reinterpret_cast<uintptr_t>(scene->features) & 31) == 0 &&
+                            (scene->feature_width & 7) == 0;
     pp.viewmats = cams->viewmats;
     pp.intrinsics = cams->intrinsics;
     pp.env_xforms = cams->env_xforms;

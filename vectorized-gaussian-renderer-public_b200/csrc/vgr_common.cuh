@@ -61,6 +61,13 @@ __device__ __forceinline__ float vexp(float x) {
   return fmul(p, __int_as_float((e + 127) << 23));
 }
 
+// One 256-bit read-only load of eight floats (p 32-byte aligned).
+__device__ __forceinline__ void ldg8(const float* p, float (&v)[8]) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+      : "l"(p));
+}
+
 // ln(y) for positive normal finite y: y = m 2^e with m in [sqrt(1/2), sqrt(2)),
 // ln m = 2 atanh(s), s = (m-1)/(m+1), atanh by its odd series through s^11
 // (|s| <= 0.1716, truncation < 1e-10 relative), ln 2 split in two parts.

@@ -40,6 +40,7 @@ struct ProjectParams {
   const float* features;
   int64_t feature_width;
   bool vector_feature_loads;  // rows 16-byte aligned and a multiple of 4 floats
+  bool wide_feature_loads;    // rows 32-byte aligned and a multiple of 8 floats
   const float* viewmats;
   const float* intrinsics;
   const float* env_xforms;
