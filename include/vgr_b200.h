@@ -68,13 +68,21 @@ typedef struct vgr_scene {
    * per chunk of VGR_PROJECT_CHUNK consecutive Gaussians of a registered
    * scene, (min x, min y, min z, max covariance trace, max x, max y, max z,
    * 0) from vgr_scene_chunk_bounds; chunk_offsets[s] is scene s's first
-   * chunk.  A chunk outside a camera's frustum is then not projected. */
+   * chunk.  A chunk outside a camera's frustum is then not projected.
+   * cluster_bounds (with chunk_bounds): the same bounds per cluster of
+   * VGR_PROJECT_CLUSTER consecutive Gaussians, VGR_PROJECT_CHUNK /
+   * VGR_PROJECT_CLUSTER clusters per chunk (cluster k of chunk c at row
+   * c * 16 + k), from vgr_scene_cluster_bounds; a cluster outside a camera's
+   * frustum inside a chunk that is not is then skipped as well. */
   const int32_t* gaussian_ids;         /* [G] or NULL */
   const float* chunk_bounds;           /* [C,8] or NULL */
   const int64_t* chunk_offsets;        /* [S+1], required with chunk_bounds */
+  const float* cluster_bounds;         /* [C*16,8] or NULL */
 } vgr_scene;
 /* Gaussians per projection chunk (the unit of vgr_scene.chunk_bounds). */
 #define VGR_PROJECT_CHUNK 512
+/* Gaussians per projection cluster (the unit of vgr_scene.cluster_bounds). */
+#define VGR_PROJECT_CLUSTER 32
 
 /* Camera batch.  The plain form leaves the four per-camera resolution arrays
  * NULL and renders every camera at (height,width) of vgr_render_options.
@@ -304,6 +312,11 @@ int vgr_scene_spatial_order(const float* means, int64_t gaussian_count, int32_t*
  * max x, max y, max z, 0), ceil(gaussian_count / VGR_PROJECT_CHUNK) chunks. */
 int vgr_scene_chunk_bounds(const float* means, const float* covariances,
                            int64_t gaussian_count, float* bounds, void* stream);
+/* The same bounds per cluster of VGR_PROJECT_CLUSTER consecutive Gaussians
+ * of one scene: ceil(gaussian_count / VGR_PROJECT_CHUNK) * 16 rows of 8
+ * floats (clusters past the end of the scene hold an empty box). */
+int vgr_scene_cluster_bounds(const float* means, const float* covariances,
+                             int64_t gaussian_count, float* bounds, void* stream);
 /* ---------------------------------------------------------------- ingestion */
 /* Scalar types of PLY properties (PLY names: char uchar short ushort int uint
  * float double, and int64 for a semantic_id written by 64-bit tools). */

@@ -256,6 +256,29 @@ def test_large_tile_grid_bitwise():
     assert_bitwise_equal(_sorted_gids(gpu), cpu.sorted_gaussian_ids, "sorted gaussian ids")
 
 
+def _check_cluster_bounds(packed) -> None:
+    # Each cluster row bounds its 32 Gaussians' means and holds their largest
+    # covariance trace; clusters past a scene's end hold an empty box.
+    means = packed["means"].cpu().numpy()
+    cov = packed["covariances"].cpu().numpy()
+    offsets = packed["scene_offsets"].cpu().tolist()
+    chunk_offsets = packed["chunk_offsets"].cpu().tolist()
+    rows = packed["cluster_bounds"].cpu().numpy()
+    for s in range(len(offsets) - 1):
+        count = offsets[s + 1] - offsets[s]
+        for k in range(-(-count // 512) * 16):
+            row = rows[chunk_offsets[s] * 16 + k]
+            g0, g1 = offsets[s] + 32 * k, min(offsets[s] + 32 * k + 32, offsets[s + 1])
+            if g0 >= offsets[s + 1]:
+                assert np.all(row[:3] == np.inf) and np.all(row[4:7] == -np.inf), (s, k, row)
+                continue
+            m = means[g0:g1]
+            np.testing.assert_array_equal(row[:3], m.min(axis=0))
+            np.testing.assert_array_equal(row[4:7], m.max(axis=0))
+            trace = cov[g0:g1, 0] + cov[g0:g1, 3] + cov[g0:g1, 5]
+            assert row[3] == trace.astype(np.float32).max(), (s, k)
+
+
 def test_spatial_layout_renders_identically():
     # Scenes stored in Morton order with per-chunk frustum culling render
     # exactly what the scene in id order renders: cameras inside a large
@@ -270,7 +293,9 @@ def test_spatial_layout_renders_identically():
     ids = [4, 4, 6, 4]
     with_layout = render_gpu(scenes, rig, ids, sh_degree=1, spatial_layout=True)
     without = render_gpu(scenes, rig, ids, sh_degree=1, spatial_layout=False)
-    assert "chunk_bounds" in with_layout.backend._packed_scene
+    packed = with_layout.backend._packed_scene
+    assert "chunk_bounds" in packed and "cluster_bounds" in packed
+    _check_cluster_bounds(packed)
     for name in ("rgb", "depth", "alpha", "semantic_id"):
         assert torch.equal(with_layout.outputs[name], without.outputs[name]), name
     assert with_layout.counters == without.counters

@@ -512,14 +512,22 @@ __device__ __forceinline__ void sort_tile(const BucketParams& p, int64_t tile, T
   auto place = [&](int i, int lo, int hi, int64_t out_base) {
     const uint64_t v = s_items[i];
     const uint32_t d = static_cast<uint32_t>(v >> 32);
-    int rank = 0;
-    bool tie = false;
-    for (int f = lo; f < hi; ++f) {
-      const uint32_t df = static_cast<uint32_t>(s_items[f] >> 32);
-      rank += df < d ? 1 : 0;
-      tie |= df == d && f != i;
+    // Entries of the split below d, and equal to d (the entry itself
+    // included): the depth words alone, four per iteration.
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(s_items) + 1;
+    int rank = 0, equal = 0;
+    int f = lo;
+    for (; f + 4 <= hi; f += 4) {
+      const uint32_t d0 = words[2 * f], d1 = words[2 * f + 2], d2 = words[2 * f + 4], d3 = words[2 * f + 6];
+      rank += (d0 < d) + (d1 < d) + (d2 < d) + (d3 < d);
+      equal += (d0 == d) + (d1 == d) + (d2 == d) + (d3 == d);
     }
-    if (tie) {
+    for (; f < hi; ++f) {
+      const uint32_t df = words[2 * f];
+      rank += df < d;
+      equal += df == d;
+    }
+    if (equal > 1) {
       const uint32_t g = gaussian_id(v);
       for (int f = lo; f < hi; ++f) {
         const uint64_t w = s_items[f];
@@ -895,10 +903,11 @@ __global__ void __launch_bounds__(256) large_tile_list_kernel(BucketParams p) {
 // cameras inside dense scenes keeps most of its intersections in a few long
 // buckets of neighbouring tiles; with one CTA per tile in tile order they
 // ran as a tail at the end of the grid.
-// Five resident CTAs per SM (as many as the shared-memory footprint allows):
-// the sort is barrier- and latency-bound, and the fifth CTA measured 10 %
-// faster than four despite the tighter register cap.
-__global__ void __launch_bounds__(kTileSortThreads, 5) tile_sort_kernel(BucketParams p) {
+// Four resident CTAs per SM: a 64-register cap (five CTAs, the most the
+// shared-memory footprint allows, cap registers at 48 and spilled about
+// 2 KB per thread to local memory; four measured 5.26 -> 4.56 ms on the
+// 1,024-camera ragged frame, three 5.11 ms).
+__global__ void __launch_bounds__(kTileSortThreads, 4) tile_sort_kernel(BucketParams p) {
   __shared__ TileSortSmem sm;
   const int64_t workers = p.large_workers;
   if (static_cast<int64_t>(blockIdx.x) >= workers) {

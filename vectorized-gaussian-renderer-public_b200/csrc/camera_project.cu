@@ -539,6 +539,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
   __shared__ CamConst s_cams[kTicketBatch];
   __shared__ __align__(8) CamPlan s_plans[kTicketBatch];
   __shared__ int64_t s_vbs[kTicketBatch];
+  __shared__ uint32_t s_cmask[kTicketBatch];  // live clusters of each staged block
   __shared__ int s_nlive;
   __shared__ int s_exhausted;
   __shared__ uint64_t s_base_vis, s_base_isect;
@@ -607,10 +608,35 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         if (s_exhausted) break;
         continue;
       }
+      if (p.cluster_bounds && !kRay) {
+        // Cluster cull of the staged blocks, the chunk test on each
+        // cluster's box: bit k of s_cmask[v] is set when cluster k (tasks
+        // [32 k, 32 k + 32) of block v, one warp-round) may hold a Gaussian
+        // the screen cull keeps.  One lane per cluster; 32 lanes cover two
+        // blocks.
+        static_assert(kProjectClusters == 16, "two blocks' clusters per warp ballot");
+        for (int base = warp * 32; base < nlive * kProjectClusters; base += kProjectThreads) {
+          const int idx = base + lane;
+          bool keep = true;
+          if (idx < nlive * kProjectClusters) {
+            const int v = idx / kProjectClusters;
+            const int64_t ci = p.chunk_offsets[s_plans[v].scene_slot] + s_vbs[v] / p.active_count;
+            const int64_t row = ci * kProjectClusters + (idx - v * kProjectClusters);
+            keep = !chunk_outside_frustum(s_cams[v], p.cluster_bounds[row * 2], p.cluster_bounds[row * 2 + 1],
+                                          p.near_plane, p.far_plane, p.support_sigma, p.cov_eps);
+          }
+          const uint32_t bits = __ballot_sync(0xffffffffu, keep);
+          const int v0 = base / kProjectClusters;
+          if (lane == 0) s_cmask[v0] = bits & 0xffffu;
+          if (lane == 16 && v0 + 1 < nlive) s_cmask[v0 + 1] = bits >> 16;
+        }
+        __syncthreads();
+      }
     }
     const int64_t b = s_vbs[cursor];
     const CamPlan& plan = s_plans[cursor];
     const CamConst& s_cam = s_cams[cursor];
+    const uint32_t cluster_mask = p.cluster_bounds && !kRay ? s_cmask[cursor] : 0xffffffffu;
     ++cursor;
     const int64_t chunk = b / p.active_count;
     const int64_t local_begin = chunk * kProjectChunk;
@@ -629,7 +655,7 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
       vis[round] = false;
       ntiles[round] = 0;
       Projected pr;
-      if (live && local < plan.g_count) {
+      if (live && local < plan.g_count && ((cluster_mask >> (round * (kProjectThreads / 32) + warp)) & 1u)) {
         const int64_t g = plan.g_begin + local;
         vis[round] = project_gaussian<kRay>(p.means, p.covariances, p.opacities, g, s_cam, p.near_plane,
                                       p.far_plane, p.support_sigma, p.cov_eps, p.antialiased, &pr);
@@ -943,16 +969,19 @@ __global__ void __launch_bounds__(kProjectThreads, 4) project_emit_kernel(Projec
         const uint64_t r = base_vis + i;
         uint64_t key = ~0ull;
         int32_t value = 0;
+        const uint64_t tile = static_cast<uint64_t>(plan.tile_base) +
+                              static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
         if (r < vcap) {
-          const uint64_t tile = static_cast<uint64_t>(plan.tile_base) +
-                                static_cast<uint64_t>(min_ty + ty) * tiles_x + (min_tx + tx);
           key = (tile << 32) | static_cast<uint64_t>(__float_as_uint(s_rec[slot].b.z));
           value = static_cast<int32_t>(r);
-          // Bucket size for the tile sort (a tile past the batch's range - a
-          // caller's inconsistent ragged offsets - is left to the scatter's
-          // overflow tail).
-          if (tile < static_cast<uint64_t>(p.tile_count)) atomicAdd(p.tile_counts + tile, 1u);
         }
+        // Bucket size for the tile sort (a tile past the batch's range - a
+        // caller's inconsistent ragged offsets - is left to the scatter's
+        // overflow tail): one atomic per group of lanes with the same tile.
+        const bool counted = r < vcap && tile < static_cast<uint64_t>(p.tile_count);
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, counted ? static_cast<uint32_t>(tile) : 0xffffffffu);
+        if (counted && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(p.tile_counts + tile, __popc(peers));
         p.keys[base_isect + j] = key;
         p.values[base_isect + j] = value;
       }

@@ -160,6 +160,40 @@ __global__ void __launch_bounds__(kBoundsThreads) chunk_bounds_kernel(
   }
 }
 
+// One warp per cluster of kProjectCluster Gaussians (lane = Gaussian): the
+// same bounds as chunk_bounds_kernel; a cluster past the end of the scene
+// gets an empty box (lo = +inf, hi = -inf) and trace 0.
+__global__ void __launch_bounds__(256) cluster_bounds_kernel(const float* __restrict__ means,
+                                                             const float* __restrict__ covariances,
+                                                             int64_t count, int64_t clusters,
+                                                             float4* __restrict__ bounds) {
+  const int64_t cluster = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (cluster >= clusters) return;  // warp-uniform
+  const int lane = threadIdx.x & 31;
+  const int64_t g = cluster * kProjectCluster + lane;
+  const float inf = __int_as_float(0x7f800000);
+  float v[7] = {inf, inf, inf, inf, inf, inf, 0.0f};  // lo xyz, -hi xyz, -trace
+  if (g < count) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      v[a] = means[g * 3 + a];
+      v[3 + a] = -v[a];
+    }
+    const float* s = covariances + g * 6;
+    v[6] = -(s[0] + s[3] + s[5]);
+  }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+  }
+  if (lane == 0) {
+    // A non-finite mean or trace disables culling for the cluster.
+    bounds[cluster * 2 + 0] = make_float4(v[0], v[1], v[2], -v[6]);
+    bounds[cluster * 2 + 1] = make_float4(-v[3], -v[4], -v[5], 0.0f);
+  }
+}
+
 unsigned grid_for(int64_t items, int threads) {
   const int64_t blocks = (items + threads - 1) / threads;
   return static_cast<unsigned>(blocks < 1 ? 1 : blocks);
@@ -255,4 +289,17 @@ extern "C" int vgr_scene_chunk_bounds(const float* means, const float* covarianc
                         static_cast<cudaStream_t>(stream_ptr)>>>(means, covariances, count,
                                                                  reinterpret_cast<float4*>(bounds));
   return check_launch("chunk bounds");
+}
+
+extern "C" int vgr_scene_cluster_bounds(const float* means, const float* covariances, int64_t count,
+                                        float* bounds, void* stream_ptr) {
+  if (!means || !covariances || !bounds) return fail(VGR_ERR_INVALID_ARGUMENT, "arguments must be non-null");
+  if (count <= 0 || count > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "a scene needs 1..INT_MAX Gaussians");
+  if ((reinterpret_cast<uintptr_t>(bounds) & 15) != 0) {
+    return fail(VGR_ERR_INVALID_ARGUMENT, "bounds must be 16-byte aligned");
+  }
+  const int64_t clusters = (count + kProjectChunk - 1) / kProjectChunk * kProjectClusters;
+  cluster_bounds_kernel<<<grid_for(clusters * 32, 256), 256, 0, static_cast<cudaStream_t>(stream_ptr)>>>(
+      means, covariances, count, clusters, reinterpret_cast<float4*>(bounds));
+  return check_launch("cluster bounds");
 }

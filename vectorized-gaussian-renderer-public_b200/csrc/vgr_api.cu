@@ -33,6 +33,7 @@ thread_local OccupancyCache g_occ;
 }  // namespace
 
 static_assert(vgr::kProjectChunk == VGR_PROJECT_CHUNK, "projection chunk of the C ABI");
+static_assert(vgr::kProjectCluster == VGR_PROJECT_CLUSTER, "projection cluster of the C ABI");
 static_assert(vgr::kDenseBuckets == VGR_DENSE_DEPTH_BUCKETS, "dense depth buckets of the C ABI");
 static_assert(vgr::kDenseSubtile == VGR_DENSE_CELL, "dense optical-thickness cell of the C ABI");
 
@@ -510,10 +511,14 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     pp.gaussian_ids = scene->gaussian_ids;
     pp.chunk_bounds = reinterpret_cast<const float4*>(scene->chunk_bounds);
     pp.chunk_offsets = scene->chunk_offsets;
+    pp.cluster_bounds = scene->chunk_bounds ? reinterpret_cast<const float4*>(scene->cluster_bounds) : nullptr;
     if (scene->chunk_bounds &&
         (!scene->chunk_offsets || (reinterpret_cast<uintptr_t>(scene->chunk_bounds) & 15) != 0)) {
       return fail(VGR_ERR_INVALID_ARGUMENT,
                   "chunk_bounds must be 16-byte aligned and come with chunk_offsets");
+    }
+    if ((reinterpret_cast<uintptr_t>(scene->cluster_bounds) & 15) != 0) {
+      return fail(VGR_ERR_INVALID_ARGUMENT, "cluster_bounds must be 16-byte aligned");
     }
     if (pp.mirror_means2d && !(pp.mirror_conics && pp.mirror_depths && pp.mirror_opacities &&
                                pp.mirror_camera_ids && pp.mirror_gaussian_ids && pp.mirror_radii)) {
@@ -616,7 +621,7 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     bucket_scatter_kernel<<<static_cast<unsigned>(sgrid), 256, 0, stream>>>(bp);
     if ((rc = check_launch("render: bucket scatter")) != VGR_OK) return rc;
     mark(4);
-    bp.large_workers = static_cast<int64_t>(sms) * 5;
+    bp.large_workers = static_cast<int64_t>(sms) * 4;  // one per resident tile-sort CTA
     bp.large_list = ws->values_in;
     if (global_tiles + bp.large_workers > INT_MAX) {
       return fail(VGR_ERR_INVALID_ARGUMENT, "tile sort grid exceeds CUDA limit");

@@ -159,6 +159,10 @@ static_assert(sizeof(ScratchHeader) == 128, "ScratchHeader layout");
 constexpr int kProjectThreads = 256;
 constexpr int kProjectRounds = 2;
 constexpr int kProjectChunk = kProjectThreads * kProjectRounds;  // tasks per virtual block
+// A warp-round of the projection: the unit of the cluster cull.
+constexpr int kProjectCluster = 32;
+constexpr int kProjectClusters = kProjectChunk / kProjectCluster;  // clusters per chunk
+static_assert(kProjectClusters <= 32, "one bit per cluster in a 32-bit mask");
 constexpr int kTicketBatch = 32;  // virtual blocks taken per queue ticket (one per lane)
 constexpr int kOwnerKeys = 2048;  // keys per block whose owners the projection tabulates
 

@@ -74,6 +74,7 @@ struct ProjectParams {
   const int32_t* gaussian_ids; // reported id of packed Gaussian g, or null (g itself)
   const float4* chunk_bounds;  // [C,2] per-chunk bounds, or null (no chunk culling)
   const int64_t* chunk_offsets;// [S+1] first chunk of each registered scene
+  const float4* cluster_bounds;// [C*kProjectClusters,2] per-cluster bounds, or null
   float4* ray_ext;             // exact-ray mode: [V,3] extension records, else null
   // Dense mode (optical-thickness depth cutoff).
   float* depth_tau;            // [B * sub-tiles, kDenseBuckets] optical-thickness lower bounds

@@ -21,6 +21,7 @@ VGR_ERR_SCRATCH_TOO_SMALL = -3
 VGR_ERR_UNSUPPORTED = -4
 RECORD_BYTES = 48
 PROJECT_CHUNK = 512
+PROJECT_CLUSTER = 32
 DENSE_DEPTH_BUCKETS = 256
 DENSE_CELL = 4
 STAGE_EVENTS = 7
@@ -46,6 +47,7 @@ class VgrScene(ctypes.Structure):
         ("gaussian_ids", _c_p),
         ("chunk_bounds", _c_p),
         ("chunk_offsets", _c_p),
+        ("cluster_bounds", _c_p),
     ]
 
 
@@ -230,6 +232,7 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
     ("vgr_scene_spatial_order_temp_bytes", _c_i64, [_c_i64]),
     ("vgr_scene_spatial_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
     ("vgr_scene_chunk_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
+    ("vgr_scene_cluster_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
     (
         "vgr_train_activate",
         ctypes.c_int,

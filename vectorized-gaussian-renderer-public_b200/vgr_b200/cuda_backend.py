@@ -716,6 +716,7 @@ class CustomCudaBackend:
             gaussian_ids=packed["gaussian_ids"].data_ptr() if "gaussian_ids" in packed else None,
             chunk_bounds=packed["chunk_bounds"].data_ptr() if "chunk_bounds" in packed else None,
             chunk_offsets=packed["chunk_offsets"].data_ptr() if "chunk_offsets" in packed else None,
+            cluster_bounds=packed["cluster_bounds"].data_ptr() if "cluster_bounds" in packed else None,
         )
 
     def set_stage_events(self, events: list[torch.cuda.Event] | None) -> None:
@@ -1316,6 +1317,9 @@ class CustomCudaBackend:
             for scene in scenes:
                 chunk_offsets.append(chunk_offsets[-1] + (scene.count + chunk - 1) // chunk)
             bounds = torch.empty((chunk_offsets[-1], 8), dtype=torch.float32, device=self.device)
+            clusters_per_chunk = chunk // _native.PROJECT_CLUSTER
+            cluster_bounds = torch.empty((chunk_offsets[-1] * clusters_per_chunk, 8), dtype=torch.float32,
+                                         device=self.device)
             for s, scene in enumerate(scenes):
                 off = offsets[s]
                 _native.check(
@@ -1325,7 +1329,15 @@ class CustomCudaBackend:
                     ),
                     "chunk bounds",
                 )
+                _native.check(
+                    lib.vgr_scene_cluster_bounds(
+                        packed["means"][off:].data_ptr(), covariances[off:].data_ptr(), scene.count,
+                        cluster_bounds[chunk_offsets[s] * clusters_per_chunk:].data_ptr(), stream,
+                    ),
+                    "cluster bounds",
+                )
             packed["chunk_bounds"] = bounds
+            packed["cluster_bounds"] = cluster_bounds
             packed["chunk_offsets"] = torch.tensor(chunk_offsets, device=self.device, dtype=torch.int64)
         packed["registered_scene_ids"] = torch.tensor(list(self._scenes), device=self.device, dtype=torch.int64)
         packed["scene_offsets"] = torch.tensor(offsets, device=self.device, dtype=torch.int64)
