@@ -48,11 +48,11 @@ constexpr int kMaxCluster = 16;  // candidates kept per cluster window in one tr
 constexpr uint32_t kNonPlanarKey = 1u << 30;
 
 struct __align__(16) Surfel {
-  float4 m;   // mean xyz, opacity
+  float4 m;   // mean xyz, max(scale0, scale1)^2 (all the distance pre-test reads)
   float4 n;   // normal xyz, surface confidence
   float4 a0;  // tangent axis 0 xyz, scale 0
   float4 a1;  // tangent axis 1 xyz, scale 1
-  float4 e;   // reflectivity, max(scale0, scale1)^2, -, -
+  float4 e;   // reflectivity, opacity, -, -
 };
 static_assert(sizeof(Surfel) == 80, "Surfel layout");
 
@@ -228,12 +228,12 @@ __global__ void __launch_bounds__(kLidarThreads) lidar_gather_kernel(BuildParams
   float3 axes[3];
   quaternion_axes(p.rotations + g * 4, axes);
   Surfel s;
-  s.m = make_float4(p.means[g * 3 + 0], p.means[g * 3 + 1], p.means[g * 3 + 2], p.opacities[g]);
+  const float smax = fmaxf(sc[t0], sc[t1]);
+  s.m = make_float4(p.means[g * 3 + 0], p.means[g * 3 + 1], p.means[g * 3 + 2], smax * smax);
   s.n = make_float4(axes[n].x, axes[n].y, axes[n].z, p.confidence ? p.confidence[g] : 1.0f);
   s.a0 = make_float4(axes[t0].x, axes[t0].y, axes[t0].z, sc[t0]);
   s.a1 = make_float4(axes[t1].x, axes[t1].y, axes[t1].z, sc[t1]);
-  const float smax = fmaxf(sc[t0], sc[t1]);
-  s.e = make_float4(p.reflectivity ? p.reflectivity[g] : -1.0f, smax * smax, 0.0f, 0.0f);
+  s.e = make_float4(p.reflectivity ? p.reflectivity[g] : -1.0f, p.opacities[g], 0.0f, 0.0f);
   surfels[i] = s;
   sem[i] = p.semantics[g];
 }
@@ -450,13 +450,12 @@ struct Candidate {
 __device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const TraceParams& p,
                                          Candidate* c) {
   const float4 m = __ldg(&sp->m);
-  const float4 e = __ldg(&sp->e);
   const float3 dm = make_float3(m.x - r.o.x, m.y - r.o.y, m.z - r.o.z);
   const float cx = dm.y * r.d.z - dm.z * r.d.y;
   const float cy = dm.z * r.d.x - dm.x * r.d.z;
   const float cz = dm.x * r.d.y - dm.y * r.d.x;
   const float dist2 = (cx * cx + cy * cy + cz * cz) * r.inv_dd;
-  if (!(dist2 <= p.q_max * e.y * 1.001f + 1.0e-5f)) return false;
+  if (!(dist2 <= p.q_max * m.w * 1.001f + 1.0e-5f)) return false;
   const float4 n = __ldg(&sp->n);
   const float denom = n.x * r.d.x + n.y * r.d.y + n.z * r.d.z;
   const float incidence = fabsf(denom);
@@ -472,7 +471,8 @@ __device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const T
   const float q = u * u + v * v;
   if (!(q <= p.q_max)) return false;
   const float support = expf(-0.5f * q);
-  const float weight = m.w * support * n.w;
+  const float4 e = __ldg(&sp->e);
+  const float weight = e.y * support * n.w;
   if (!(weight >= p.threshold) || !isfinite(weight)) return false;
   const float refl = e.x >= 0.0f ? e.x : p.fallback_reflectivity;
   c->t = t;
@@ -498,20 +498,19 @@ struct TraceStats {
 // instead of up to 32 divergent ones (coherent rays of a scan share most of
 // their nodes).  Children hit by several lanes are ordered by the majority's
 // nearer child.
+// The node-code and lane-mask stacks of a warp whose 32 lanes traverse one
+// hierarchy together live in shared memory (the entries are the same in
+// every lane, and every lane writes the same values, so no lane can read a
+// slot another lane has not finished writing); each lane's entry distances
+// stay in its own local array.  A partial group keeps all three locally.
+__shared__ int s_trace_stack[kTraceThreads / 32][kMaxStack];
+__shared__ uint32_t s_trace_lanes[kTraceThreads / 32][kMaxStack];
+
 template <typename Visit>
-__device__ __forceinline__ void traverse(const LidarDescriptor& sc, int leaves, const Ray& r,
-                                         float tmin, float* tmax, TraceStats& st, Visit visit) {
-  if (leaves <= 0) return;
-  if (leaves == 1) {
-    ++st.nodes;
-    visit(0);
-    return;
-  }
-  const unsigned group =
-      __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(sc.nodes));
+__device__ __forceinline__ void traverse_walk(const LidarDescriptor& sc, const Ray& r, float tmin,
+                                              float* tmax, TraceStats& st, Visit& visit,
+                                              unsigned group, int* stack, uint32_t* lanes) {
   const int lane = threadIdx.x & 31;
-  int stack[kMaxStack];
-  uint32_t lanes[kMaxStack];
   float entry[kMaxStack];
   int top = 0;
   stack[top] = 0;
@@ -569,6 +568,27 @@ __device__ __forceinline__ void traverse(const LidarDescriptor& sc, int leaves, 
       entry[top] = er;
       ++top;
     }
+  }
+}
+
+template <bool kWarpStack, typename Visit>
+__device__ __forceinline__ void traverse(const LidarDescriptor& sc, int leaves, const Ray& r,
+                                         float tmin, float* tmax, TraceStats& st, Visit visit) {
+  if (leaves <= 0) return;
+  if (leaves == 1) {
+    ++st.nodes;
+    visit(0);
+    return;
+  }
+  const unsigned group =
+      __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(sc.nodes));
+  if (kWarpStack && group == 0xffffffffu) {
+    const int warp = threadIdx.x >> 5;
+    traverse_walk(sc, r, tmin, tmax, st, visit, group, s_trace_stack[warp], s_trace_lanes[warp]);
+  } else {
+    int stack[kMaxStack];
+    uint32_t lanes[kMaxStack];
+    traverse_walk(sc, r, tmin, tmax, st, visit, group, stack, lanes);
   }
 }
 
@@ -668,7 +688,7 @@ __global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TracePar
           bool list_full = false;
           int32_t list_idx[kMaxCluster];
           float list_t[kMaxCluster];
-          traverse(sc, leaves, r, p.near_plane, &window, st, [&](int leaf) {
+          traverse<true>(sc, leaves, r, p.near_plane, &window, st, [&](int leaf) {
             const int begin = leaf * sc.packet;
             const int end = min(begin + sc.packet, m);
             for (int i = begin; i < end; ++i) {
@@ -739,7 +759,7 @@ __global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TracePar
             }
           } else {
             float window_end = cluster_end;
-            traverse(sc, leaves, r, first_t, &window_end, st, [&](int leaf) {
+            traverse<false>(sc, leaves, r, first_t, &window_end, st, [&](int leaf) {
               const int begin = leaf * sc.packet;
               const int end = min(begin + sc.packet, m);
               for (int i = begin; i < end; ++i) {
