@@ -451,7 +451,7 @@ __device__ __forceinline__ void sh_direction_grad(float x, float y, float z, con
 }
 
 template <int kShDegree>
-__global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kernel(ProjectBackwardParams p) {
+__global__ void __launch_bounds__(kProjectBackwardThreads, 4) project_backward_kernel(ProjectBackwardParams p) {
   constexpr int kCount = kShDegree < 0 ? 1 : (kShDegree + 1) * (kShDegree + 1);
   constexpr int kFloats = kShDegree < 0 ? 3 : kCount * 3;
   constexpr int kVec = (kFloats + 3) / 4;
@@ -479,24 +479,10 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
   const float s00 = p.covariances[g * 6 + 0], s01 = p.covariances[g * 6 + 1];
   const float s02 = p.covariances[g * 6 + 2], s11 = p.covariances[g * 6 + 3];
   const float s12 = p.covariances[g * 6 + 4], s22 = p.covariances[g * 6 + 5];
-  // The Gaussian's colour coefficients, loaded once.
-  float coef[kVec * 4];
-  {
-    const float* row = p.features + g * p.feature_width;
-    if (p.vector_feature_loads) {
-#pragma unroll
-      for (int i = 0; i < kVec; ++i) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(row) + i);
-        coef[4 * i + 0] = v.x;
-        coef[4 * i + 1] = v.y;
-        coef[4 * i + 2] = v.z;
-        coef[4 * i + 3] = v.w;
-      }
-    } else {
-#pragma unroll
-      for (int f = 0; f < kVec * 4; ++f) coef[f] = f < kFloats ? __ldg(row + f) : 0.0f;
-    }
-  }
+  // The Gaussian's colour coefficients are read again at each camera that
+  // sees it (L1 hits after the first): held in registers across the loop
+  // they capped the kernel at two CTAs per SM.
+  const float* coef_row = p.features + g * p.feature_width;
 
   float dm[3] = {0.0f, 0.0f, 0.0f};
   float dcov[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
@@ -634,6 +620,20 @@ __global__ void __launch_bounds__(kProjectBackwardThreads) project_backward_kern
       const float x = fmul(dvx, inv), y = fmul(dvy, inv), z = fmul(dvz, inv);
       float basis[16];
       sh_basis<kShDegree < 0 ? 0 : kShDegree>(x, y, z, basis);
+      float coef[kVec * 4];
+      if (p.vector_feature_loads) {
+#pragma unroll
+        for (int i = 0; i < kVec; ++i) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(coef_row) + i);
+          coef[4 * i + 0] = v.x;
+          coef[4 * i + 1] = v.y;
+          coef[4 * i + 2] = v.z;
+          coef[4 * i + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < kVec * 4; ++f) coef[f] = f < kFloats ? __ldg(coef_row + f) : 0.0f;
+      }
       float acc[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
       for (int k = 0; k < kCount; ++k) {
