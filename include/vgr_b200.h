@@ -207,6 +207,10 @@ const char* vgr_version(void);
 /* Number of kernels this library has launched in this process (all threads).
  * No counterpart in the reference; used to attribute launches in benchmarks. */
 int64_t vgr_kernel_launch_count(void);
+/* VGR_PROJECT_CHUNK of the loaded library: the number of Gaussians per row of
+ * vgr_scene.chunk_bounds (a host that sizes the bounds at run time asks the
+ * library rather than its own copy of the header). */
+int64_t vgr_project_chunk(void);
 /* Thread-local message of the last failing call on this thread. */
 const char* vgr_last_error(void);
 

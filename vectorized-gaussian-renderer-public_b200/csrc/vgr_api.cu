@@ -91,6 +91,7 @@ extern "C" const char* vgr_version(void) { return "vgr_b200 0.1.0 sm_100a"; }
 extern "C" const char* vgr_last_error(void) { return g_last_error; }
 
 extern "C" int64_t vgr_kernel_launch_count(void) { return g_launch_count.load(); }
+extern "C" int64_t vgr_project_chunk(void) { return kProjectChunk; }
 
 extern "C" int64_t vgr_render_scratch_bytes(int64_t intersection_capacity,
                                             int64_t max_projection_tasks, int64_t global_tiles,

@@ -176,6 +176,7 @@ class VgrPlyLayout(ctypes.Structure):
 CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
     ("vgr_version", ctypes.c_char_p, []),
     ("vgr_kernel_launch_count", _c_i64, []),
+    ("vgr_project_chunk", _c_i64, []),
     ("vgr_last_error", ctypes.c_char_p, []),
     ("vgr_render_scratch_bytes", _c_i64, [_c_i64, _c_i64, _c_i64, _c_i64]),
     ("vgr_sort_temp_bytes", _c_i64, [_c_i64, _c_i64]),

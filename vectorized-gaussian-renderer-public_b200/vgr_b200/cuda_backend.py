@@ -1312,7 +1312,7 @@ class CustomCudaBackend:
             packed["gaussian_ids"] = torch.cat(
                 [order + off for order, off in zip(orders, offsets[:-1])]
             ).to(torch.int32).contiguous()
-            chunk = _native.PROJECT_CHUNK
+            chunk = int(lib.vgr_project_chunk())
             chunk_offsets = [0]
             for scene in scenes:
                 chunk_offsets.append(chunk_offsets[-1] + (scene.count + chunk - 1) // chunk)
