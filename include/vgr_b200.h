@@ -464,6 +464,15 @@ typedef struct vgr_lidar_scene {
 
 /* Shared sensor-local rays against per-sensor scenes
  * (lidar_renderer.cpp:133-210 inputs[6]). */
+/* A trace order for vgr_lidar_inputs.ray_order (no counterpart in the
+ * reference): the rays sorted by a 30-bit Morton code of their direction's
+ * azimuth and elevation on one angular grid, so 32 consecutive entries are a
+ * compact patch of directions.  temp: vgr_lidar_ray_order_temp_bytes(rays)
+ * bytes, 256-byte aligned.  Compute it once per direction set. */
+int64_t vgr_lidar_ray_order_temp_bytes(int64_t rays);
+int vgr_lidar_ray_order(const float* ray_directions, int64_t rays, int32_t* order, void* temp,
+                        int64_t temp_bytes, void* stream);
+
 typedef struct vgr_lidar_inputs {
   const float* ray_directions;      /* [R,3] unit, sensor frame */
   int64_t rays;                     /* R */
@@ -475,6 +484,13 @@ typedef struct vgr_lidar_inputs {
   int64_t batch;                    /* B */
   const int64_t* active_sensor_ids; /* [A] strictly increasing, or NULL (all) */
   int64_t active_count;
+  /* Optional (no counterpart in the reference; NULL = ray order): a
+   * permutation of 0..R-1 in which the rays are traced, 32 consecutive
+   * entries per warp.  Rays whose directions are close share most of their
+   * hierarchy walk, so an order that groups them (vgr_lidar_ray_order)
+   * traces faster; outputs stay indexed by ray.  An entry outside 0..R-1 is counted as an
+   * invalid direction and traces nothing. */
+  const int32_t* ray_order;         /* [R] or NULL */
 } vgr_lidar_inputs;
 
 /* outputs[7] of the reference: every element is rewritten each call. */

@@ -374,6 +374,7 @@ struct TraceParams {
   const int64_t* scene_ids;
   const int64_t* active;
   int64_t active_count;
+  const int32_t* ray_order;  // [rays] trace order, or null
   int64_t batch;
   int returns;
   float near_plane, far_plane, q_max, threshold, min_cos, cluster_abs, cluster_rel;
@@ -617,10 +618,14 @@ __global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TracePar
   TraceStats st{0u, 0u, 0u, false};
   if (work < total) {
     const int64_t a = work / p.rays;
-    const int64_t ray = work - a * p.rays;
+    const int64_t local = work - a * p.rays;
+    const int64_t ray = p.ray_order ? static_cast<int64_t>(p.ray_order[local]) : local;
     int64_t sensor = p.active ? p.active[a] : a;
     bool ok = true;
-    if (p.active && a > 0 && sensor <= p.active[a - 1]) {
+    if (ray < 0 || ray >= p.rays) {
+      bad_dir = 1u;  // a ray order that is not a permutation
+      ok = false;
+    } else if (p.active && a > 0 && sensor <= p.active[a - 1]) {
       bad_active = ray == 0 ? 1u : 0u;
       ok = false;
     } else if (sensor < 0 || sensor >= p.batch) {
@@ -1028,6 +1033,7 @@ extern "C" int vgr_render_lidar(const void* descriptors, int64_t scene_count,
   tp.scene_count = static_cast<int>(scene_count);
   tp.dirs = in->ray_directions;
   tp.rays = in->rays;
+  tp.ray_order = in->ray_order;
   tp.times_i64 = in->time_offsets_are_int64 ? static_cast<const int64_t*>(in->time_offsets) : nullptr;
   tp.times_i32 = in->time_offsets_are_int64 ? nullptr : static_cast<const int32_t*>(in->time_offsets);
   tp.sensor_to_world = in->sensor_to_world;

@@ -57,6 +57,17 @@ OrderLayout make_order_layout(int64_t count) {
   return l;
 }
 
+// Spreads the low 15 bits of v to every other bit (one axis of a 30-bit 2D
+// Morton code).
+__device__ __forceinline__ uint64_t spread_bits2(uint32_t v) {
+  uint64_t x = v & 0x7fffu;
+  x = (x | (x << 8)) & 0x00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0full;
+  x = (x | (x << 2)) & 0x33333333ull;
+  x = (x | (x << 1)) & 0x55555555ull;
+  return x;
+}
+
 __global__ void order_init_kernel(unsigned char* base, OrderLayout l, int64_t count) {
   OrderHeader* h = reinterpret_cast<OrderHeader*>(base + l.header);
   for (int a = 0; a < 3; ++a) {
@@ -111,6 +122,31 @@ __global__ void __launch_bounds__(256) order_keys_kernel(const float* __restrict
   }
   keys[g] = expand_bits(q[0]) | (expand_bits(q[1]) << 1) | (expand_bits(q[2]) << 2);
   vals[g] = static_cast<int32_t>(g);
+}
+
+// 30-bit Morton key of each direction's (azimuth, elevation) on one angular
+// grid of 2 pi / 32768 per step on both axes (isotropic in angle, so 32
+// consecutive keys form a compact patch of directions); value = index.  A
+// non-finite direction gets key 0.
+__global__ void __launch_bounds__(256) order_angle_keys_kernel(const float* __restrict__ dirs,
+                                                               int64_t count, uint64_t* keys,
+                                                               int32_t* vals) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float x = dirs[i * 3 + 0], y = dirs[i * 3 + 1], z = dirs[i * 3 + 2];
+  const float norm = sqrtf(x * x + y * y + z * z);
+  uint64_t key = 0;
+  if (isfinite(norm) && norm > 0.0f) {
+    constexpr float kPi = 3.14159265358979f;
+    constexpr float kStep = 32768.0f / (2.0f * kPi);
+    const float az = atan2f(y, x);                                // [-pi, pi]
+    const float el = asinf(fminf(fmaxf(z / norm, -1.0f), 1.0f));  // [-pi/2, pi/2]
+    const uint32_t qa = min(static_cast<uint32_t>(fmaxf((az + kPi) * kStep, 0.0f)), 32767u);
+    const uint32_t qe = min(static_cast<uint32_t>(fmaxf((el + 0.5f * kPi) * kStep, 0.0f)), 32767u);
+    key = spread_bits2(qa) | (spread_bits2(qe) << 1);
+  }
+  keys[i] = key;
+  vals[i] = static_cast<int32_t>(i);
 }
 
 __global__ void __launch_bounds__(256) order_copy_kernel(const int32_t* __restrict__ sorted,
@@ -211,10 +247,15 @@ extern "C" int64_t vgr_scene_spatial_order_temp_bytes(int64_t gaussian_count) {
   return make_order_layout(gaussian_count).total;
 }
 
-extern "C" int vgr_scene_spatial_order(const float* means, int64_t count, int32_t* order,
-                                       void* temp, int64_t temp_bytes, void* stream_ptr) {
+namespace {
+
+// Stable order of `count` points by a 30-bit Morton key: of the 3D points
+// over their bounding box, or (angular) of the directions' azimuth and
+// elevation.
+int morton_order(const float* means, int64_t count, int32_t* order, void* temp, int64_t temp_bytes,
+                 void* stream_ptr, bool angular) {
   if (!means || !order || !temp) return fail(VGR_ERR_INVALID_ARGUMENT, "arguments must be non-null");
-  if (count <= 0 || count > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "a scene needs 1..INT_MAX Gaussians");
+  if (count <= 0 || count > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "an order needs 1..INT_MAX items");
   if ((reinterpret_cast<uintptr_t>(temp) & 255) != 0) {
     return fail(VGR_ERR_INVALID_ARGUMENT, "temp buffer must be 256-byte aligned");
   }
@@ -233,13 +274,19 @@ extern "C" int vgr_scene_spatial_order(const float* means, int64_t count, int32_
   if ((rc = check_launch("spatial order: init")) != VGR_OK) return rc;
   unsigned bgrid = grid_for(count, 256);
   if (bgrid > static_cast<unsigned>(sms * 4)) bgrid = static_cast<unsigned>(sms * 4);
-  order_bounds_kernel<<<bgrid, 256, 0, stream>>>(means, count, h);
-  if ((rc = check_launch("spatial order: bounds")) != VGR_OK) return rc;
+  if (!angular) {
+    order_bounds_kernel<<<bgrid, 256, 0, stream>>>(means, count, h);
+    if ((rc = check_launch("spatial order: bounds")) != VGR_OK) return rc;
+  }
   uint64_t* kin = reinterpret_cast<uint64_t*>(base + layout.keys_a);
   uint64_t* kout = reinterpret_cast<uint64_t*>(base + layout.keys_b);
   int32_t* vin = reinterpret_cast<int32_t*>(base + layout.vals_a);
   int32_t* vout = reinterpret_cast<int32_t*>(base + layout.vals_b);
-  order_keys_kernel<<<grid_for(count, 256), 256, 0, stream>>>(means, count, h, kin, vin);
+  if (angular) {
+    order_angle_keys_kernel<<<grid_for(count, 256), 256, 0, stream>>>(means, count, kin, vin);
+  } else {
+    order_keys_kernel<<<grid_for(count, 256), 256, 0, stream>>>(means, count, h, kin, vin);
+  }
   if ((rc = check_launch("spatial order: keys")) != VGR_OK) return rc;
 
   // Stable raw-key radix sort of the 30-bit keys (the onesweep of the LBVH).
@@ -275,6 +322,23 @@ extern "C" int vgr_scene_spatial_order(const float* means, int64_t count, int32_
   }
   order_copy_kernel<<<grid_for(count, 256), 256, 0, stream>>>(vin, count, order);
   return check_launch("spatial order: copy");
+}
+
+}  // namespace
+
+extern "C" int vgr_scene_spatial_order(const float* means, int64_t count, int32_t* order,
+                                       void* temp, int64_t temp_bytes, void* stream_ptr) {
+  return morton_order(means, count, order, temp, temp_bytes, stream_ptr, false);
+}
+
+extern "C" int64_t vgr_lidar_ray_order_temp_bytes(int64_t rays) {
+  if (rays <= 0 || rays > INT_MAX) return fail(VGR_ERR_INVALID_ARGUMENT, "an order needs 1..INT_MAX rays");
+  return make_order_layout(rays).total;
+}
+
+extern "C" int vgr_lidar_ray_order(const float* ray_directions, int64_t rays, int32_t* order, void* temp,
+                                   int64_t temp_bytes, void* stream_ptr) {
+  return morton_order(ray_directions, rays, order, temp, temp_bytes, stream_ptr, true);
 }
 
 extern "C" int vgr_scene_chunk_bounds(const float* means, const float* covariances, int64_t count,

@@ -234,6 +234,8 @@ CAMERA_SIGNATURES: list[tuple[str, object, list[object]]] = [
     ("vgr_scene_spatial_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
     ("vgr_scene_chunk_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
     ("vgr_scene_cluster_bounds", ctypes.c_int, [_c_p, _c_p, _c_i64, _c_p, _c_p]),
+    ("vgr_lidar_ray_order_temp_bytes", _c_i64, [_c_i64]),
+    ("vgr_lidar_ray_order", ctypes.c_int, [_c_p, _c_i64, _c_p, _c_p, _c_i64, _c_p]),
     (
         "vgr_train_activate",
         ctypes.c_int,

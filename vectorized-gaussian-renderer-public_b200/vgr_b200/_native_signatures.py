@@ -38,6 +38,7 @@ class VgrLidarInputs(ctypes.Structure):
         ("batch", _i64),
         ("active_sensor_ids", _p),
         ("active_count", _i64),
+        ("ray_order", _p),
     ]
 
 

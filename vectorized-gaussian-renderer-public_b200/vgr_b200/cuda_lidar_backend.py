@@ -61,6 +61,35 @@ class _SceneAcceleration:
         return int(self.accel.numel())
 
 
+class RayOrder:
+    """Trace order of a ray-direction tensor: ``vgr_lidar_ray_order``, a Morton
+    order of the directions' azimuth and elevation, so the 32 rays a warp
+    traces together are a compact patch of directions and share most of their
+    hierarchy walk.  Recomputed only when the tensor's storage, length or
+    version changes."""
+
+    def __init__(self) -> None:
+        self._key: tuple | None = None
+        self._order: torch.Tensor | None = None
+
+    def __call__(self, directions: torch.Tensor) -> torch.Tensor:
+        key = (directions.device, directions.data_ptr(), directions.shape[0], directions._version)
+        if key != self._key or self._order is None:
+            rays = directions.shape[0]
+            lib = _native.load_library()
+            temp_bytes = _native.check_size(lib.vgr_lidar_ray_order_temp_bytes(rays), "ray order")
+            order = torch.empty((rays,), dtype=torch.int32, device=directions.device)
+            temp = torch.empty((temp_bytes,), dtype=torch.uint8, device=directions.device)
+            stream = torch.cuda.current_stream(directions.device).cuda_stream
+            _native.check(
+                lib.vgr_lidar_ray_order(directions.data_ptr(), rays, order.data_ptr(), temp.data_ptr(),
+                                        temp_bytes, stream),
+                "ray order",
+            )
+            self._key, self._order = key, order
+        return self._order
+
+
 def native_scene(scene: GaussianLidarScene) -> VgrLidarScene:
     return VgrLidarScene(
         means=scene.means.data_ptr(),
@@ -135,6 +164,7 @@ class CudaLidarBackend:
         self.stage: Any | None = None
         self.workspace: dict[str, torch.Tensor] = {}
         self._scenes: OrderedDict[int, _SceneAcceleration] = OrderedDict()
+        self._ray_order = RayOrder()
 
     # ------------------------------------------------------------ lifecycle
     def initialize(self, stage: Any, device: torch.device) -> None:
@@ -203,6 +233,7 @@ class CudaLidarBackend:
             batch=request.sensor_to_world.shape[0],
             active_sensor_ids=None if request.active_sensor_ids is None else request.active_sensor_ids.data_ptr(),
             active_count=0 if request.active_sensor_ids is None else request.active_sensor_ids.numel(),
+            ray_order=self._ray_order(request.ray_directions).data_ptr(),
         )
         out = request.outputs
         outputs = VgrLidarOutputs(

@@ -32,6 +32,7 @@ from typing import Sequence
 import torch
 
 from . import _native
+from .cuda_lidar_backend import RayOrder
 from ._native_signatures import (
     LIDAR_COUNTERS,
     LIDAR_DESCRIPTOR_BYTES,
@@ -42,6 +43,9 @@ from ._native_signatures import (
 )
 
 DESCRIPTOR_COLUMNS = 14
+
+# Trace order of the last direction tensor rendered (see cuda_lidar_backend.RayOrder).
+_RAY_ORDER = RayOrder()
 
 
 def _check(cond: bool, message: str) -> None:
@@ -261,6 +265,7 @@ def render_lidar(
         batch=batch,
         active_sensor_ids=_ptr(active),
         active_count=active.numel(),
+        ray_order=_RAY_ORDER(directions).data_ptr(),
     )
     native_outputs = VgrLidarOutputs(
         range_m=rng.data_ptr(),
