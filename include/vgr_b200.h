@@ -465,9 +465,9 @@ typedef struct vgr_lidar_scene {
 /* Shared sensor-local rays against per-sensor scenes
  * (lidar_renderer.cpp:133-210 inputs[6]). */
 /* A trace order for vgr_lidar_inputs.ray_order (no counterpart in the
- * reference): the rays sorted by a 30-bit Morton code of their direction's
- * azimuth and elevation on one angular grid, so 32 consecutive entries are a
- * compact patch of directions.  temp: vgr_lidar_ray_order_temp_bytes(rays)
+ * reference): the rays sorted by the 30-bit Hilbert-curve position of their
+ * direction's azimuth and elevation on one angular grid, so 32 consecutive
+ * entries are a compact patch of directions.  temp: vgr_lidar_ray_order_temp_bytes(rays)
  * bytes, 256-byte aligned.  Compute it once per direction set. */
 int64_t vgr_lidar_ray_order_temp_bytes(int64_t rays);
 int vgr_lidar_ray_order(const float* ray_directions, int64_t rays, int32_t* order, void* temp,

@@ -239,10 +239,10 @@ def test_lidar_ray_order_is_a_permutation_in_compact_patches():
     az, beam = order // 128, order % 128
     az_span = np.ptp(az.reshape(-1, 32), axis=1)
     beam_span = np.ptp(beam.reshape(-1, 32), axis=1)
-    # Outside the azimuth seam a warp typically covers about 14 azimuths x 5
-    # beams (2.3 x 1.3 degrees), and almost never more than 64 x 32 (the
-    # Z-order's jumps between quadrants); the given order spans 1 x 32.
+    # Outside the azimuth seam a warp typically covers 8 azimuths x 4 beams
+    # (1.4 x 1.3 degrees) and rarely more than 24 x 8; the given order spans
+    # 1 x 32.
     inner = az_span < 1024
     assert inner.mean() > 0.99
-    assert np.median(az_span[inner]) <= 16 and np.median(beam_span[inner]) <= 8
-    assert np.percentile(az_span[inner], 99) <= 64 and np.percentile(beam_span[inner], 99) <= 32
+    assert np.median(az_span[inner]) <= 10 and np.median(beam_span[inner]) <= 5
+    assert np.percentile(az_span[inner], 99) <= 24 and np.percentile(beam_span[inner], 99) <= 8

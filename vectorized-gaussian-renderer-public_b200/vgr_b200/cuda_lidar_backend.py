@@ -62,7 +62,7 @@ class _SceneAcceleration:
 
 
 class RayOrder:
-    """Trace order of a ray-direction tensor: ``vgr_lidar_ray_order``, a Morton
+    """Trace order of a ray-direction tensor: ``vgr_lidar_ray_order``, a Hilbert
     order of the directions' azimuth and elevation, so the 32 rays a warp
     traces together are a compact patch of directions and share most of their
     hierarchy walk.  Recomputed only when the tensor's storage, length or
