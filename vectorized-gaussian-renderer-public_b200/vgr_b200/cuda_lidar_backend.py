@@ -71,6 +71,7 @@ class RayOrder:
     def __init__(self) -> None:
         self._key: tuple | None = None
         self._order: torch.Tensor | None = None
+        self._temp: torch.Tensor | None = None
 
     def __call__(self, directions: torch.Tensor) -> torch.Tensor:
         key = (directions.device, directions.data_ptr(), directions.shape[0], directions._version)
@@ -78,15 +79,17 @@ class RayOrder:
             rays = directions.shape[0]
             lib = _native.load_library()
             temp_bytes = _native.check_size(lib.vgr_lidar_ray_order_temp_bytes(rays), "ray order")
-            order = torch.empty((rays,), dtype=torch.int32, device=directions.device)
-            temp = torch.empty((temp_bytes,), dtype=torch.uint8, device=directions.device)
+            # Buffers are reused while the ray count and device stay the same.
+            if self._order is None or self._order.shape[0] != rays or self._order.device != directions.device:
+                self._order = torch.empty((rays,), dtype=torch.int32, device=directions.device)
+                self._temp = torch.empty((temp_bytes,), dtype=torch.uint8, device=directions.device)
             stream = torch.cuda.current_stream(directions.device).cuda_stream
             _native.check(
-                lib.vgr_lidar_ray_order(directions.data_ptr(), rays, order.data_ptr(), temp.data_ptr(),
-                                        temp_bytes, stream),
+                lib.vgr_lidar_ray_order(directions.data_ptr(), rays, self._order.data_ptr(),
+                                        self._temp.data_ptr(), temp_bytes, stream),
                 "ray order",
             )
-            self._key, self._order = key, order
+            self._key = key
         return self._order
 
 
