@@ -171,8 +171,10 @@ __device__ __forceinline__ float fast_rcp(float x) {
 // A record that was not blended enters with alpha = 0, which leaves the
 // pixel state unchanged and adds nothing.  Derivative values use the
 // special-function unit's exp and reciprocal (relative error ~1e-7).
-__device__ __forceinline__ void backward_pixel(PixelGrad& q, bool c, float oe, float e,
-                                               const float4& col, float dx, float dy, float* g) {
+// Returns dL/dpower; the caller forms the moments of the thread's pixels
+// (which share dx) together.
+__device__ __forceinline__ float backward_pixel(PixelGrad& q, bool c, float oe, float e,
+                                                const float4& col, float* g) {
   const bool unclamped = c && oe < kMaxAlpha;
   const float alpha = c ? fminf(kMaxAlpha, oe) : 0.0f;
   const float de = unclamped ? e : 0.0f;          // d alpha / d opacity
@@ -189,14 +191,7 @@ __device__ __forceinline__ void backward_pixel(PixelGrad& q, bool c, float oe, f
   g[kGBlue] = fmaf(q.gb, w, g[kGBlue]);
   g[kGDepth] = fmaf(q.gz, w, g[kGDepth]);
   g[kGOpacity] = fmaf(d_alpha, de, g[kGOpacity]);
-  const float dp = d_alpha * dpow;
-  const float dpx = dp * dx;
-  const float dpy = dp * dy;
-  g[kMDx] += dpx;
-  g[kMDy] += dpy;
-  g[kMDxx] = fmaf(dpx, dx, g[kMDxx]);
-  g[kMDxy] = fmaf(dpx, dy, g[kMDxy]);
-  g[kMDyy] = fmaf(dpy, dy, g[kMDyy]);
+  return d_alpha * dpow;
 }
 
 template <int kTile>
@@ -305,8 +300,15 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
           float g[kRecordGradCount];
 #pragma unroll
           for (int f = 0; f < kRecordGradCount; ++f) g[f] = 0.0f;
-          backward_pixel(q0, c0, oe0, e0, col, dx, dy0, g);
-          backward_pixel(q1, c1, oe1, e1, col, dx, dy1, g);
+          const float dp0 = backward_pixel(q0, c0, oe0, e0, col, g);
+          const float dp1 = backward_pixel(q1, c1, oe1, e1, col, g);
+          // Moments of dp against the offsets: the two pixels share dx.
+          const float dpy0 = dp0 * dy0, dpy1 = dp1 * dy1;
+          g[kMDx] = dx * (dp0 + dp1);
+          g[kMDy] = dpy0 + dpy1;
+          g[kMDxx] = dx * g[kMDx];
+          g[kMDxy] = dx * g[kMDy];
+          g[kMDyy] = fmaf(dpy0, dy0, dpy1 * dy1);
           // Transposed warp sum: four halving exchanges leave lane l with a
           // partial sum of term (l >> 1) over 16 lanes, the last one adds the
           // other half; 16 shuffles instead of 5 per term.  (Direct shared
