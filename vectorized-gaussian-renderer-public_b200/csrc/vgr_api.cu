@@ -611,8 +611,19 @@ int render_camera(const vgr_scene* scene, const vgr_cameras* cams, const vgr_out
     bp.tile_ends = ws->tile_ends;
     bp.records = static_cast<const Record*>(ws->records);
     bp.visible_capacity = ws->visible_capacity;
-    tile_scan_kernel<<<1, kTileScanThreads, 0, stream>>>(bp);
-    if ((rc = check_launch("render: tile scan")) != VGR_OK) return rc;
+    {
+      const int64_t spans = (global_tiles + kTileScanSpan - 1) / kTileScanSpan;
+      if (spans > 0) {
+        tile_span_sum_kernel<<<static_cast<unsigned>(spans), kTileSpanThreads, 0, stream>>>(bp);
+        if ((rc = check_launch("render: tile scan (sums)")) != VGR_OK) return rc;
+      }
+      tile_span_scan_kernel<<<1, kTileScanThreads, 0, stream>>>(bp, spans);
+      if ((rc = check_launch("render: tile scan (spans)")) != VGR_OK) return rc;
+      if (spans > 0) {
+        tile_span_apply_kernel<<<static_cast<unsigned>(spans), kTileSpanThreads, 0, stream>>>(bp);
+        if ((rc = check_launch("render: tile scan")) != VGR_OK) return rc;
+      }
+    }
     mark(3);
     int64_t sgrid = (ws->intersection_capacity + 2047) / 2048;
     // 16 CTAs per SM of grid-stride scatter (8: 1.09 ms, 16: 1.03 ms per

@@ -145,9 +145,9 @@ struct ScratchHeader {
   uint32_t composite_queue;    // work-item ticket of the persistent compositor
   uint32_t sort_queue[8];      // partition ticket per radix pass (LBVH sort)
   uint32_t ranges_done;
-  uint32_t bucket_total;       // keys placed in tile buckets (tile_scan_kernel)
+  uint32_t bucket_total;       // keys placed in tile buckets (tile_span_scan_kernel)
   uint32_t tail_cursor;        // overflow-sentinel keys placed after the buckets
-  uint32_t pad1;
+  uint32_t active_tiles;       // tiles with at least one key (tile_span_sum_kernel)
   unsigned long long visible_total;  // records reserved by the projection blocks
   unsigned long long isect_total;    // keys reserved by the projection blocks
   uint32_t large_tile_queue;         // tile ticket of the tile sort's large-bucket workers
@@ -184,6 +184,9 @@ constexpr int kTileSortCap = kTileSortThreads * kTileSortItems;
 constexpr int kTileSortSplitBits = 11;  // depth-range splits of one bucket
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanItems = 16;
+// Tile scan in three passes: spans of kTileScanSpan tiles, one CTA each.
+constexpr int kTileSpanThreads = 256;
+constexpr int kTileScanSpan = kTileSpanThreads * kTileScanItems;
 
 
 __host__ __device__ inline int64_t align_up(int64_t v, int64_t a) {

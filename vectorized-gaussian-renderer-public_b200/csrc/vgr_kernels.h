@@ -334,7 +334,9 @@ __global__ void project_emit_kernel(ProjectParams p);
 __global__ void dense_cutoff_kernel(DenseCutoffParams p);
 __global__ void sort_histogram_kernel(SortParams p);
 __global__ void sort_onesweep_kernel(SortParams p);
-__global__ void tile_scan_kernel(BucketParams p);
+__global__ void tile_span_sum_kernel(BucketParams p);
+__global__ void tile_span_scan_kernel(BucketParams p, int64_t spans);
+__global__ void tile_span_apply_kernel(BucketParams p);
 __global__ void bucket_scatter_kernel(BucketParams p);
 __global__ void large_tile_list_kernel(BucketParams p);
 __global__ void tile_sort_kernel(BucketParams p);
