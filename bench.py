@@ -680,8 +680,8 @@ def run_batched(args, device) -> dict:
     scene, rig = batched_workload(cameras=count)
 
     def frame_ms(sh_degree, with_stages: bool):
-        backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=16,
-                                    composite_shape=args.composite_shape or 0)
+        shape = {} if args.composite_shape is None else {"composite_shape": args.composite_shape}
+        backend = CustomCudaBackend(sh_degree=sh_degree, output_srgb=False, tile_size=16, **shape)
         service = RendererService(backend, height=rig.height, width=rig.width, max_views=count)
         service.initialize(stage=None, device=device)
         kw = scene.to(device).as_kwargs()

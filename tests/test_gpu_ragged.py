@@ -92,8 +92,9 @@ def _check_against_oracle(ragged, outputs, view, intr, tile_size):
 # pixels per thread at half occupancy) renders the oracle's bits.
 @pytest.mark.parametrize(
     "tile_size,persistent,shape",
-    [(8, False, 0), (8, False, 1), (8, True, 1), (16, False, 0), (16, True, 0), (16, False, 1), (16, True, 1),
-     (16, False, 2), (16, True, 2), (32, False, 0), (32, True, 0), (32, False, 1), (32, False, 2), (32, True, 2)],
+    [(8, False, 0), (8, False, 1), (8, True, 1), (8, False, 2), (8, True, 2), (16, False, 0), (16, True, 0),
+     (16, False, 1), (16, True, 1), (16, False, 2), (16, True, 2), (32, False, 0), (32, True, 0), (32, False, 1),
+     (32, False, 2), (32, True, 2)],
 )
 def test_ragged_batch_matches_oracle_per_camera(tile_size, persistent, shape):
     ragged, device = _setup(tile_size, persistent, shape)
@@ -142,8 +143,8 @@ def test_autotuner_picks_a_candidate_and_caches_it():
     tile = autotune_tile_size(ragged, vm, km, ids, outputs, **kw)
     persistent, shape = ragged.persistent_compositor, ragged.composite_shape
     assert tile in (8, 16, 32) and ragged.tile_size == tile and len(cache) == 1
-    # Tiles 8 (shapes 0, 1), 16 and 32 (shapes 0, 1, 2), each with both launches.
-    assert len(ragged.autotune_ms) == 16
+    # Tiles 8, 16 and 32, shapes 0, 1 and 2, each with both launches.
+    assert len(ragged.autotune_ms) == 18
     assert autotune_tile_size(ragged, vm, km, ids, outputs, **kw) == tile
     assert (ragged.persistent_compositor, ragged.composite_shape) == (persistent, shape) and len(cache) == 1
     ragged.render(vm, km, ids, outputs)

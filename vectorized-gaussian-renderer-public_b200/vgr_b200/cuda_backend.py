@@ -125,7 +125,7 @@ class CustomCudaBackend:
         mirror_reference_workspace: bool = False,
         spatial_layout: bool = True,
         persistent_compositor: bool = False,
-        composite_shape: int = 0,
+        composite_shape: int = 2,
     ) -> None:
         if max_visible_records is not None and max_visible_records <= 0:
             raise ValueError("max_visible_records must be positive.")

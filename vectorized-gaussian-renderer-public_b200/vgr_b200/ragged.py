@@ -49,7 +49,7 @@ class RaggedBatch:
         full_sensor_output: bool = True,
         headroom: float = 1.25,
         persistent_compositor: bool = False,
-        composite_shape: int = 0,
+        composite_shape: int = 2,
     ) -> None:
         if backend.device is None or not backend._packed_scene:
             raise RuntimeError("RaggedBatch needs an initialized backend with registered scenes.")
@@ -71,8 +71,9 @@ class RaggedBatch:
         # once and the hardware scheduler balances the rest).
         self.persistent_compositor = bool(persistent_compositor)
         # Compositor CTA shape (vgr_render_options.composite_shape): 0 two
-        # pixels per thread, 1 one pixel per thread, 2 two pixels per thread
-        # at half occupancy; every shape renders the same bits.
+        # pixels per thread, 1 one pixel per thread, 2 (the default) two
+        # pixels per thread at half occupancy with 512-record batches; every
+        # shape renders the same bits.
         self.composite_shape = int(composite_shape)
         self.tile_size = int(tile_size or backend.tile_size)
         self._visible_capacity = 0
@@ -350,8 +351,7 @@ def autotune_tile_size(
     class: tile size x (with ``persistent_candidates``) one CTA per tile or
     the resident work-queue grid x (with ``shape_candidates``) the
     compositor's CTA shape (composite_shape: pixels per thread and
-    occupancy; 4-pixel tiles have one shape, and on 8-pixel tiles shapes 0
-    and 2 coincide).  Each candidate is timed on the device after
+    occupancy; 4-pixel tiles have one shape).  Each candidate is timed on the device after
     calibrating its workspace; ``ragged`` is left set to the winner.
     ``cache`` maps shape classes (resolution multiset, camera count, scene
     sizes) to earlier choices.  Returns the tile size; the launch choices are
@@ -381,7 +381,7 @@ def autotune_tile_size(
     for persistent in persistent_candidates:
         for tile in candidates:
             for shape in shape_candidates:
-                if (tile == 4 and shape != 0) or (tile == 8 and shape == 2):
+                if tile == 4 and shape != 0:
                     continue  # the same kernel as shape 0
                 apply((tile, persistent, shape))
                 start = torch.cuda.Event(enable_timing=True)
