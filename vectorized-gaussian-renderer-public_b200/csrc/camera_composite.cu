@@ -228,10 +228,11 @@ __global__ void __launch_bounds__(CompositeOccupancy<kTile, kTrain, kShape>::kTh
                                   CompositeOccupancy<kTile, kTrain, kShape>::kBlocks)
     composite_kernel(CompositeParams p) {
   constexpr int kPix = CompositeShape<kShape>::kPix;
-  // Records staged per batch: the half-occupancy shape has the shared memory
-  // for 512 (fewer batch barriers: 11.0 -> 10.9 ms on the ragged frame), the
-  // others 256.
-  constexpr int kBatch = kShape == kShapeHalfOccupancy ? 2 * kCompositeBatch : kCompositeBatch;
+  // Records staged per batch: the half-occupancy shape of 16-pixel tiles has
+  // the shared memory for 512 (fewer batch barriers: 11.0 -> 10.9 ms on the
+  // ragged frame), the others 256 (one-warp CTAs of 8-pixel tiles need their
+  // residency more than fewer barriers).
+  constexpr int kBatch = kTile == 16 && kShape == kShapeHalfOccupancy ? 2 * kCompositeBatch : kCompositeBatch;
   __shared__ float4 s_geo[kBatch];  // mean_x, mean_y, -conic_xx/2, -conic_xy
   __shared__ float4 s_cpo[kBatch];  // -conic_yy/2, lo, opacity, -
   __shared__ float4 s_col[kBatch];  // r, g, b, depth

@@ -351,7 +351,8 @@ def autotune_tile_size(
     class: tile size x (with ``persistent_candidates``) one CTA per tile or
     the resident work-queue grid x (with ``shape_candidates``) the
     compositor's CTA shape (composite_shape: pixels per thread and
-    occupancy; 4-pixel tiles have one shape).  Each candidate is timed on the device after
+    occupancy; 4-pixel tiles have one shape, and on 8-pixel tiles shapes 0
+    and 2 coincide).  Each candidate is timed on the device after
     calibrating its workspace; ``ragged`` is left set to the winner.
     ``cache`` maps shape classes (resolution multiset, camera count, scene
     sizes) to earlier choices.  Returns the tile size; the launch choices are
@@ -381,7 +382,7 @@ def autotune_tile_size(
     for persistent in persistent_candidates:
         for tile in candidates:
             for shape in shape_candidates:
-                if tile == 4 and shape != 0:
+                if (tile == 4 and shape != 0) or (tile == 8 and shape == 2):
                     continue  # the same kernel as shape 0
                 apply((tile, persistent, shape))
                 start = torch.cuda.Event(enable_timing=True)
