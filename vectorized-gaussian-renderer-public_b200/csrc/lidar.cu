@@ -448,15 +448,20 @@ struct Candidate {
 // sqrt(q_max) * max(scale0, scale1) of the mean, and the ray must pass at
 // least that close (distance from the cross product, which does not cancel).
 // Only surfels that pass it load their frame and take the exact test.
-__device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const TraceParams& p,
-                                         Candidate* c) {
-  const float4 m = __ldg(&sp->m);
+__device__ __forceinline__ bool near_surfel(const float4& m, const Ray& r, const TraceParams& p) {
   const float3 dm = make_float3(m.x - r.o.x, m.y - r.o.y, m.z - r.o.z);
   const float cx = dm.y * r.d.z - dm.z * r.d.y;
   const float cy = dm.z * r.d.x - dm.x * r.d.z;
   const float cz = dm.x * r.d.y - dm.y * r.d.x;
   const float dist2 = (cx * cx + cy * cy + cz * cz) * r.inv_dd;
-  if (!(dist2 <= p.q_max * m.w * 1.001f + 1.0e-5f)) return false;
+  return dist2 <= p.q_max * m.w * 1.001f + 1.0e-5f;
+}
+
+// The exact test of a surfel that passed near_surfel.
+__device__ __forceinline__ bool evaluate_near(const Surfel* sp, const Ray& r, const TraceParams& p,
+                                              Candidate* c) {
+  const float4 m = __ldg(&sp->m);
+  const float3 dm = make_float3(m.x - r.o.x, m.y - r.o.y, m.z - r.o.z);
   const float4 n = __ldg(&sp->n);
   const float denom = n.x * r.d.x + n.y * r.d.y + n.z * r.d.z;
   const float incidence = fabsf(denom);
@@ -480,6 +485,11 @@ __device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const T
   c->weight = weight;
   c->intensity = fminf(fmaxf(refl * support * incidence, 0.0f), 1.0f);
   return true;
+}
+
+__device__ __forceinline__ bool evaluate(const Surfel* sp, const Ray& r, const TraceParams& p,
+                                         Candidate* c) {
+  return near_surfel(__ldg(&sp->m), r, p) && evaluate_near(sp, r, p, c);
 }
 
 struct TraceStats {
@@ -514,60 +524,69 @@ __device__ __forceinline__ void traverse_walk(const LidarDescriptor& sc, const R
   const int lane = threadIdx.x & 31;
   float entry[kMaxStack];
   int top = 0;
-  stack[top] = 0;
-  lanes[top] = group;
-  entry[top] = tmin;
-  ++top;
+  // The entry to process next is held in registers (the root first, then
+  // the nearer child of each node): only the farther child of a node whose
+  // two children are both hit goes through the stack.  The order of visits
+  // is the one of a stack that pushes the nearer child last.
+  int code = 0;
+  uint32_t held = group;
+  float held_entry = tmin;
+  bool have = true;
   const float kInf = __int_as_float(0x7f800000);
-  while (top > 0) {  // top, stack[] and lanes[] are the same in every lane of the group
-    --top;
-    const int code = stack[top];
-    const bool mine = ((lanes[top] >> lane) & 1u) != 0u && entry[top] <= *tmax;
+  while (true) {  // top, code, held, stack[] and lanes[] are the same in every lane of the group
+    if (!have) {
+      if (top == 0) break;
+      --top;
+      code = stack[top];
+      held = lanes[top];
+      held_entry = entry[top];
+    }
+    have = false;
+    const bool mine = ((held >> lane) & 1u) != 0u && held_entry <= *tmax;
     if (code < 0) {
       if (mine) visit(~code);
       continue;
     }
     if (!__any_sync(group, mine)) continue;
+    const BvhNode* node = sc.nodes + code;
+    const int4 kids = __ldg(&node->c);  // the same node for every lane of the group
     float el = kInf, er = kInf;
     bool hl = false, hr = false;
     if (mine) {
       ++st.nodes;
-      const BvhNode n = sc.nodes[code];
-      hl = hit_box(r, n.b0.x, n.b0.y, n.b0.z, n.b0.w, n.b1.x, n.b1.y, tmin, *tmax, &el);
-      hr = hit_box(r, n.b1.z, n.b1.w, n.b2.x, n.b2.y, n.b2.z, n.b2.w, tmin, *tmax, &er);
+      const float4 b0 = __ldg(&node->b0), b1 = __ldg(&node->b1), b2 = __ldg(&node->b2);
+      hl = hit_box(r, b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, tmin, *tmax, &el);
+      hr = hit_box(r, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w, tmin, *tmax, &er);
       if (!hl) el = kInf;
       if (!hr) er = kInf;
     }
     const unsigned ml = __ballot_sync(group, hl);
     const unsigned mr = __ballot_sync(group, hr);
     const unsigned left_first = __ballot_sync(group, hl && hr && el <= er);
-    const int needed = static_cast<int>(ml != 0u) + static_cast<int>(mr != 0u);
-    if (needed == 0) continue;
-    if (top + needed > kMaxStack) {
-      st.overflow = true;
-      return;
-    }
-    const int4 kids = sc.nodes[code].c;  // the same node for every lane of the group
     if (ml != 0u && mr != 0u) {
+      if (top + 1 > kMaxStack) {
+        st.overflow = true;
+        return;
+      }
       const bool left_near = 2 * __popc(left_first) >= __popc(ml & mr);
       stack[top] = left_near ? kids.y : kids.x;
       lanes[top] = left_near ? mr : ml;
       entry[top] = left_near ? er : el;
       ++top;
-      stack[top] = left_near ? kids.x : kids.y;
-      lanes[top] = left_near ? ml : mr;
-      entry[top] = left_near ? el : er;
-      ++top;
+      code = left_near ? kids.x : kids.y;
+      held = left_near ? ml : mr;
+      held_entry = left_near ? el : er;
+      have = true;
     } else if (ml != 0u) {
-      stack[top] = kids.x;
-      lanes[top] = ml;
-      entry[top] = el;
-      ++top;
-    } else {
-      stack[top] = kids.y;
-      lanes[top] = mr;
-      entry[top] = er;
-      ++top;
+      code = kids.x;
+      held = ml;
+      held_entry = el;
+      have = true;
+    } else if (mr != 0u) {
+      code = kids.y;
+      held = mr;
+      held_entry = er;
+      have = true;
     }
   }
 }
@@ -602,15 +621,17 @@ __device__ __forceinline__ void add_counter(int64_t* counters, int index, uint32
   }
 }
 
-// Two-warp CTAs, twenty resident per SM (1,280 threads and a 51-register
-// cap, some spills to L1): the traversal is latency-bound, and the extra
-// warps beat the spills (at 256 threads, 4 / 5 / 6 / 8 CTAs per SM measured
-// 24.5 / 22.3 / 23.2 / 24.9 ms per 16.8M-ray frame, 28.4 ms uncapped at 80
-// registers).  Ray costs vary a lot (hits, misses, grazing rays), and a CTA
-// keeps its slot until its slowest warp is done: small CTAs free their
-// slots at a finer grain, while the hardware scheduler still hands out
-// consecutive rays, which share most of their nodes.
-__global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TraceParams p) {
+// Two-warp CTAs, eighteen resident per SM (1,152 threads and a 56-register
+// cap, some spills to L1): the traversal is latency-bound, and extra warps
+// pay for some spills (per 16.8M-ray frame in ray-direction order: 20 / 18
+// CTAs per SM at 48 / 56 registers measured 13.6 / 13.3 ms, and 24 at 40
+// registers 9 % slower than 20; in the given ray order, 256-thread CTAs at
+// 4 / 5 / 6 / 8 per SM measured 24.5 / 22.3 / 23.2 / 24.9 ms).  Ray costs vary a lot (hits,
+// misses, grazing rays), and a CTA keeps its slot until its slowest warp is
+// done: small CTAs free their slots at a finer grain, while the hardware
+// scheduler still hands out consecutive rays, which share most of their
+// nodes.
+__global__ void __launch_bounds__(kTraceThreads, 18) lidar_trace_kernel(TraceParams p) {
   const int64_t work = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t total = p.active_count * p.rays;
   uint32_t traced = 0, bad_dir = 0, bad_scene = 0, bad_active = 0, returns_found = 0;
@@ -696,10 +717,19 @@ __global__ void __launch_bounds__(kTraceThreads, 20) lidar_trace_kernel(TracePar
           traverse<true>(sc, leaves, r, p.near_plane, &window, st, [&](int leaf) {
             const int begin = leaf * sc.packet;
             const int end = min(begin + sc.packet, m);
+            // Distance pre-tests of the whole leaf first, so that its
+            // surfels' loads are in flight together.
+            uint32_t near = 0u;
+#pragma unroll 4
             for (int i = begin; i < end; ++i) {
-              ++st.tests;
+              near |= near_surfel(__ldg(&sc.surfels[i].m), r, p) ? 1u << (i - begin) : 0u;
+            }
+            st.tests += static_cast<uint32_t>(end - begin);
+            while (near) {
+              const int i = begin + __ffs(near) - 1;
+              near &= near - 1u;
               Candidate c;
-              if (!evaluate(sc.surfels + i, r, p, &c)) continue;
+              if (!evaluate_near(sc.surfels + i, r, p, &c)) continue;
               ++st.candidates;
               if (!(c.t > previous_end) || c.t > window) continue;
               if (!found || c.t < best) {
