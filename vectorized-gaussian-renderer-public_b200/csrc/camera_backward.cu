@@ -276,7 +276,9 @@ __global__ void __launch_bounds__(CompositeGeometry<kTile>::kThreads)
           const float p1 = ffma(fmul(cpo.x, dy1), dy1, ffma(bdx, dy1, adx));
           const bool in0 = p0 >= cpo.y && p0 <= 0.0f && pos < q0.last;
           const bool in1 = p1 >= cpo.y && p1 <= 0.0f && pos < q1.last;
-          if (!__any_sync(0xffffffffu, in0 || in1)) continue;
+          // One vote (the ballot below) decides whether the warp takes the
+          // record: a vote on in0 || in1 before the two exponentials cost
+          // more than the exponentials it skipped.
           const float o = cpo.z;
           float e0 = fast_exp(p0);
           float e1 = fast_exp(p1);
