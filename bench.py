@@ -331,8 +331,8 @@ def time_ragged_cpu(work, cams: list[int], steps: int, warmup: int) -> tuple[flo
 # --------------------------------------------------------------------------- algorithmic bytes
 def camera_stage_bytes(g_total: int, feature_floats: int, visible: int, isects: int, tiles: int,
                        pixels: int, cameras: int) -> dict[str, float]:
-    """Algorithmic bytes per launch of each camera stage, per unit as the
-    survey's camera formula counts them: the scene read once per frame
+    """Algorithmic bytes per launch of each camera stage, counted per unit of
+    work: the scene read once per frame
     (G x (12 mean + 16 quaternion + 12 scale + 4 opacity + 8 semantic + 4F)),
     a 48-byte record written once by the projection and read once by the
     compositor, 12 bytes of key + value per intersection at emission, the
